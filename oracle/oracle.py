@@ -1,0 +1,198 @@
+"""ctypes wrapper of the CPU oracle (oracle/liboracle.so) -- test infrastructure.
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg use this
+module, always as the checker.  The product package never imports it.
+
+``Hnsw.search(mode=REFERENCE)`` reproduces hnswlib 0.9.0's ``searchKnn``
+bit-for-bit (heap tie order included); ``mode=CANONICAL`` is the tie-broken
+form the CUDA kernel implements.  ``ref_module()`` imports the reference's own
+compiled extension from ``oracle/_ref`` when it has been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+REFERENCE = 0
+CANONICAL = 1
+SPACES = {"l2": 0, "ip": 1, "cosine": 1}
+
+_lib = None
+
+
+def build(force: bool = False) -> None:
+    """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
+    targets = ["oracle"]
+    if os.path.isdir("/root/reference"):
+        targets.append("ref")
+    if force or not os.path.exists(LIB_PATH) or targets != ["oracle"]:
+        subprocess.check_call(["make", "-s", "-C", HERE] + targets)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P, U64, I32, F32 = C.c_void_p, C.c_uint64, C.c_int32, C.c_float
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_distance.restype = F32
+        L.orc_distance.argtypes = [C.c_int, P, P, U64]
+        L.orc_distances.argtypes = [C.c_int, P, P, U64, U64, P]
+        L.orc_normalize.argtypes = [P, P, U64, U64]
+        L.orc_hnsw_load.restype = P
+        L.orc_hnsw_load.argtypes = [C.c_char_p, C.c_int, U64]
+        L.orc_hnsw_free.argtypes = [P]
+        L.orc_hnsw_count.restype = U64
+        L.orc_hnsw_count.argtypes = [P]
+        L.orc_hnsw_num_deleted.restype = U64
+        L.orc_hnsw_num_deleted.argtypes = [P]
+        L.orc_hnsw_maxM0.restype = U64
+        L.orc_hnsw_maxM0.argtypes = [P]
+        L.orc_hnsw_maxlevel.restype = C.c_int
+        L.orc_hnsw_maxlevel.argtypes = [P]
+        L.orc_hnsw_labels.argtypes = [P, P]
+        L.orc_hnsw_set_deleted.restype = C.c_int
+        L.orc_hnsw_set_deleted.argtypes = [P, U64, C.c_int]
+        L.orc_hnsw_search.restype = C.c_int
+        L.orc_hnsw_search.argtypes = [P, P, U64, U64, U64, C.c_int, P, P, P, P, P, C.c_int]
+        L.orc_bf_load.restype = P
+        L.orc_bf_load.argtypes = [C.c_char_p, C.c_int, U64]
+        L.orc_bf_free.argtypes = [P]
+        L.orc_bf_count.restype = U64
+        L.orc_bf_count.argtypes = [P]
+        L.orc_bf_search.restype = C.c_int
+        L.orc_bf_search.argtypes = [P, P, U64, U64, P, P, P, P, C.c_int]
+        L.orc_bf_matrix.restype = C.c_int
+        L.orc_bf_matrix.argtypes = [C.c_int, P, U64, U64, P, U64, U64, P, P, C.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def distances(space: str, q: np.ndarray, x: np.ndarray) -> np.ndarray:
+    """Reference-order distances from one query to every row of ``x``."""
+    q = np.ascontiguousarray(q, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty(x.shape[0], np.float32)
+    lib().orc_distances(SPACES[space], _ptr(q), _ptr(x), x.shape[0], x.shape[1], _ptr(out))
+    return out
+
+
+def normalize(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(np.atleast_2d(x), np.float32)
+    out = np.empty_like(x)
+    lib().orc_normalize(_ptr(x), _ptr(out), x.shape[0], x.shape[1])
+    return out
+
+
+class Hnsw:
+    """A reference-format HNSW index file loaded by the oracle."""
+
+    def __init__(self, path: str, space: str, dim: int):
+        self.space, self.dim = space, dim
+        self._h = lib().orc_hnsw_load(path.encode(), SPACES[space], dim)
+        if not self._h:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_hnsw_free(self._h)
+            self._h = None
+
+    @property
+    def count(self) -> int:
+        return lib().orc_hnsw_count(self._h)
+
+    @property
+    def num_deleted(self) -> int:
+        return lib().orc_hnsw_num_deleted(self._h)
+
+    def labels(self) -> np.ndarray:
+        out = np.empty(self.count, np.uint64)
+        lib().orc_hnsw_labels(self._h, _ptr(out))
+        return out
+
+    def set_deleted(self, label: int, flag: bool) -> int:
+        return lib().orc_hnsw_set_deleted(self._h, int(label), int(bool(flag)))
+
+    def search(self, q, k, ef, mode=REFERENCE, allow=None, trace=False, nthreads=0):
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        if self.space == "cosine":
+            q = normalize(q)
+        nq = q.shape[0]
+        labels = np.empty((nq, k), np.uint64)
+        dists = np.empty((nq, k), np.float32)
+        counts = np.empty(nq, np.int32)
+        tr = np.zeros((nq, 4), np.int64) if trace else None
+        if allow is not None:
+            allow = np.ascontiguousarray(allow, np.uint8)
+        rc = lib().orc_hnsw_search(self._h, _ptr(q), nq, k, ef, mode, _ptr(allow), _ptr(labels), _ptr(dists),
+                                   _ptr(counts), _ptr(tr), nthreads)
+        if rc != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return (labels, dists, counts, tr) if trace else (labels, dists, counts)
+
+
+class Bf:
+    """A reference-format brute-force index file loaded by the oracle."""
+
+    def __init__(self, path: str, space: str, dim: int):
+        self.space, self.dim = space, dim
+        self._h = lib().orc_bf_load(path.encode(), SPACES[space], dim)
+        if not self._h:
+            raise RuntimeError(lib().orc_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_bf_free(self._h)
+            self._h = None
+
+    def search(self, q, k, allow=None, nthreads=0):
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        if self.space == "cosine":
+            q = normalize(q)
+        nq = q.shape[0]
+        labels = np.empty((nq, k), np.uint64)
+        dists = np.empty((nq, k), np.float32)
+        counts = np.empty(nq, np.int32)
+        if allow is not None:
+            allow = np.ascontiguousarray(allow, np.uint8)
+        lib().orc_bf_search(self._h, _ptr(q), nq, k, _ptr(allow), _ptr(labels), _ptr(dists), _ptr(counts), nthreads)
+        return labels, dists, counts
+
+
+def bf_matrix(space: str, x: np.ndarray, q: np.ndarray, k: int, nthreads: int = 0):
+    """Exact top-k rows of ``x`` for each query, in reference arithmetic."""
+    x = np.ascontiguousarray(x, np.float32)
+    q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+    labels = np.empty((q.shape[0], k), np.uint64)
+    dists = np.empty((q.shape[0], k), np.float32)
+    lib().orc_bf_matrix(SPACES[space], _ptr(x), x.shape[0], x.shape[1], _ptr(q), q.shape[0], k, _ptr(labels),
+                        _ptr(dists), nthreads)
+    return labels, dists
+
+
+def ref_module():
+    """The reference's compiled ``hnswlib`` extension from oracle/_ref, or None."""
+    if not os.path.isdir(REF_DIR):
+        return None
+    if REF_DIR not in sys.path:
+        sys.path.insert(0, REF_DIR)
+    try:
+        import hnswlib  # noqa: F401  (the reference build, not this project)
+    except ImportError:
+        return None
+    return sys.modules["hnswlib"]
