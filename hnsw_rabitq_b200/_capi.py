@@ -1,0 +1,82 @@
+"""ctypes binding of libhnswgpu.so (the C ABI declared in include/hnswgpu.h).
+
+The library is loaded from this package directory.  There is no fallback: if
+it has not been built (``python -m hnsw_rabitq_b200.build``) or cannot be
+loaded, every use raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhnswgpu.so")
+
+OK = 0
+ERR_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_LABEL, ERR_STATE, ERR_KERNEL, ERR_UNSUPPORTED = \
+    -1, -2, -3, -4, -5, -6, -7, -8, -9
+SPACE_L2, SPACE_IP, SPACE_COSINE = 0, 1, 2
+DEVICE_PTRS = 0x1
+TRACE = 0x2
+STATUS_TIMEOUT = 0x1
+STATUS_OVERFLOW = 0x2
+
+# Every function the header declares, with its ctypes signature.
+P, U64, U32, I32 = C.c_void_p, C.c_uint64, C.c_uint32, C.c_int32
+
+
+class Info(C.Structure):
+    _fields_ = [("count", U64), ("max_elements", U64), ("dim", U64), ("M", U64), ("maxM", U64), ("maxM0", U64),
+                ("ef_construction", U64), ("ef", U64), ("num_deleted", U64), ("maxlevel", I32),
+                ("enterpoint", U32), ("space", I32), ("is_bruteforce", I32), ("device_bytes", U64)]
+
+
+class SearchOpts(C.Structure):
+    _fields_ = [("flags", U32), ("reserved0", U32), ("ef", U64), ("allow", P), ("trace", P), ("stream", P)]
+
+
+SIGNATURES = {
+    "hnswgpu_last_error": (C.c_char_p, []),
+    "hnswgpu_version": (C.c_char_p, []),
+    "hnswgpu_load_hnsw": (C.c_int, [C.c_char_p, C.c_int, U64, U64, C.c_int, C.POINTER(P)]),
+    "hnswgpu_load_bf": (C.c_int, [C.c_char_p, C.c_int, U64, C.c_int, C.POINTER(P)]),
+    "hnswgpu_create_bf": (C.c_int, [C.c_int, U64, P, P, U64, U64, C.c_int, C.POINTER(P)]),
+    "hnswgpu_free": (C.c_int, [P]),
+    "hnswgpu_get_info": (C.c_int, [P, C.POINTER(Info)]),
+    "hnswgpu_set_ef": (C.c_int, [P, U64]),
+    "hnswgpu_get_labels": (C.c_int, [P, P]),
+    "hnswgpu_mark_deleted": (C.c_int, [P, U64]),
+    "hnswgpu_unmark_deleted": (C.c_int, [P, U64]),
+    "hnswgpu_search": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), P, P, P]),
+    "hnswgpu_get_status": (C.c_int, [P, C.POINTER(U32)]),
+}
+
+_lib = None
+
+
+class HnswGpuError(RuntimeError):
+    """A C-ABI call failed; ``code`` is its HNSWGPU_ERR_* status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+def lib():
+    """The loaded library (raises if it is missing: there is no CPU path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; build it with `python -m hnsw_rabitq_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise HnswGpuError(rc, lib().hnswgpu_last_error().decode())

@@ -1,0 +1,460 @@
+// Batched HNSW k-NN search on B200 (sm_100a): one warp per query.
+//
+// Replaces HierarchicalNSW::searchKnn (hnswlib/hnswalg.h:1269-1323) and its
+// level-0 beam searchBaseLayerST (hnswlib/hnswalg.h:308-440) for a whole
+// batch of queries in one launch.
+//
+// Per warp (= per query in flight) the shared memory holds
+//   * the query row,
+//   * a staging area that TMA bulk copies fill with the neighbour vectors of
+//     the node being expanded (one 16-byte aligned row per neighbour),
+//   * the candidate pool: up to ef (distance, id) keys sorted ascending, each
+//     with an "expanded" flag -- it plays the role of both of the reference's
+//     heaps (top_candidates and candidate_set, hnswalg.h:321-322),
+//   * for filtered / delete-aware searches, a second sorted list of accepted
+//     nodes that may not be returned (deleted or rejected by the filter) but
+//     must still be expanded (hnswalg.h:398-412),
+//   * a direct-mapped visited cache of node ids that replaces the
+//     VisitedListPool (hnswlib/visited_list_pool.h).
+//
+// Exactness.  The warp evaluates all neighbours of one expansion in parallel
+// and then applies the reference's sequential acceptance test
+// (`top.size() < ef || lowerBound > dist`, hnswalg.h:395, neighbours in link
+// order) in closed form: neighbour j is accepted iff
+//     #{pool entries with d <= d_j} + #{earlier allowed neighbours with d <= d_j} < ef,
+// which equals the sequential test because lowerBound after the earlier
+// insertions is the ef-th smallest distance among the pool and the earlier
+// neighbours.  A node that misses in the visited cache but was seen before is
+// either still in the pool / second list (found by exact key lookup and
+// skipped) or has d >= lowerBound and is rejected again, so cache misses cost
+// only a repeated distance, never a different result.  Ties in distance are
+// broken by internal id; on the same index the kernel therefore returns the
+// reference's labels except where distances tie exactly (the oracle's
+// "canonical" mode computes exactly this kernel's result).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device_common.cuh"
+#include "hnsw_search.h"
+
+namespace hnswgpu {
+
+namespace {
+
+struct WarpSmem {
+    uint64_t* bar;
+    float* q;
+    float* stage;
+    uint64_t* pool;
+    uint64_t* extra;
+    uint32_t* vis;
+};
+
+__device__ __forceinline__ bool is_allowed(const SearchParams& p, uint32_t id) {
+    if (p.deleted_bits && ((p.deleted_bits[id >> 5] >> (id & 31)) & 1u)) return false;
+    if (p.allow && !p.allow[id]) return false;
+    return true;
+}
+
+__device__ __forceinline__ uint32_t vis_slot(uint32_t id, uint32_t log2v) {
+    return (id * 0x9E3779B1u) >> (32 - log2v);
+}
+
+// Count of entries of the sorted array with (key & KEY_MASK) < key.
+__device__ __forceinline__ int lower_bound_key(const uint64_t* a, int n, uint64_t key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if ((a[mid] & KEY_MASK) < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+// Count of entries whose distance key is <= dk.
+__device__ __forceinline__ int upper_bound_hi(const uint64_t* a, int n, uint32_t dk) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (khi(a[mid]) <= dk) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// First unexpanded entry at index >= hint, or -1.  Updates hint.
+__device__ __forceinline__ int find_unexpanded(const uint64_t* a, int n, int& hint, int lane) {
+    for (int b = hint; b < n; b += 32) {
+        int i = b + lane;
+        bool u = i < n && !((uint32_t)a[i] & EXP_BIT);
+        unsigned m = __ballot_sync(FULL, u);
+        if (m) {
+            hint = b + __ffs(m) - 1;
+            return hint;
+        }
+    }
+    hint = n;
+    return -1;
+}
+
+// Insert the keys held by the lanes of `amask` (distinct, not present in the
+// array; `pos` = lower_bound_key of the lane's key) into the sorted array a[0,
+// size), keeping at most cap entries.  Returns the smallest insertion index.
+__device__ __forceinline__ int merge_sorted(uint64_t* a, int& size, int cap, unsigned amask, uint64_t key, int pos,
+                                            int lane) {
+    int na = __popc(amask);
+    bool mine = (amask >> lane) & 1u;
+    int rank = 0;
+    for (unsigned m = amask; m; m &= m - 1) {
+        int src = __ffs(m) - 1;
+        uint64_t k2 = shfl64(key, src);
+        rank += (k2 < key);
+    }
+    int mpos = mine ? pos : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) mpos = min(mpos, __shfl_xor_sync(FULL, mpos, o));
+    if (size > mpos) {
+        // Move the entries [mpos, size) right, last chunk first.
+        int nmove = size - mpos;
+        for (int base = mpos + ((nmove - 1) & ~31); base >= mpos; base -= 32) {
+            int i = base + lane;
+            bool have = i < size;
+            uint64_t e = have ? a[i] : 0;
+            uint64_t em = e & KEY_MASK;
+            int sh = 0;
+            for (unsigned m = amask; m; m &= m - 1) {
+                int src = __ffs(m) - 1;
+                uint64_t k2 = shfl64(key, src);
+                sh += (k2 < em);
+            }
+            __syncwarp();
+            if (have && i + sh < cap) a[i + sh] = e;
+            __syncwarp();
+        }
+    }
+    int np = pos + rank;
+    if (mine && np < cap) a[np] = key;
+    __syncwarp();
+    size = min(size + na, cap);
+    return mpos;
+}
+
+// Stage the rows of up to `cnt` nodes into stage slots [0, cnt): lane `slot`
+// ... the calling lane copies row `id` into slot `slot` when `mine`.
+__device__ __forceinline__ bool stage_rows(const SearchParams& p, WarpSmem& s, uint32_t& phase, bool mine,
+                                           uint32_t id, int slot, int cnt, int lane) {
+    if (cnt == 0) return true;
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)cnt * p.row_bytes);
+    __syncwarp();
+    if (mine)
+        bulk_g2s(s.stage + (size_t)slot * p.stage_stride, p.vecs + (size_t)id * p.row_floats, p.row_bytes, s.bar);
+    bool ok = mbar_wait(s.bar, phase);
+    phase ^= 1u;
+    return __all_sync(FULL, ok);
+}
+
+template <int SPACE>
+__device__ __forceinline__ float stage_dist(const SearchParams& p, const WarpSmem& s, int slot) {
+    return distance<SPACE>(s.q, s.stage + (size_t)slot * p.stage_stride, (int)p.dim);
+}
+
+struct Counters {
+    uint32_t upper_hops, upper_dists, l0_exp, l0_dists;
+};
+
+// Distances of `cnt` (<= 32) nodes held by lanes [0, cnt) (id per lane);
+// result returned in the owning lane.  False on a wait timeout.
+template <int SPACE>
+__device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t id,
+                                               int cnt, int lane, float& d) {
+    d = __int_as_float(0x7f800000);
+    for (int s0 = 0; s0 < cnt; s0 += (int)p.stage_slots) {
+        int n = min((int)p.stage_slots, cnt - s0);
+        bool mine = lane >= s0 && lane < s0 + n;
+        if (!stage_rows(p, s, phase, mine, id, lane - s0, n, lane)) return false;
+        float dt = lane < n ? stage_dist<SPACE>(p, s, lane) : 0.f;
+        float got = __shfl_sync(FULL, dt, (lane - s0) & 31);
+        if (mine) d = got;
+    }
+    return true;
+}
+
+template <int SPACE>
+__device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
+                           Counters& ct) {
+    const int dim = (int)p.dim;
+    const uint32_t ef = p.ef;
+    // ---- query row (normalised for the cosine space)
+    const float* qg = p.queries + (size_t)qi * p.q_stride;
+    for (int i = lane; i < (int)p.row_floats; i += 32) s.q[i] = i < dim ? qg[i] : 0.f;
+    __syncwarp();
+    if (p.normalize) {
+        float sc = 0.f;
+        if (lane == 0) sc = norm_scale(s.q, dim);
+        sc = __shfl_sync(FULL, sc, 0);
+        __syncwarp();
+        for (int i = lane; i < dim; i += 32) s.q[i] = __fmul_rn(s.q[i], sc);
+        __syncwarp();
+    }
+    const uint32_t nvis = 1u << p.log2_vis;
+    for (uint32_t i = lane; i < nvis; i += 32) s.vis[i] = INVALID_ID;
+
+    // ---- upper-layer greedy descent (hnswalg.h:1274-1302)
+    uint32_t cur = p.ep;
+    float curd;
+    if (!lane_distances<SPACE>(p, s, phase, cur, 1, lane, curd)) return false;
+    curd = __shfl_sync(FULL, curd, 0);
+    ct.upper_dists += 1;
+    const uint32_t up_stride = p.maxM + 1;
+    for (int level = p.maxlevel; level > 0; level--) {
+        while (true) {
+            const uint32_t* row = p.upper_links + (size_t)(p.upper_off[cur] + (uint32_t)(level - 1)) * up_stride;
+            int cnt = (int)(row[0] & 0xffffu);
+            ct.upper_hops += 1;
+            ct.upper_dists += cnt;
+            float best = curd;
+            uint32_t best_id = INVALID_ID;
+            for (int c0 = 0; c0 < cnt; c0 += 32) {
+                int n = min(32, cnt - c0);
+                uint32_t id = lane < n ? row[1 + c0 + lane] : INVALID_ID;
+                float d;
+                if (!lane_distances<SPACE>(p, s, phase, id, n, lane, d)) return false;
+                float m = lane < n ? d : __int_as_float(0x7f800000);
+#pragma unroll
+                for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, o));
+                if (m < best) {
+                    unsigned hit = __ballot_sync(FULL, lane < n && d == m);
+                    best = m;
+                    best_id = __shfl_sync(FULL, id, __ffs(hit) - 1);
+                }
+            }
+            if (best_id == INVALID_ID) break;
+            cur = best_id;
+            curd = best;
+        }
+    }
+
+    // ---- level-0 beam (hnswalg.h:308-440)
+    const bool bare = p.bare != 0;
+    int psize = 0, xsize = 0, hint_p = 0, hint_x = 0;
+    const int xcap = (int)p.extra_cap;
+    uint32_t status = 0;
+    if (bare || is_allowed(p, cur)) {
+        float d0;
+        if (!lane_distances<SPACE>(p, s, phase, cur, 1, lane, d0)) return false;
+        d0 = __shfl_sync(FULL, d0, 0);
+        ct.l0_dists += 1;
+        if (lane == 0) s.pool[0] = mkkey(d0, cur);
+        psize = 1;
+    } else {
+        if (lane == 0) s.extra[0] = mkkey(__int_as_float(0x7f7fffff), cur);
+        xsize = 1;
+    }
+    if (lane == 0) s.vis[vis_slot(cur, p.log2_vis)] = cur;
+    __syncwarp();
+
+    while (true) {
+        int ip = find_unexpanded(s.pool, psize, hint_p, lane);
+        int ix = bare ? -1 : find_unexpanded(s.extra, xsize, hint_x, lane);
+        uint64_t kp = ip >= 0 ? (s.pool[ip] & KEY_MASK) : ~0ull;
+        uint64_t kx = ix >= 0 ? (s.extra[ix] & KEY_MASK) : ~0ull;
+        if (ip < 0 && ix < 0) break;
+        bool from_extra = kx < kp;
+        if (from_extra && psize == (int)ef && khi(kx) > khi(s.pool[psize - 1])) break;
+        uint64_t ck = from_extra ? kx : kp;
+        __syncwarp();
+        if (lane == 0) {
+            if (from_extra) s.extra[ix] = ck | EXP_BIT;
+            else s.pool[ip] = ck | EXP_BIT;
+        }
+        __syncwarp();
+        const uint32_t cid = kid(ck);
+        ct.l0_exp += 1;
+        if (ct.l0_exp > p.max_expansions) {
+            // only reachable after a candidate-list overflow (nodes dropped
+            // from the list can be re-admitted); stop and flag the query
+            status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+            break;
+        }
+        const uint32_t* lrow = p.links0 + (size_t)cid * p.maxM0;
+        for (uint32_t c0 = 0; c0 < p.maxM0; c0 += 32) {
+            uint32_t j = c0 + lane;
+            uint32_t id = j < p.maxM0 ? __ldg(lrow + j) : INVALID_ID;
+            bool valid = id != INVALID_ID;
+            if (__ballot_sync(FULL, valid) == 0) break;
+            // duplicate ids within one list: keep the first occurrence
+            unsigned peers = __match_any_sync(FULL, id);
+            bool fresh = valid && (__ffs(peers) - 1 == lane);
+            uint32_t slot = fresh ? vis_slot(id, p.log2_vis) : 0;
+            if (fresh && s.vis[slot] == id) fresh = false;
+            __syncwarp();
+            if (fresh) s.vis[slot] = id;
+            unsigned nmask = __ballot_sync(FULL, fresh);
+            int nnew = __popc(nmask);
+            if (nnew == 0) continue;
+            ct.l0_dists += nnew;
+            // compact the fresh ids to lanes [0, nnew), evaluate, route back
+            int ci = __popc(nmask & lanemask_lt());
+            int src = __fns(nmask, 0, lane + 1);  // lane holding the (lane)-th fresh id
+            uint32_t cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
+            float dc;
+            if (!lane_distances<SPACE>(p, s, phase, cid2, nnew, lane, dc)) return false;
+            float d = __shfl_sync(FULL, dc, ci & 31);
+            // ---- acceptance (closed form of the sequential test)
+            uint32_t dk = fkey(d);
+            bool full = psize == (int)ef;
+            uint32_t lbk = full ? khi(s.pool[psize - 1]) : 0xffffffffu;
+            bool live = fresh && !(full && dk >= lbk);
+            uint64_t key = ((uint64_t)dk << 32) | id;
+            int posP = 0, posX = 0, cntP = 0;
+            if (live) {
+                posP = lower_bound_key(s.pool, psize, key);
+                if (posP < psize && (s.pool[posP] & KEY_MASK) == key) live = false;
+                if (live && !bare) {
+                    posX = lower_bound_key(s.extra, xsize, key);
+                    if (posX < xsize && (s.extra[posX] & KEY_MASK) == key) live = false;
+                }
+                if (live) cntP = upper_bound_hi(s.pool, psize, dk);
+            }
+            bool allowed = bare || (live && is_allowed(p, id));
+            unsigned amask = __ballot_sync(FULL, live && allowed);
+            int cntN = 0;
+            for (unsigned m = amask; m; m &= m - 1) {
+                int src2 = __ffs(m) - 1;
+                uint32_t dk2 = __shfl_sync(FULL, dk, src2);
+                cntN += (src2 < lane && dk2 <= dk);
+            }
+            bool accept = live && (uint32_t)(cntP + cntN) < ef;
+            unsigned pmask = __ballot_sync(FULL, accept && allowed);
+            unsigned xmask = bare ? 0u : __ballot_sync(FULL, accept && !allowed);
+            if (pmask) {
+                int m = merge_sorted(s.pool, psize, (int)ef, pmask, key, posP, lane);
+                hint_p = min(hint_p, m);
+            }
+            if (xmask) {
+                if (xsize + __popc(xmask) > xcap) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+                int m = merge_sorted(s.extra, xsize, xcap, xmask, key, posX, lane);
+                hint_x = min(hint_x, m);
+            }
+            if (!bare && psize == (int)ef && xsize > 0) {
+                // entries beyond lowerBound can never be expanded again
+                xsize = upper_bound_hi(s.extra, xsize, khi(s.pool[psize - 1]));
+                hint_x = min(hint_x, xsize);
+            }
+        }
+    }
+
+    // ---- results: the k smallest pool entries, ordered by (distance, label)
+    const uint32_t k = p.k;
+    const int kk = min((int)k, psize);
+    uint64_t* olab = p.out_labels + (size_t)qi * k;
+    float* odist = p.out_dists + (size_t)qi * k;
+    for (int r = lane; r < kk; r += 32) {
+        uint64_t e = s.pool[r];
+        uint32_t dk = khi(e);
+        uint64_t lab = p.labels[kid(e)];
+        int st = r;
+        while (st > 0 && khi(s.pool[st - 1]) == dk) st--;
+        int below = 0;
+        for (int t = st; t < kk && khi(s.pool[t]) == dk; t++) {
+            uint64_t lt = p.labels[kid(s.pool[t])];
+            if (t != r && (lt < lab || (lt == lab && t < r))) below++;
+        }
+        olab[st + below] = lab;
+        odist[st + below] = funkey(dk);
+    }
+    for (int r = kk + lane; r < (int)k; r += 32) {
+        olab[r] = ~0ull;
+        odist[r] = __int_as_float(0x7f800000);
+    }
+    if (lane == 0) {
+        p.out_counts[qi] = kk;
+        if (status) atomicOr(p.status, status);
+    }
+    return true;
+}
+
+template <int SPACE>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) hnsw_search_kernel(SearchParams p) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* base = smem + (size_t)warp * p.warp_smem;
+    WarpSmem s;
+    s.bar = reinterpret_cast<uint64_t*>(base);
+    s.q = reinterpret_cast<float*>(base + p.off_query);
+    s.stage = reinterpret_cast<float*>(base + p.off_stage);
+    s.pool = reinterpret_cast<uint64_t*>(base + p.off_pool);
+    s.extra = reinterpret_cast<uint64_t*>(base + p.off_extra);
+    s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
+    if (lane == 0) mbar_init(s.bar, 1);
+    fence_mbar_init();
+    __syncwarp();
+    uint32_t phase = 0;
+    while (true) {
+        uint32_t qi = 0;
+        if (lane == 0) qi = atomicAdd(p.work_counter, 1u);
+        qi = __shfl_sync(FULL, qi, 0);
+        if (qi >= p.nq) break;
+        Counters ct = {0, 0, 0, 0};
+        if (!search_one<SPACE>(p, s, phase, qi, lane, ct)) {
+            if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
+            // wait (bounded) for this warp's copies still in flight, then leave
+            mbar_wait(s.bar, phase);
+            return;
+        }
+        if (p.trace && lane == 0) {
+            uint32_t* t = p.trace + (size_t)qi * 4;
+            t[0] = ct.upper_hops;
+            t[1] = ct.upper_dists;
+            t[2] = ct.l0_exp;
+            t[3] = ct.l0_dists;
+        }
+    }
+}
+
+}  // namespace
+
+size_t warp_smem_layout(SearchParams& p) {
+    size_t off = 16;  // mbarrier (8 bytes) + pad
+    p.off_query = (uint32_t)off;
+    off += (size_t)p.row_floats * 4;
+    off = (off + 15) & ~(size_t)15;
+    p.off_stage = (uint32_t)off;
+    off += (size_t)p.stage_slots * p.stage_stride * 4;
+    off = (off + 7) & ~(size_t)7;
+    p.off_pool = (uint32_t)off;
+    off += (size_t)p.ef * 8;
+    p.off_extra = (uint32_t)off;
+    off += (size_t)p.extra_cap * 8;
+    off = (off + 15) & ~(size_t)15;
+    p.off_vis = (uint32_t)off;
+    off += ((size_t)1 << p.log2_vis) * 4;
+    off = (off + 127) & ~(size_t)127;
+    p.warp_smem = (uint32_t)off;
+    return off;
+}
+
+cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
+    const void* fn = space == 0 ? (const void*)hnsw_search_kernel<0> : (const void*)hnsw_search_kernel<1>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWarpsPerBlock * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    uint64_t need = (p.nq + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)num_sms;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    if (blocks_out) *blocks_out = (int)blocks;
+    if (space == 0)
+        hnsw_search_kernel<0><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    else
+        hnsw_search_kernel<1><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    return cudaGetLastError();
+}
+
+}  // namespace hnswgpu

@@ -1,0 +1,47 @@
+// Launch parameters of the HNSW search kernel (shared by host and device).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace hnswgpu {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr uint32_t HNSWGPU_STATUS_TIMEOUT_BIT = 0x1u;
+constexpr uint32_t HNSWGPU_STATUS_OVERFLOW_BIT = 0x2u;
+
+struct SearchParams {
+    // index (device pointers)
+    const float* vecs;            // count x row_floats, rows zero-padded
+    const uint32_t* links0;       // count x maxM0 ids, unused slots = 0xffffffff
+    const uint32_t* upper_off;    // per node: first upper-level row, or 0xffffffff
+    const uint32_t* upper_links;  // rows of (maxM + 1) u32: [count][ids]
+    const uint64_t* labels;       // count
+    const uint32_t* deleted_bits; // bitmap over internal ids (null: none deleted)
+    const uint8_t* allow;         // filter mask over internal ids (null: no filter)
+    uint32_t count, dim, row_floats, row_bytes;
+    uint32_t maxM, maxM0, ep;
+    int32_t maxlevel;
+    // query batch
+    const float* queries;
+    uint32_t nq, q_stride, k, ef;
+    uint32_t bare, normalize;
+    uint32_t max_expansions;      // safety bound on level-0 expansions per query
+    // outputs
+    uint64_t* out_labels;
+    float* out_dists;
+    int32_t* out_counts;
+    uint32_t* trace;
+    uint32_t* work_counter;
+    uint32_t* status;
+    // per-warp shared memory layout
+    uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
+    uint32_t off_query, off_stage, off_pool, off_extra, off_vis, warp_smem;
+};
+
+// Fills the off_* fields and warp_smem from the sizes; returns warp_smem.
+size_t warp_smem_layout(SearchParams& p);
+cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out);
+
+}  // namespace hnswgpu

@@ -1,0 +1,667 @@
+// Host side of libhnswgpu: index-file loading, device layout, C-ABI entry
+// points (declared in include/hnswgpu.h).
+//
+// Device layout of a HierarchicalNSW index (repacked from the reference's
+// array-of-structs level-0 block, hnswlib/hnswalg.h:120-124, whose vector
+// offset 4 + 4*maxM0 is not 16-byte aligned):
+//   vecs        count x row_floats float32, row_floats = round_up(dim, 4),
+//               zero padded -> every row is a 16-byte aligned TMA source;
+//   links0      count x maxM0 uint32 neighbour ids, list order preserved,
+//               unused slots 0xffffffff (the count is implied);
+//   upper_off   per node: row index of its level-1 list in upper_links, or
+//               0xffffffff when the node has no upper levels;
+//   upper_links rows of (1 + maxM) uint32 = [count][ids] per (node, level),
+//               copied verbatim from the reference's linkLists_ blocks;
+//   labels      count x uint64 external labels;
+//   deleted     bitmap over internal ids (byte 2 bit 0 of the level-0 header,
+//               hnswalg.h:872-885).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "hnswgpu.h"
+#include "bf_search.h"
+#include "device_common.cuh"
+#include "hnsw_search.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw ApiError(e == cudaErrorMemoryAllocation ? HNSWGPU_ERR_NOMEM : HNSWGPU_ERR_CUDA,
+                       std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        cuda_check(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void ensure(size_t count) {
+        if (count > n) alloc(count);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+    ~DevBuf() { release(); }
+};
+
+template <class T>
+void rd(std::ifstream& in, T& v) {
+    in.read((char*)&v, sizeof(T));
+}
+
+}  // namespace
+
+struct hnswgpu_index {
+    int is_bf = 0;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int space = 0;
+    uint64_t dim = 0;
+    uint32_t row_floats = 0;
+    uint64_t count = 0, max_elements = 0;
+    uint64_t M = 0, maxM = 0, maxM0 = 0, efc = 0, ef = 10;
+    int32_t maxlevel = 0;
+    uint32_t ep = 0;
+    std::vector<uint64_t> labels;
+    std::unordered_map<uint64_t, uint32_t> lookup;
+    std::vector<uint32_t> deleted;  // host copy of the bitmap
+    uint64_t num_deleted = 0;
+    DevBuf<float> vecs;
+    DevBuf<uint32_t> links0, upper_off, upper_links, deleted_bits;
+    DevBuf<uint64_t> dlabels;
+    // per-call workspace
+    DevBuf<uint32_t> counters;  // ring of work counters
+    uint32_t next_counter = 0;
+    DevBuf<uint32_t> status;
+    DevBuf<unsigned char> io;  // host-pointer calls: queries + outputs
+    DevBuf<uint8_t> allow;
+    DevBuf<float> bf_norms;    // brute force: per-row helper values
+    std::mutex mu;
+    uint64_t device_bytes() const {
+        return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
+               dlabels.bytes() + bf_norms.bytes();
+    }
+};
+
+namespace {
+
+void set_device(hnswgpu_index* h) { cuda_check(cudaSetDevice(h->device), "cudaSetDevice"); }
+
+void init_common(hnswgpu_index* h, int device) {
+    h->device = device;
+    cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    cuda_check(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+    cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    h->counters.alloc(256);
+    cuda_check(cudaMemset(h->counters.p, 0, h->counters.bytes()), "cudaMemset");
+    h->status.alloc(1);
+    cuda_check(cudaMemset(h->status.p, 0, 4), "cudaMemset");
+}
+
+// HierarchicalNSW::loadIndex (hnswlib/hnswalg.h:715-821) plus the structural
+// checks a GPU kernel needs before it may follow the links (ids in range,
+// upper-level lists present where the descent reads them).
+void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim, uint64_t max_elements_i) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+    in.seekg(0, in.end);
+    const std::streamoff total = in.tellg();
+    in.seekg(0, in.beg);
+    uint64_t offsetLevel0, max_elements, cur, size_data, label_offset, offsetData, maxM, maxM0, M, efc;
+    int32_t maxlevel;
+    uint32_t ep;
+    double mult;
+    rd(in, offsetLevel0);
+    rd(in, max_elements);
+    rd(in, cur);
+    rd(in, size_data);
+    rd(in, label_offset);
+    rd(in, offsetData);
+    rd(in, maxlevel);
+    rd(in, ep);
+    rd(in, maxM);
+    rd(in, maxM0);
+    rd(in, M);
+    rd(in, mult);
+    rd(in, efc);
+    const char* corrupt = "Index seems to be corrupted or unsupported";
+    if (!in) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    const std::streamoff header_end = in.tellg();
+    // file-length walk (hnswalg.h:753-769)
+    if (size_data != 0 && cur > (uint64_t)(total - header_end) / size_data) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    std::streamoff pos = header_end + (std::streamoff)(cur * size_data);
+    in.seekg(pos, in.beg);
+    std::vector<uint32_t> ll_sizes(cur);
+    for (uint64_t i = 0; i < cur; i++) {
+        if (pos < 0 || pos >= total) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+        uint32_t sz;
+        rd(in, sz);
+        pos += 4;
+        ll_sizes[i] = sz;
+        if (sz) {
+            pos += sz;
+            in.seekg(sz, in.cur);
+        }
+    }
+    if (pos != total) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    in.clear();
+    // layout consistency the kernels rely on
+    const uint64_t size_links0 = maxM0 * 4 + 4, size_links = maxM * 4 + 4;
+    if (offsetLevel0 != 0 || offsetData != size_links0 || label_offset != offsetData + dim * 4 ||
+        size_data != label_offset + 8)
+        throw ApiError(HNSWGPU_ERR_FORMAT,
+                       "index layout does not match dim=" + std::to_string(dim) + " (" + corrupt + ")");
+    if (maxM0 == 0 || maxM0 > 4096 || maxM > 4096) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "unsupported M");
+    if (cur > 0xfffffffeull) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "more than 2^32-2 elements");
+    if (cur > 0 && (ep >= cur || maxlevel < 0)) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+
+    h->space = space;
+    h->dim = dim;
+    h->count = cur;
+    h->max_elements = max_elements_i < cur ? max_elements : max_elements_i;
+    h->M = M;
+    h->maxM = maxM;
+    h->maxM0 = maxM0;
+    h->efc = efc;
+    h->ef = 10;
+    h->maxlevel = maxlevel;
+    h->ep = ep;
+    h->row_floats = (uint32_t)((dim + 3) / 4 * 4);
+
+    // level-0 block -> vectors, links, labels, delete marks
+    in.seekg(header_end, in.beg);
+    const size_t chunk_rows = std::max<size_t>(1, (64u << 20) / std::max<uint64_t>(size_data, 1));
+    std::vector<char> buf(chunk_rows * size_data);
+    std::vector<float> hv(cur * h->row_floats, 0.f);
+    std::vector<uint32_t> hl(cur * maxM0, 0xffffffffu);
+    h->labels.resize(cur);
+    h->deleted.assign((cur + 31) / 32 + 1, 0u);
+    h->num_deleted = 0;
+    for (uint64_t r0 = 0; r0 < cur; r0 += chunk_rows) {
+        size_t nr = (size_t)std::min<uint64_t>(chunk_rows, cur - r0);
+        in.read(buf.data(), nr * size_data);
+        if (!in) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+        for (size_t r = 0; r < nr; r++) {
+            const char* rec = buf.data() + r * size_data;
+            uint64_t i = r0 + r;
+            uint16_t cnt;
+            memcpy(&cnt, rec, 2);
+            if (cnt > maxM0) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+            const uint32_t* ids = (const uint32_t*)(rec + 4);
+            for (uint32_t j = 0; j < cnt; j++) {
+                uint32_t v;
+                memcpy(&v, ids + j, 4);
+                if (v >= cur) throw ApiError(HNSWGPU_ERR_FORMAT, "cand error");
+                hl[i * maxM0 + j] = v;
+            }
+            if (rec[2] & 1) {
+                h->deleted[i >> 5] |= 1u << (i & 31);
+                h->num_deleted++;
+            }
+            memcpy(&hv[i * h->row_floats], rec + offsetData, dim * 4);
+            uint64_t lab;
+            memcpy(&lab, rec + label_offset, 8);
+            h->labels[i] = lab;
+            h->lookup[lab] = (uint32_t)i;
+        }
+    }
+    // upper levels (hnswalg.h:795-809)
+    std::vector<uint32_t> hoff(cur, 0xffffffffu);
+    std::vector<int> level(cur, 0);
+    uint64_t upper_rows = 0;
+    for (uint64_t i = 0; i < cur; i++) {
+        uint32_t sz = ll_sizes[i];
+        if (sz % size_links) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+        level[i] = (int)(sz / size_links);
+        if (sz) {
+            hoff[i] = (uint32_t)upper_rows;
+            upper_rows += sz / size_links;
+        }
+    }
+    if (cur > 0 && level[ep] < maxlevel) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    std::vector<uint32_t> hup(std::max<uint64_t>(upper_rows, 1) * (maxM + 1), 0u);
+    in.seekg(header_end + (std::streamoff)(cur * size_data), in.beg);
+    for (uint64_t i = 0; i < cur; i++) {
+        uint32_t sz;
+        rd(in, sz);
+        if (!sz) continue;
+        char* dst = (char*)(hup.data() + (size_t)hoff[i] * (maxM + 1));
+        in.read(dst, sz);
+        for (int L = 1; L <= level[i]; L++) {
+            const uint32_t* row = hup.data() + ((size_t)hoff[i] + L - 1) * (maxM + 1);
+            uint32_t c = row[0] & 0xffffu;
+            if (c > maxM) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+            for (uint32_t j = 0; j < c; j++)
+                if (row[1 + j] >= cur || level[row[1 + j]] < L) throw ApiError(HNSWGPU_ERR_FORMAT, "cand error");
+        }
+    }
+    if (!in) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+
+    h->vecs.alloc(std::max<size_t>(hv.size(), 4));
+    h->links0.alloc(std::max<size_t>(hl.size(), 1));
+    h->upper_off.alloc(std::max<size_t>(hoff.size(), 1));
+    h->upper_links.alloc(hup.size());
+    h->dlabels.alloc(std::max<size_t>(cur, 1));
+    h->deleted_bits.alloc(h->deleted.size());
+    auto up = [&](void* d, const void* s, size_t b) {
+        if (b) cuda_check(cudaMemcpy(d, s, b, cudaMemcpyHostToDevice), "cudaMemcpy");
+    };
+    up(h->vecs.p, hv.data(), hv.size() * 4);
+    up(h->links0.p, hl.data(), hl.size() * 4);
+    up(h->upper_off.p, hoff.data(), hoff.size() * 4);
+    up(h->upper_links.p, hup.data(), hup.size() * 4);
+    up(h->dlabels.p, h->labels.data(), cur * 8);
+    up(h->deleted_bits.p, h->deleted.data(), h->deleted.size() * 4);
+}
+
+// BruteforceSearch::loadIndex (hnswlib/bruteforce.h:142-161).
+void load_bf_file(hnswgpu_index* h, const char* path, int space, uint64_t dim) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+    in.seekg(0, in.end);
+    const std::streamoff total = in.tellg();
+    in.seekg(0, in.beg);
+    uint64_t maxel, size_per, cur;
+    rd(in, maxel);
+    rd(in, size_per);
+    rd(in, cur);
+    const char* corrupt = "Index seems to be corrupted or unsupported";
+    if (!in) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    size_per = dim * 4 + 8;  // recomputed from the space, as bruteforce.h:153
+    if (cur > maxel || (uint64_t)(total - 24) < cur * size_per) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    if (cur > 0xfffffffeull) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "more than 2^32-2 elements");
+    h->is_bf = 1;
+    h->space = space;
+    h->dim = dim;
+    h->count = cur;
+    h->max_elements = maxel;
+    h->row_floats = (uint32_t)((dim + 3) / 4 * 4);
+    std::vector<float> hv(cur * h->row_floats, 0.f);
+    h->labels.resize(cur);
+    std::vector<char> row(size_per);
+    for (uint64_t i = 0; i < cur; i++) {
+        in.read(row.data(), size_per);
+        memcpy(&hv[i * h->row_floats], row.data(), dim * 4);
+        uint64_t lab;
+        memcpy(&lab, row.data() + dim * 4, 8);
+        h->labels[i] = lab;
+        h->lookup[lab] = (uint32_t)i;
+    }
+    if (!in) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
+    h->vecs.alloc(std::max<size_t>(hv.size(), 4));
+    h->dlabels.alloc(std::max<size_t>(cur, 1));
+    if (!hv.empty()) cuda_check(cudaMemcpy(h->vecs.p, hv.data(), hv.size() * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+    if (cur) cuda_check(cudaMemcpy(h->dlabels.p, h->labels.data(), cur * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+}
+
+__global__ void normalize_rows_kernel(float* v, uint64_t n, uint32_t dim, uint32_t stride) {
+    uint64_t r = (uint64_t)blockIdx.x * (blockDim.x / 32) + (threadIdx.x / 32);
+    int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    float* x = v + r * stride;
+    float sc = 0.f;
+    if (lane == 0) sc = hnswgpu::norm_scale(x, (int)dim);
+    sc = __shfl_sync(0xffffffffu, sc, 0);
+    for (uint32_t i = lane; i < dim; i += 32) x[i] = __fmul_rn(x[i], sc);
+}
+
+void create_bf_from_rows(hnswgpu_index* h, int space, uint64_t dim, const float* data, const uint64_t* labels,
+                         uint64_t n, uint64_t max_elements) {
+    if (n > 0xfffffffeull) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "more than 2^32-2 elements");
+    h->is_bf = 1;
+    h->space = space;
+    h->dim = dim;
+    h->count = n;
+    h->max_elements = std::max(max_elements, n);
+    h->row_floats = (uint32_t)((dim + 3) / 4 * 4);
+    h->labels.assign(labels, labels + n);
+    for (uint64_t i = 0; i < n; i++) h->lookup[labels[i]] = (uint32_t)i;
+    std::vector<float> hv(n * h->row_floats, 0.f);
+    for (uint64_t i = 0; i < n; i++) memcpy(&hv[i * h->row_floats], data + i * dim, dim * 4);
+    h->vecs.alloc(std::max<size_t>(hv.size(), 4));
+    h->dlabels.alloc(std::max<size_t>(n, 1));
+    if (n) {
+        cuda_check(cudaMemcpy(h->vecs.p, hv.data(), hv.size() * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+        cuda_check(cudaMemcpy(h->dlabels.p, labels, n * 8, cudaMemcpyHostToDevice), "cudaMemcpy");
+        if (space == HNSWGPU_SPACE_COSINE) {
+            unsigned blocks = (unsigned)((n + 7) / 8);
+            normalize_rows_kernel<<<blocks, 256, 0, h->stream>>>(h->vecs.p, n, (uint32_t)dim, h->row_floats);
+            cuda_check(cudaGetLastError(), "normalize launch");
+            cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        }
+    }
+}
+
+uint32_t next_pow2_log2(uint64_t v) {
+    uint32_t l = 0;
+    while ((1ull << l) < v) l++;
+    return l;
+}
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(F fn) {
+    try {
+        g_last_error.clear();
+        return fn();
+    } catch (const ApiError& e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(HNSWGPU_ERR_NOMEM, "Not enough memory");
+    } catch (const std::exception& e) {
+        return fail(HNSWGPU_ERR_ARG, e.what());
+    }
+}
+
+// One HNSW search launch on device buffers.
+void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
+              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st) {
+    hnswgpu::SearchParams p{};
+    p.vecs = h->vecs.p;
+    p.links0 = h->links0.p;
+    p.upper_off = h->upper_off.p;
+    p.upper_links = h->upper_links.p;
+    p.labels = h->dlabels.p;
+    p.deleted_bits = h->num_deleted ? h->deleted_bits.p : nullptr;
+    p.allow = dallow;
+    p.count = (uint32_t)h->count;
+    p.dim = (uint32_t)h->dim;
+    p.row_floats = h->row_floats;
+    p.row_bytes = h->row_floats * 4;
+    p.maxM = (uint32_t)h->maxM;
+    p.maxM0 = (uint32_t)h->maxM0;
+    p.ep = h->ep;
+    p.maxlevel = h->maxlevel;
+    p.queries = dq;
+    p.nq = (uint32_t)nq;
+    p.q_stride = (uint32_t)h->dim;
+    p.k = (uint32_t)k;
+    p.ef = (uint32_t)std::max(ef, k);
+    p.bare = (h->num_deleted == 0 && dallow == nullptr) ? 1u : 0u;
+    p.normalize = h->space == HNSWGPU_SPACE_COSINE ? 1u : 0u;
+    p.max_expansions = (uint32_t)std::min<uint64_t>(0xffffff00ull, 2 * h->count + 1024);
+    p.out_labels = dl;
+    p.out_dists = dd;
+    p.out_counts = dc;
+    p.trace = dtrace;
+    p.status = h->status.p;
+    p.stage_stride = h->row_floats + 4;
+    uint32_t slots = (uint32_t)((17u * 1024u) / (p.stage_stride * 4));
+    p.stage_slots = std::max(1u, std::min(32u, slots));
+    p.extra_cap = p.bare ? 0u : std::max<uint32_t>(128u, 4u * p.ef);
+    p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
+    size_t ws = hnswgpu::warp_smem_layout(p);
+    int max_optin = 0;
+    cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+    while (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin && p.log2_vis > 8) {
+        p.log2_vis--;
+        ws = hnswgpu::warp_smem_layout(p);
+    }
+    if (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin)
+        throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
+    uint32_t slot = h->next_counter++ % (uint32_t)h->counters.n;
+    p.work_counter = h->counters.p + slot;
+    cuda_check(cudaMemsetAsync(p.work_counter, 0, 4, st), "cudaMemsetAsync");
+    cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
+               "hnsw_search launch");
+}
+
+void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
+                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st) {
+    if (h->is_bf) {
+        hnswgpu::BfParams b{};
+        b.vecs = h->vecs.p;
+        b.labels = h->dlabels.p;
+        b.allow = dallow;
+        b.count = (uint32_t)h->count;
+        b.dim = (uint32_t)h->dim;
+        b.row_floats = h->row_floats;
+        b.queries = dq;
+        b.nq = (uint32_t)nq;
+        b.k = (uint32_t)k;
+        b.normalize = h->space == HNSWGPU_SPACE_COSINE ? 1u : 0u;
+        b.out_labels = dl;
+        b.out_dists = dd;
+        b.out_counts = dc;
+        b.status = h->status.p;
+        cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
+                   "bf_search launch");
+    } else {
+        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hnswgpu_last_error(void) { return g_last_error.c_str(); }
+
+const char* hnswgpu_version(void) { return "hnswgpu 0.1 (sm_100a)"; }
+
+int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_elements, int device,
+                      hnswgpu_index** out) {
+    return guarded([&] {
+        if (!path || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
+        *out = nullptr;
+        std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
+        init_common(h.get(), device);
+        load_hnsw_file(h.get(), path, space, dim, max_elements);
+        *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_load_bf(const char* path, int space, uint64_t dim, int device, hnswgpu_index** out) {
+    return guarded([&] {
+        if (!path || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
+        *out = nullptr;
+        std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
+        init_common(h.get(), device);
+        load_bf_file(h.get(), path, space, dim);
+        *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_create_bf(int space, uint64_t dim, const float* data, const uint64_t* labels, uint64_t n,
+                      uint64_t max_elements, int device, hnswgpu_index** out) {
+    return guarded([&] {
+        if (!out || dim == 0 || (n && (!data || !labels))) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
+        *out = nullptr;
+        std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
+        init_common(h.get(), device);
+        create_bf_from_rows(h.get(), space, dim, data, labels, n, max_elements);
+        *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_free(hnswgpu_index* h) {
+    if (!h) return HNSWGPU_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) {
+        cudaStreamSynchronize(h->stream);
+        cudaStreamDestroy(h->stream);
+    }
+    delete h;
+    return HNSWGPU_OK;
+}
+
+int hnswgpu_get_info(const hnswgpu_index* h, hnswgpu_info* o) {
+    if (!h || !o) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+    memset(o, 0, sizeof(*o));
+    o->count = h->count;
+    o->max_elements = h->max_elements;
+    o->dim = h->dim;
+    o->M = h->M;
+    o->maxM = h->maxM;
+    o->maxM0 = h->maxM0;
+    o->ef_construction = h->efc;
+    o->ef = h->ef;
+    o->num_deleted = h->num_deleted;
+    o->maxlevel = h->maxlevel;
+    o->enterpoint = h->ep;
+    o->space = h->space;
+    o->is_bruteforce = h->is_bf;
+    o->device_bytes = h->device_bytes();
+    return HNSWGPU_OK;
+}
+
+int hnswgpu_set_ef(hnswgpu_index* h, uint64_t ef) {
+    if (!h) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+    h->ef = ef;
+    return HNSWGPU_OK;
+}
+
+int hnswgpu_get_labels(const hnswgpu_index* h, uint64_t* out) {
+    if (!h || (!out && h->count)) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+    if (h->count) memcpy(out, h->labels.data(), h->count * 8);
+    return HNSWGPU_OK;
+}
+
+static int set_mark(hnswgpu_index* h, uint64_t label, bool mark) {
+    return guarded([&] {
+        if (!h) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (h->is_bf) return fail(HNSWGPU_ERR_UNSUPPORTED, "brute-force indexes have no delete marks");
+        std::lock_guard<std::mutex> g(h->mu);
+        auto it = h->lookup.find(label);
+        if (it == h->lookup.end()) return fail(HNSWGPU_ERR_LABEL, "Label not found");
+        uint32_t id = it->second;
+        uint32_t& w = h->deleted[id >> 5];
+        bool cur = (w >> (id & 31)) & 1u;
+        if (mark && cur) return fail(HNSWGPU_ERR_STATE, "The requested to delete element is already deleted");
+        if (!mark && !cur) return fail(HNSWGPU_ERR_STATE, "The requested to undelete element is not deleted");
+        w ^= 1u << (id & 31);
+        h->num_deleted += mark ? 1 : (uint64_t)-1;
+        set_device(h);
+        cuda_check(cudaMemcpyAsync(h->deleted_bits.p + (id >> 5), &w, 4, cudaMemcpyHostToDevice, h->stream),
+                   "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_mark_deleted(hnswgpu_index* h, uint64_t label) { return set_mark(h, label, true); }
+int hnswgpu_unmark_deleted(hnswgpu_index* h, uint64_t label) { return set_mark(h, label, false); }
+
+int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t k, const hnswgpu_search_opts* opts,
+                   uint64_t* out_labels, float* out_dists, int32_t* out_counts) {
+    return guarded([&] {
+        if (!h || k == 0 || (nq && (!queries || !out_labels || !out_dists || !out_counts)))
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (nq > 0xffffffffull || k > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "batch too large");
+        hnswgpu_search_opts o{};
+        if (opts) o = *opts;
+        const bool dev = (o.flags & HNSWGPU_DEVICE_PTRS) != 0;
+        const bool want_trace = (o.flags & HNSWGPU_TRACE) && o.trace;
+        const uint64_t ef = o.ef ? o.ef : h->ef;
+        cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (nq == 0) return HNSWGPU_OK;
+        if (h->count == 0) {
+            // empty index: searchKnn returns nothing (hnswalg.h:1272)
+            if (dev) {
+                cuda_check(cudaMemsetAsync(out_counts, 0, nq * 4, st), "cudaMemsetAsync");
+                cuda_check(cudaMemsetAsync(out_labels, 0xff, nq * k * 8, st), "cudaMemsetAsync");
+                cuda_check(cudaMemsetAsync(out_dists, 0x7f, nq * k * 4, st), "cudaMemsetAsync");
+            } else {
+                memset(out_counts, 0, nq * 4);
+                for (uint64_t i = 0; i < nq * k; i++) {
+                    out_labels[i] = ~0ull;
+                    out_dists[i] = __builtin_inff();
+                }
+            }
+            return HNSWGPU_OK;
+        }
+        if (dev) {
+            run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
+                       want_trace ? o.trace : nullptr, st);
+            return HNSWGPU_OK;
+        }
+        // host pointers: stage through the index's device I/O buffer
+        const size_t qb = nq * h->dim * 4, lb = nq * k * 8, db = nq * k * 4, cb = nq * 4,
+                     tb = want_trace ? nq * 16 : 0;
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        h->io.ensure(al(qb) + al(lb) + al(db) + al(cb) + al(tb));
+        unsigned char* base = h->io.p;
+        float* dq = (float*)base;
+        uint64_t* dl = (uint64_t*)(base + al(qb));
+        float* dd = (float*)(base + al(qb) + al(lb));
+        int32_t* dc = (int32_t*)(base + al(qb) + al(lb) + al(db));
+        uint32_t* dt = want_trace ? (uint32_t*)(base + al(qb) + al(lb) + al(db) + al(cb)) : nullptr;
+        const uint8_t* dallow = nullptr;
+        if (o.allow) {
+            h->allow.ensure(h->count);
+            cuda_check(cudaMemcpyAsync(h->allow.p, o.allow, h->count, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+            dallow = h->allow.p;
+        }
+        cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st);
+        cuda_check(cudaMemcpyAsync(out_labels, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        if (dt) cuda_check(cudaMemcpyAsync(o.trace, dt, tb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        uint32_t status = 0;
+        cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (status & HNSWGPU_STATUS_TIMEOUT) {
+            cudaMemsetAsync(h->status.p, 0, 4, st);
+            cudaStreamSynchronize(st);
+            return fail(HNSWGPU_ERR_KERNEL, "search kernel timed out waiting for a copy");
+        }
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_get_status(hnswgpu_index* h, uint32_t* out_bits) {
+    return guarded([&] {
+        if (!h || !out_bits) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        uint32_t v = 0;
+        cuda_check(cudaMemcpyAsync(&v, h->status.p, 4, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaMemsetAsync(h->status.p, 0, 4, h->stream), "cudaMemsetAsync");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        *out_bits = v;
+        return HNSWGPU_OK;
+    });
+}
+
+}  // extern "C"

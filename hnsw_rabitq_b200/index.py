@@ -1,0 +1,373 @@
+"""Python surface of the GPU query path, shaped like hnswlib's own module.
+
+``Index`` and ``BFIndex`` keep the names, arguments, return types and error
+messages of the reference's pybind11 classes (python_bindings/bindings.cpp:
+``Index`` :145-723 / module table :933-999, ``BFIndex`` :725-930 / :1011-1033)
+for the query path: ``load_index``, ``knn_query``, ``set_ef`` / ``ef``,
+``mark_deleted`` / ``unmark_deleted`` and the metadata accessors.  Searches run
+on the GPU through libhnswgpu.so; ``num_threads`` is accepted for signature
+compatibility and has no effect.
+
+Index construction (``init_index`` / ``add_items`` / ``save_index`` on an HNSW
+``Index``) stays with the reference library: build and save there, load here.
+``BFIndex`` has no graph, so ``init_index`` / ``add_items`` work directly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import _capi
+
+_SPACES = {"l2": _capi.SPACE_L2, "ip": _capi.SPACE_IP, "cosine": _capi.SPACE_COSINE}
+
+
+def _input_rows(data) -> np.ndarray:
+    """The binding's forcecast + shape rules (bindings.cpp:97-112, 617)."""
+    a = np.ascontiguousarray(np.asarray(data), dtype=np.float32)
+    if a.ndim == 1:
+        return a.reshape(1, -1)
+    if a.ndim != 2:
+        raise RuntimeError(
+            f"Input vector data wrong shape. Number of dimensions {a.ndim}. Data must be a 1D or 2D array.")
+    return a
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class _GpuIndex:
+    def __init__(self, space: str, dim: int):
+        if space not in _SPACES:
+            raise RuntimeError("Space name must be one of l2, ip, or cosine.")
+        self.space = space
+        self.dim = int(dim)
+        self.num_threads = -1
+        self.device = 0
+        self._h = None
+        self._labels = None
+        self._filter_cache = None
+
+    # -- lifecycle
+    def _free(self):
+        if self._h:
+            _capi.lib().hnswgpu_free(self._h)
+            self._h = None
+        self._labels = None
+        self._filter_cache = None
+
+    def __del__(self):
+        try:
+            self._free()
+        except Exception:
+            pass
+
+    def set_num_threads(self, num_threads: int) -> None:
+        self.num_threads = num_threads
+
+    def _info(self) -> _capi.Info:
+        info = _capi.Info()
+        _capi.check(_capi.lib().hnswgpu_get_info(self._h, C.byref(info)))
+        return info
+
+    def _require(self):
+        if not self._h:
+            raise RuntimeError("Index not loaded: call load_index first")
+
+    def labels_by_internal_id(self) -> np.ndarray:
+        """External labels in internal-id order (positions used by filters)."""
+        self._require()
+        if self._labels is None:
+            n = self._info().count
+            out = np.empty(n, np.uint64)
+            _capi.check(_capi.lib().hnswgpu_get_labels(self._h, _ptr(out)))
+            self._labels = out
+        return self._labels
+
+    def _allow_mask(self, filter: Optional[Callable[[int], bool]]) -> Optional[np.ndarray]:
+        """Evaluate the filter functor once per label (it is called per
+        candidate in the reference, bindings.cpp:83-94); cached per callable."""
+        if filter is None:
+            return None
+        c = self._filter_cache
+        if c is not None and c[0] is filter:
+            return c[1]
+        labels = self.labels_by_internal_id()
+        mask = np.fromiter((1 if filter(int(l)) else 0 for l in labels), dtype=np.uint8, count=labels.shape[0])
+        self._filter_cache = (filter, mask)
+        return mask
+
+    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False):
+        self._require()
+        q = _input_rows(data)
+        if q.shape[1] != self.dim:
+            raise RuntimeError("Wrong dimensionality of the vectors")
+        k = int(k)
+        if k <= 0:
+            raise RuntimeError("k must be positive")
+        nq = q.shape[0]
+        labels = np.empty((nq, k), np.uint64)
+        dists = np.empty((nq, k), np.float32)
+        counts = np.empty(nq, np.int32)
+        opts = _capi.SearchOpts()
+        opts.ef = int(ef)
+        mask = self._allow_mask(filter)
+        opts.allow = mask.ctypes.data if mask is not None else None
+        tr = None
+        if trace:
+            tr = np.zeros((nq, 4), np.uint32)
+            opts.flags |= _capi.TRACE
+            opts.trace = tr.ctypes.data
+        _capi.check(_capi.lib().hnswgpu_search(self._h, _ptr(q), nq, k, C.byref(opts), _ptr(labels), _ptr(dists),
+                                               _ptr(counts)))
+        return labels, dists, counts, tr
+
+    def get_current_count(self) -> int:
+        return self._info().count if self._h else 0
+
+    def get_max_elements(self) -> int:
+        return self._info().max_elements if self._h else 0
+
+    def get_ids_list(self):
+        return [int(x) for x in self.labels_by_internal_id()]
+
+    @property
+    def element_count(self) -> int:
+        return self.get_current_count()
+
+    @property
+    def max_elements(self) -> int:
+        return self.get_max_elements()
+
+    def get_status(self) -> int:
+        """OR of kernel status bits since the last call (STATUS_OVERFLOW:
+        a filtered search overflowed its candidate list; STATUS_TIMEOUT)."""
+        self._require()
+        v = C.c_uint32()
+        _capi.check(_capi.lib().hnswgpu_get_status(self._h, C.byref(v)))
+        return int(v.value)
+
+    def device_bytes(self) -> int:
+        return self._info().device_bytes if self._h else 0
+
+
+class Index(_GpuIndex):
+    """GPU-backed ``hnswlib.Index`` (query path)."""
+
+    def __init__(self, space: str, dim: int):
+        super().__init__(space, dim)
+        self._default_ef = 10
+
+    def __repr__(self):
+        return f"<hnsw_rabitq_b200.Index(space='{self.space}', dim={self.dim})>"
+
+    def load_index(self, path_to_index: str, max_elements: int = 0, allow_replace_deleted: bool = False) -> None:
+        """Load a file written by hnswlib's ``save_index`` onto the GPU
+        (bindings.cpp:230-238 -> HierarchicalNSW::loadIndex).  ef is reset to
+        10 as the reference does (hnswalg.h:794)."""
+        self._free()
+        h = C.c_void_p()
+        _capi.check(_capi.lib().hnswgpu_load_hnsw(str(path_to_index).encode(), _SPACES[self.space], self.dim,
+                                                  int(max_elements), self.device, C.byref(h)))
+        self._h = h
+        self._default_ef = 10
+
+    def init_index(self, *args, **kwargs):
+        raise NotImplementedError(
+            "graph construction is not part of the GPU query path: build the index with hnswlib "
+            "(init_index/add_items/save_index) and load the saved file with load_index")
+
+    def add_items(self, *args, **kwargs):
+        self.init_index()
+
+    def save_index(self, *args, **kwargs):
+        raise NotImplementedError("this index is loaded read-only from an hnswlib file")
+
+    # -- ef
+    def set_ef(self, ef: int) -> None:
+        self._default_ef = int(ef)
+        if self._h:
+            _capi.check(_capi.lib().hnswgpu_set_ef(self._h, int(ef)))
+
+    @property
+    def ef(self) -> int:
+        return self._info().ef if self._h else self._default_ef
+
+    @ef.setter
+    def ef(self, value: int) -> None:
+        self.set_ef(value)
+
+    @property
+    def M(self) -> int:
+        return self._info().M if self._h else 0
+
+    @property
+    def ef_construction(self) -> int:
+        return self._info().ef_construction if self._h else 0
+
+    # -- deletes
+    def mark_deleted(self, label: int) -> None:
+        self._require()
+        _capi.check(_capi.lib().hnswgpu_mark_deleted(self._h, int(label)))
+
+    def unmark_deleted(self, label: int) -> None:
+        self._require()
+        _capi.check(_capi.lib().hnswgpu_unmark_deleted(self._h, int(label)))
+
+    # -- search
+    def knn_query(self, data, k: int = 1, num_threads: int = -1, filter: Optional[Callable[[int], bool]] = None):
+        """(labels uint64 [N, k], distances float32 [N, k]), closest first
+        (bindings.cpp:612-697).  Raises RuntimeError when a query has fewer
+        than k results, with the reference's message."""
+        labels, dists, counts, _ = self._search(data, k, filter)
+        if counts.size and counts.min() < k:
+            raise RuntimeError(
+                "Cannot return the results in a contiguous 2D array. Probably ef or M is too small")
+        return labels, dists
+
+    def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0):
+        """knn_query plus per-query work counters [upper link lists read,
+        upper distances, level-0 expansions, level-0 distances] and counts;
+        no exception for short results."""
+        return self._search(data, k, filter, ef=ef, trace=True)
+
+
+class BFIndex(_GpuIndex):
+    """GPU-backed ``hnswlib.BFIndex``."""
+
+    def __init__(self, space: str, dim: int):
+        super().__init__(space, dim)
+        self._rows = None
+        self._row_labels = None
+        self._maxel = 0
+        self._dirty = False
+        self.cur_l = 0
+
+    def __repr__(self):
+        return f"<hnsw_rabitq_b200.BFIndex(space='{self.space}', dim={self.dim})>"
+
+    def init_index(self, max_elements: int) -> None:
+        if self._rows is not None or self._h:
+            raise RuntimeError("The index is already initiated.")
+        self._maxel = int(max_elements)
+        self._rows = np.empty((0, self.dim), np.float32)
+        self._row_labels = np.empty(0, np.uint64)
+        self._dirty = True
+        self.cur_l = 0
+
+    def add_items(self, data, ids=None) -> None:
+        """BruteforceSearch::addPoint per row (bruteforce.h:64-83): a known
+        label overwrites its row in place, a new label is appended."""
+        if self._rows is None:
+            if self._h:
+                self._pull_rows()
+            else:
+                raise RuntimeError("Index not initialised: call init_index first")
+        x = _input_rows(data)
+        if x.shape[1] != self.dim:
+            raise RuntimeError("Wrong dimensionality of the vectors")
+        n = x.shape[0]
+        if ids is None:
+            ids = np.arange(self.cur_l, self.cur_l + n, dtype=np.uint64)
+        else:
+            ids = np.atleast_1d(np.asarray(ids, dtype=np.uint64))
+            if ids.shape[0] != n:
+                raise RuntimeError(
+                    f"The input label shape {ids.ndim} does not match the input data vector shape {x.ndim}")
+        if self._rows.shape[0] == 0 and np.unique(ids).shape[0] == n:
+            # fast path: a fresh index and distinct labels
+            if n > self._maxel:
+                raise RuntimeError("The number of elements exceeds the specified limit\n")
+            self._rows = x.copy()
+            self._row_labels = ids.astype(np.uint64).copy()
+            self.cur_l += n
+            self._dirty = True
+            return
+        pos = {int(l): i for i, l in enumerate(self._row_labels)}
+        rows, labs = list(self._rows), list(self._row_labels)
+        for i in range(n):
+            lab = int(ids[i])
+            if lab in pos:
+                rows[pos[lab]] = x[i]
+            else:
+                if len(rows) >= self._maxel:
+                    raise RuntimeError("The number of elements exceeds the specified limit\n")
+                pos[lab] = len(rows)
+                rows.append(x[i])
+                labs.append(lab)
+        self._rows = np.asarray(rows, np.float32).reshape(-1, self.dim)
+        self._row_labels = np.asarray(labs, np.uint64)
+        self.cur_l += n
+        self._dirty = True
+
+    def delete_vector(self, label: int) -> None:
+        """BruteforceSearch::removePoint (bruteforce.h:86-103): the last row
+        moves into the freed slot; unknown labels are ignored."""
+        if self._rows is None:
+            self._pull_rows()
+        idx = np.nonzero(self._row_labels == np.uint64(label))[0]
+        if idx.size == 0:
+            return
+        i, last = int(idx[0]), self._rows.shape[0] - 1
+        self._rows[i] = self._rows[last]
+        self._row_labels[i] = self._row_labels[last]
+        self._rows = self._rows[:last].copy()
+        self._row_labels = self._row_labels[:last].copy()
+        self._dirty = True
+
+    def _pull_rows(self):
+        raise NotImplementedError("rows of a file-loaded BFIndex are device-resident; add_items after load_index "
+                                  "is not supported")
+
+    def _sync(self):
+        if self._rows is not None and (self._dirty or not self._h):
+            if self._h:
+                _capi.lib().hnswgpu_free(self._h)
+                self._h = None
+            self._labels = None
+            self._filter_cache = None
+            h = C.c_void_p()
+            r = np.ascontiguousarray(self._rows, np.float32)
+            lab = np.ascontiguousarray(self._row_labels, np.uint64)
+            _capi.check(_capi.lib().hnswgpu_create_bf(_SPACES[self.space], self.dim, _ptr(r), _ptr(lab), r.shape[0],
+                                                      self._maxel, self.device, C.byref(h)))
+            self._h = h
+            self._dirty = False
+
+    def load_index(self, path_to_index: str, max_elements: int = 0) -> None:
+        """Load a file written by ``BFIndex.save_index`` (bruteforce.h:142-161)."""
+        self._free()
+        self._rows = None
+        h = C.c_void_p()
+        _capi.check(_capi.lib().hnswgpu_load_bf(str(path_to_index).encode(), _SPACES[self.space], self.dim,
+                                                self.device, C.byref(h)))
+        self._h = h
+        self.cur_l = self._info().count
+
+    def save_index(self, *args, **kwargs):
+        raise NotImplementedError("save_index is not part of the GPU query path")
+
+    def get_current_count(self) -> int:
+        if self._rows is not None:
+            return int(self._rows.shape[0])
+        return super().get_current_count()
+
+    def get_max_elements(self) -> int:
+        if self._rows is not None:
+            return self._maxel
+        return super().get_max_elements()
+
+    def knn_query(self, data, k: int = 1, num_threads: int = -1, filter: Optional[Callable[[int], bool]] = None):
+        """(labels, distances), closest first (bindings.cpp:850-929); raises
+        when fewer than k elements pass."""
+        data = _input_rows(data)
+        if data.shape[1] != self.dim:
+            raise RuntimeError("Wrong dimensionality of the vectors")
+        self._sync()
+        labels, dists, counts, _ = self._search(data, k, filter)
+        if counts.size and counts.min() < k:
+            raise RuntimeError("Cannot return the results in a contiguous 2D array. There are not enough elements.")
+        return labels, dists

@@ -1,0 +1,167 @@
+/*
+ * hnswgpu.h -- C ABI of the B200 (sm_100a) query path for hnswlib indexes.
+ *
+ * The library (hnsw_rabitq_b200/libhnswgpu.so) loads index files written by
+ * hnswlib 0.9.0 (HierarchicalNSW::saveIndex, BruteforceSearch::saveIndex),
+ * keeps them resident in GPU memory and answers k-nearest-neighbour queries
+ * with hand-written CUDA kernels.  Every entry point returns an int status
+ * (HNSWGPU_OK == 0, negative on failure); hnswgpu_last_error() gives the
+ * message of the calling thread's last failure.  No torch types, no C++
+ * types: plain pointers and sizes only.
+ *
+ * Which reference interface each entry point replaces is cited per function
+ * (paths are relative to the hnswlib source tree).
+ */
+#ifndef HNSWGPU_H_
+#define HNSWGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HNSWGPU_API __attribute__((visibility("default")))
+#else
+#define HNSWGPU_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+#define HNSWGPU_OK 0
+#define HNSWGPU_ERR_ARG -1        /* invalid argument (null handle, k == 0 ...)      */
+#define HNSWGPU_ERR_IO -2         /* "Cannot open file"                              */
+#define HNSWGPU_ERR_FORMAT -3     /* "Index seems to be corrupted or unsupported"    */
+#define HNSWGPU_ERR_CUDA -4       /* a CUDA runtime call failed                      */
+#define HNSWGPU_ERR_NOMEM -5      /* device or host allocation failed                */
+#define HNSWGPU_ERR_LABEL -6      /* "Label not found"                               */
+#define HNSWGPU_ERR_STATE -7      /* already deleted / not deleted                   */
+#define HNSWGPU_ERR_KERNEL -8     /* a kernel reported a failure (see last_error)    */
+#define HNSWGPU_ERR_UNSUPPORTED -9
+
+/* spaces: hnswlib::L2Space, hnswlib::InnerProductSpace, and the Python
+ * binding's "cosine" (inner product over normalised vectors,
+ * python_bindings/bindings.cpp:160-172). */
+#define HNSWGPU_SPACE_L2 0
+#define HNSWGPU_SPACE_IP 1
+#define HNSWGPU_SPACE_COSINE 2
+
+/* search flags */
+#define HNSWGPU_DEVICE_PTRS 0x1u  /* queries / outputs / allow mask are device
+                                     pointers; the call is asynchronous on
+                                     `stream` and does not synchronise.  Without
+                                     it they are host pointers and the call
+                                     copies, launches and synchronises.         */
+#define HNSWGPU_TRACE 0x2u        /* write per-query work counters to `trace`   */
+
+/* kernel status bits (hnswgpu_search_opts.status / hnswgpu_get_status) */
+#define HNSWGPU_STATUS_TIMEOUT 0x1u   /* a bounded wait gave up; results invalid   */
+#define HNSWGPU_STATUS_OVERFLOW 0x2u  /* a filtered search overflowed its
+                                         candidate list; results may differ from
+                                         the reference for the flagged queries   */
+
+typedef struct hnswgpu_index hnswgpu_index;
+
+typedef struct hnswgpu_info {
+    uint64_t count;            /* cur_element_count                             */
+    uint64_t max_elements;     /* max_elements_ after load                      */
+    uint64_t dim;
+    uint64_t M, maxM, maxM0;
+    uint64_t ef_construction;
+    uint64_t ef;               /* current ef_ (reset to 10 by load, as hnswalg.h:794) */
+    uint64_t num_deleted;
+    int32_t maxlevel;
+    uint32_t enterpoint;
+    int32_t space;
+    int32_t is_bruteforce;
+    uint64_t device_bytes;     /* bytes of index data resident on the GPU       */
+} hnswgpu_info;
+
+typedef struct hnswgpu_search_opts {
+    uint32_t flags;            /* HNSWGPU_DEVICE_PTRS | HNSWGPU_TRACE           */
+    uint32_t reserved0;
+    uint64_t ef;               /* 0: use the index's ef_ (setEf)               */
+    const uint8_t* allow;      /* optional per-internal-id byte mask: nonzero =
+                                  the filter functor accepts that node's label.
+                                  Internal ids are positions in
+                                  hnswgpu_get_labels().                        */
+    uint32_t* trace;           /* HNSWGPU_TRACE: 4 uint32 per query: upper-layer
+                                  link lists read, upper-layer distances,
+                                  level-0 expansions, level-0 distances.
+                                  Same memory kind as the queries.            */
+    void* stream;              /* cudaStream_t; NULL = the index's own stream  */
+} hnswgpu_search_opts;
+
+/* Message of this thread's last failure ("" if none). */
+HNSWGPU_API const char* hnswgpu_last_error(void);
+
+/* Library version string. */
+HNSWGPU_API const char* hnswgpu_version(void);
+
+/* Load a HierarchicalNSW index file.  Replaces the load constructor
+ * HierarchicalNSW(SpaceInterface*, const std::string& location, bool nmslib,
+ * size_t max_elements, bool allow_replace_deleted) (hnswlib/hnswalg.h:78-86)
+ * and HierarchicalNSW::loadIndex (hnswlib/hnswalg.h:715-821).  The space and
+ * dimension are not stored in the file and are supplied by the caller, as in
+ * the reference.  ef starts at 10. */
+HNSWGPU_API int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_elements, int device,
+                      hnswgpu_index** out);
+
+/* Load a BruteforceSearch index file.  Replaces
+ * BruteforceSearch(SpaceInterface*, const std::string& location)
+ * (hnswlib/bruteforce.h:35-43) and BruteforceSearch::loadIndex
+ * (hnswlib/bruteforce.h:142-161). */
+HNSWGPU_API int hnswgpu_load_bf(const char* path, int space, uint64_t dim, int device, hnswgpu_index** out);
+
+/* Build a BruteforceSearch index from rows in host memory: the state that
+ * BruteforceSearch(space, maxElements) + addPoint (hnswlib/bruteforce.h:46-83)
+ * reaches after adding `n` rows with these labels, rows in this order.  For
+ * the cosine space the rows are normalised as the Python binding's add_items
+ * does (python_bindings/bindings.cpp:241-248, 790-800). */
+HNSWGPU_API int hnswgpu_create_bf(int space, uint64_t dim, const float* data, const uint64_t* labels, uint64_t n,
+                                  uint64_t max_elements, int device, hnswgpu_index** out);
+
+/* Release the index and its device memory. */
+HNSWGPU_API int hnswgpu_free(hnswgpu_index* index);
+
+/* Index metadata. */
+HNSWGPU_API int hnswgpu_get_info(const hnswgpu_index* index, hnswgpu_info* out);
+
+/* setEf (hnswlib/hnswalg.h:173-175); the Python ef property
+ * (python_bindings/bindings.cpp:979-987). */
+HNSWGPU_API int hnswgpu_set_ef(hnswgpu_index* index, uint64_t ef);
+
+/* Labels of all elements in internal-id order (count entries); the
+ * positions are the internal ids used by hnswgpu_search_opts.allow.
+ * Mirrors getExternalLabel (hnswlib/hnswalg.h:185-189). */
+HNSWGPU_API int hnswgpu_get_labels(const hnswgpu_index* index, uint64_t* out);
+
+/* markDelete / unmarkDelete (hnswlib/hnswalg.h:852-927): set or clear the
+ * delete mark of the element with this label.  Deleted elements are still
+ * traversed but never returned.  Errors as the reference: unknown label
+ * (HNSWGPU_ERR_LABEL), already deleted / not deleted (HNSWGPU_ERR_STATE). */
+HNSWGPU_API int hnswgpu_mark_deleted(hnswgpu_index* index, uint64_t label);
+HNSWGPU_API int hnswgpu_unmark_deleted(hnswgpu_index* index, uint64_t label);
+
+/* Batched HierarchicalNSW::searchKnn (hnswlib/hnswalg.h:1269-1323) or
+ * BruteforceSearch::searchKnn (hnswlib/bruteforce.h:106-125), depending on
+ * the index kind.  queries: nq x dim float32, row-major.  Outputs: nq x k
+ * labels and distances, closest first (the order of
+ * AlgorithmInterface::searchKnnCloserFirst, hnswlib/hnswlib.h:203-221, and of
+ * the Python knn_query rows, bindings.cpp:649-654); counts[i] = number of
+ * results found for query i (< k when the index or the filter yields fewer;
+ * unused slots hold label UINT64_MAX and distance +inf).  For the cosine
+ * space the queries are normalised exactly as bindings.cpp:241-248. */
+HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint64_t nq, uint64_t k,
+                   const hnswgpu_search_opts* opts, uint64_t* out_labels, float* out_dists,
+                   int32_t* out_counts);
+
+/* OR of the kernel status bits raised by searches on this index since the
+ * last call (synchronises the index's stream); clears them. */
+HNSWGPU_API int hnswgpu_get_status(hnswgpu_index* index, uint32_t* out_bits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HNSWGPU_H_ */

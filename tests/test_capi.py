@@ -1,0 +1,110 @@
+"""C ABI checks that need no GPU: the library loads, exports every symbol the
+header declares with matching struct layouts, and the Python surface keeps
+the reference's argument checks.  No compute call is made here."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from hnsw_rabitq_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hnswgpu.h")
+
+
+def declared():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"HNSWGPU_API\s+[\w\s\*]+?\b(hnswgpu_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _capi.lib()
+    names = declared()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _capi.SIGNATURES, n
+    assert set(_capi.SIGNATURES) == set(names)
+
+
+def test_struct_layouts_match_header(tmp_path):
+    prog = tmp_path / "sz.c"
+    prog.write_text('#include <stdio.h>\n#include "hnswgpu.h"\n#include <stddef.h>\n'
+                    'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(hnswgpu_info), sizeof(hnswgpu_search_opts),'
+                    ' offsetof(hnswgpu_info, device_bytes), offsetof(hnswgpu_search_opts, stream));return 0;}\n')
+    exe = tmp_path / "sz"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)])
+    a, b, c, d = map(int, subprocess.check_output([str(exe)]).split())
+    assert a == C.sizeof(_capi.Info) and b == C.sizeof(_capi.SearchOpts)
+    assert c == _capi.Info.device_bytes.offset and d == _capi.SearchOpts.stream.offset
+
+
+def test_version_and_error_string():
+    lib = _capi.lib()
+    assert b"sm_100a" in lib.hnswgpu_version()
+    # a null handle is rejected before any CUDA call
+    rc = lib.hnswgpu_set_ef(None, 5)
+    assert rc == _capi.ERR_ARG
+    assert lib.hnswgpu_last_error() == b"invalid argument"
+    info = _capi.Info()
+    assert lib.hnswgpu_get_info(None, C.byref(info)) == _capi.ERR_ARG
+
+
+def test_python_surface_argument_checks():
+    with pytest.raises(RuntimeError, match="Space name must be one of l2, ip, or cosine."):
+        H.Index("hamming", 8)
+    with pytest.raises(RuntimeError, match="Space name must be one of l2, ip, or cosine."):
+        H.BFIndex("dot", 8)
+    idx = H.Index("l2", 8)
+    assert idx.ef == 10 and idx.get_current_count() == 0
+    idx.set_ef(77)
+    assert idx.ef == 77
+    with pytest.raises(RuntimeError, match="load_index"):
+        idx.knn_query(np.zeros((1, 8), np.float32))
+    with pytest.raises(NotImplementedError):
+        idx.add_items(np.zeros((1, 8), np.float32))
+    bf = H.BFIndex("l2", 4)
+    bf.init_index(3)
+    bf.add_items(np.eye(4, dtype=np.float32)[:3])
+    assert bf.get_current_count() == 3
+    with pytest.raises(RuntimeError, match="exceeds the specified limit"):
+        bf.add_items(np.ones((1, 4), np.float32), ids=[99])
+    with pytest.raises(RuntimeError, match="wrong shape"):
+        bf.knn_query(np.zeros((1, 1, 4), np.float32))
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU failure path")
+def test_fails_loudly_without_gpu(tmp_path):
+    """No CPU fallback: without a device the load reports a CUDA error."""
+    gold = os.path.join(ROOT, "tests", "golden", "hnsw_l2_d16.bin")
+    idx = H.Index("l2", 16)
+    with pytest.raises(_capi.HnswGpuError) as e:
+        idx.load_index(gold)
+    assert e.value.code == _capi.ERR_CUDA
+
+
+def test_datasets_deterministic_and_shaped():
+    from hnsw_rabitq_b200 import datasets as D
+    x1, q1 = D.gmm_1m_128(n=2000, nq=50)
+    x2, q2 = D.gmm_1m_128(n=2000, nq=50)
+    assert np.array_equal(x1, x2) and np.array_equal(q1, q2)
+    assert x1.dtype == np.float32 and x1.min() >= 0 and x1.max() <= 255
+    assert np.array_equal(x1, np.rint(x1))
+    x, q = D.uniform_10k()
+    assert x.shape == (10000, 128) and q.shape == (1000, 128)
+    x, q = D.gmm_unit_ip(n=500, nq=10)
+    assert np.allclose(np.linalg.norm(x, axis=1), 1, atol=1e-5)
+    x, q = D.gmm_lognormal_sigma(n=1000, nq=10)
+    assert x.shape == (1000, 96)

@@ -1,0 +1,180 @@
+"""GPU HNSW search parity (needs a B200): CUDA kernel through the C ABI vs
+the oracle (canonical mode: bit-identical) and vs the reference itself
+(reference mode / golden fixtures: identical except exact distance ties)."""
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from oracle import oracle as O
+from tests.helpers import GOLDEN, build_hnsw, compare_rows, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_index(path, space, dim):
+    g = H.Index(space, dim)
+    g.load_index(str(path))
+    return g
+
+
+def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.999):
+    dim = q.shape[1]
+    g = gpu_index(path, space, dim)
+    o = O.Hnsw(str(path), space, dim)
+    for lab in deleted:
+        g.mark_deleted(int(lab))
+        assert o.set_deleted(int(lab), True) == 0
+    g.set_ef(ef)
+    allow = None
+    if allow_fn is not None:
+        allow = np.array([1 if allow_fn(int(l)) else 0 for l in o.labels()], np.uint8)
+    assert g.get_status() == 0
+    gl, gd, gc, gt = g.knn_query_traced(q, k, filter=allow_fn)
+    assert g.get_status() == 0, "candidate list overflow or timeout"
+    cl, cd, cc, ct = o.search(q, k, ef, mode=O.CANONICAL, allow=allow, trace=True)
+    # bit-exact against the canonical oracle
+    assert np.array_equal(gc, cc)
+    assert np.array_equal(gl, cl), np.nonzero(~np.all(gl == cl, axis=1))[0][:10]
+    assert np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
+    # identical work: upper-layer counters and level-0 expansions
+    assert np.array_equal(gt[:, :3].astype(np.int64), ct[:, :3])
+    assert np.all(gt[:, 3].astype(np.int64) >= ct[:, 3])
+    # against the reference algorithm (heap tie order)
+    rl, rd, rc = o.search(q, k, ef, mode=O.REFERENCE, allow=allow)
+    same, bad = compare_rows(gl, gd, rl, rd)
+    assert same >= min_same and not bad, (same, bad[:5])
+    return g
+
+
+@pytest.mark.parametrize("space,dim,M", [("l2", 16, 8), ("l2", 128, 16), ("ip", 20, 12), ("cosine", 96, 16),
+                                         ("l2", 7, 4), ("ip", 100, 32), ("l2", 3, 6), ("cosine", 33, 10)])
+def test_parity_spaces_dims(tmp_path, space, dim, M):
+    rng = np.random.default_rng(dim * 31 + M)
+    x = rng.standard_normal((4000, dim)).astype(np.float32)
+    q = rng.standard_normal((500, dim)).astype(np.float32)
+    path = tmp_path / "idx.bin"
+    build_hnsw(path, x, space, M=M, efc=100)
+    for ef, k in ((10, 1), (10, 10), (64, 10), (200, 50)):
+        check_parity(path, space, q, k, ef)
+
+
+def test_parity_integer_data_ties(tmp_path):
+    """Integer-valued vectors (many exact ties) like the 1M x 128 workload."""
+    from hnsw_rabitq_b200.datasets import gmm_1m_128
+    x, q = gmm_1m_128(n=20000, nq=1000)
+    path = tmp_path / "gmm.bin"
+    build_hnsw(path, x, "l2", M=16, efc=100, num_threads=8)
+    for ef in (10, 48, 128, 400):
+        check_parity(path, "l2", q, 10, ef, min_same=0.995)
+
+
+def test_parity_filter_and_deletes(tmp_path):
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((5000, 24)).astype(np.float32)
+    q = rng.standard_normal((400, 24)).astype(np.float32)
+    path = tmp_path / "f.bin"
+    build_hnsw(path, x, "l2", M=12, efc=80)
+    check_parity(path, "l2", q, 10, 32, allow_fn=lambda l: l % 2 == 0)
+    check_parity(path, "l2", q, 10, 100, allow_fn=lambda l: l % 3 == 0)
+    dele = rng.choice(5000, 250, replace=False)
+    check_parity(path, "l2", q, 10, 50, deleted=dele)
+    check_parity(path, "l2", q, 5, 50, deleted=dele, allow_fn=lambda l: l % 2 == 1)
+
+
+def test_golden_fixtures():
+    g = golden()
+    cases = {"hnsw_l2_d16": "l2", "hnsw_ip_d20": "ip", "hnsw_cos_d12": "cosine", "hnsw_l2_d7_int": "l2"}
+    for name, space in cases.items():
+        q = g[f"{name}/queries"]
+        idx = gpu_index(f"{GOLDEN}/{name}.bin", space, q.shape[1])
+        for ef in (10, 32, 100):
+            idx.set_ef(ef)
+            for k in (1, 10):
+                for suffix, filt in (("", None), ("_even", lambda l: l % 2 == 0)):
+                    l, d = idx.knn_query(q, k=k, filter=filt)
+                    same, bad = compare_rows(l, d, g[f"{name}/ef{ef}_k{k}{suffix}/labels"],
+                                             g[f"{name}/ef{ef}_k{k}{suffix}/dists"])
+                    assert not bad and same >= 0.95, (name, ef, k, suffix, same, bad)
+        for lab in g[f"{name}/deleted"]:
+            idx.mark_deleted(int(lab))
+        for ef in (10, 32, 100):
+            idx.set_ef(ef)
+            l, d = idx.knn_query(q, k=10)
+            same, bad = compare_rows(l, d, g[f"{name}/ef{ef}_k10_del/labels"], g[f"{name}/ef{ef}_k10_del/dists"])
+            assert not bad, (name, ef, bad)
+            assert not np.isin(l, g[f"{name}/deleted"]).any()
+
+
+def test_edge_cases(tmp_path):
+    rng = np.random.default_rng(9)
+    # empty index: searchKnn returns nothing -> knn_query raises
+    build_hnsw(tmp_path / "e.bin", np.zeros((0, 8), np.float32), "l2")
+    g = gpu_index(tmp_path / "e.bin", "l2", 8)
+    with pytest.raises(RuntimeError, match="Cannot return the results"):
+        g.knn_query(rng.random((3, 8)), k=1)
+    _, _, c, _ = g.knn_query_traced(rng.random((3, 8)), k=2)
+    assert (c == 0).all()
+    # single element
+    x1 = rng.random((1, 8)).astype(np.float32)
+    build_hnsw(tmp_path / "one.bin", x1, "l2")
+    g = gpu_index(tmp_path / "one.bin", "l2", 8)
+    l, d = g.knn_query(rng.random((5, 8)), k=1)
+    assert (l == 0).all()
+    # k larger than the index -> fewer results -> RuntimeError; counts say how many
+    x = rng.random((50, 8)).astype(np.float32)
+    build_hnsw(tmp_path / "s.bin", x, "l2", M=4)
+    g = gpu_index(tmp_path / "s.bin", "l2", 8)
+    with pytest.raises(RuntimeError, match="Probably ef or M is too small"):
+        g.knn_query(x[:4], k=60)
+    _, _, c, _ = g.knn_query_traced(x[:4], k=60)
+    assert (c == 50).all()
+    # ef < k: the beam is max(ef, k)
+    g.set_ef(1)
+    l, d = g.knn_query(x[:4], k=5)
+    assert (l[:, 0] == np.arange(4)).all()
+    # an empty query batch
+    l, d = g.knn_query(np.zeros((0, 8), np.float32), k=3)
+    assert l.shape == (0, 3)
+    # every node filtered out
+    _, _, c, _ = g.knn_query_traced(x[:4], k=3, filter=lambda l: False)
+    assert (c == 0).all()
+    # wrong dimension
+    with pytest.raises(RuntimeError, match="dimensionality"):
+        g.knn_query(rng.random((2, 9)), k=1)
+    # mark_deleted errors match the reference
+    with pytest.raises(RuntimeError, match="Label not found"):
+        g.mark_deleted(12345)
+    g.mark_deleted(3)
+    with pytest.raises(RuntimeError, match="already deleted"):
+        g.mark_deleted(3)
+    g.unmark_deleted(3)
+    with pytest.raises(RuntimeError, match="not deleted"):
+        g.unmark_deleted(3)
+
+
+def test_load_errors(tmp_path):
+    g = H.Index("l2", 4)
+    with pytest.raises(RuntimeError, match="Cannot open file"):
+        g.load_index(str(tmp_path / "nope.bin"))
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"\x01" * 200)
+    with pytest.raises(RuntimeError, match="corrupted"):
+        g.load_index(str(bad))
+    x = np.random.default_rng(0).random((100, 8)).astype(np.float32)
+    build_hnsw(tmp_path / "ok.bin", x, "l2", M=4)
+    with pytest.raises(RuntimeError, match="dim"):
+        H.Index("l2", 9).load_index(str(tmp_path / "ok.bin"))
+    raw = (tmp_path / "ok.bin").read_bytes()
+    (tmp_path / "trunc.bin").write_bytes(raw[:-7])
+    with pytest.raises(RuntimeError, match="corrupted"):
+        H.Index("l2", 8).load_index(str(tmp_path / "trunc.bin"))
+
+
+def test_large_M_and_k(tmp_path):
+    """maxM0 = 64 (two 32-lane chunks per expansion) and k = 100 > 32."""
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal((6000, 32)).astype(np.float32)
+    q = rng.standard_normal((300, 32)).astype(np.float32)
+    build_hnsw(tmp_path / "m32.bin", x, "l2", M=32, efc=100)
+    check_parity(tmp_path / "m32.bin", "l2", q, 100, 150)
+    check_parity(tmp_path / "m32.bin", "l2", q, 10, 400)

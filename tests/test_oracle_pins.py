@@ -1,0 +1,131 @@
+"""Pin the CPU oracle to the reference (CPU only).
+
+* against the committed fixtures the reference produced (always);
+* against the reference's own compiled extension (oracle/_ref) on fresh
+  random data, when it is built here.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import GOLDEN, build_bf, build_hnsw, golden, ref_or_skip
+
+DIMS = list(range(1, 41)) + [48, 63, 64, 96, 100, 127, 128, 130, 768]
+
+
+@pytest.mark.parametrize("space", ["l2", "ip"])
+def test_distances_bit_exact_vs_reference(space):
+    hnswlib = ref_or_skip()
+    rng = np.random.default_rng(5)
+    for dim in DIMS:
+        x = rng.standard_normal((64, dim)).astype(np.float32)
+        q = rng.standard_normal((2, dim)).astype(np.float32)
+        p = hnswlib.BFIndex(space, dim)
+        p.init_index(64)
+        p.add_items(x)
+        lab, dist = p.knn_query(q, k=64)
+        for i in range(2):
+            ref = np.empty(64, np.float32)
+            ref[lab[i].astype(np.int64)] = dist[i]
+            ours = O.distances(space, q[i], x)
+            assert np.array_equal(ours.view(np.uint32), ref.view(np.uint32)), (space, dim)
+
+
+def test_known_answer_distances_golden():
+    g = golden()
+    for key in g.files:
+        if not key.startswith("spaces/") or not key.endswith("/dists"):
+            continue
+        _, space, lr, _ = key.split("/")
+        left, right = map(int, lr.split("_"))
+        base = np.array([[1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1]], np.float32)
+        x = np.concatenate([np.zeros((5, left), np.float32), base, np.zeros((5, right), np.float32)], 1)
+        xs = O.normalize(x) if space == "cosine" else x
+        lab = g[key.replace("/dists", "/labels")].astype(np.int64)[0]
+        ours = O.distances("ip" if space == "cosine" else space, xs[-1], xs)[lab]
+        assert np.array_equal(ours.view(np.uint32), g[key][0].view(np.uint32)), key
+    # the reference test's expected values (tests/python/bindings_test_spaces.py)
+    exp = {"l2": [0, 1, 2, 2, 2], "ip": [-2, -1, 0, 0, 0], "cosine": [0, 0.1835, 0.423, 0.423, 0.423]}
+    for space, e in exp.items():
+        d = g[f"spaces/{space}/0_0/dists"][0]
+        assert np.allclose(d, e, atol=1e-3), space
+
+
+def _golden_hnsw_cases():
+    return ["hnsw_l2_d16", "hnsw_ip_d20", "hnsw_cos_d12", "hnsw_l2_d7_int"]
+
+
+@pytest.mark.parametrize("name", _golden_hnsw_cases())
+def test_oracle_reference_mode_matches_golden(name):
+    g = golden()
+    space = {"hnsw_l2_d16": "l2", "hnsw_ip_d20": "ip", "hnsw_cos_d12": "cosine", "hnsw_l2_d7_int": "l2"}[name]
+    q = g[f"{name}/queries"]
+    dim = q.shape[1]
+    idx = O.Hnsw(f"{GOLDEN}/{name}.bin", space, dim)
+    labels = idx.labels()
+    even = (labels % 2 == 0).astype(np.uint8)
+    for ef in (10, 32, 100):
+        for k in (1, 10):
+            for suffix, allow in (("", None), ("_even", even)):
+                l, d, c = idx.search(q, k, ef, mode=O.REFERENCE, allow=allow)
+                assert np.array_equal(l, g[f"{name}/ef{ef}_k{k}{suffix}/labels"]), (name, ef, k, suffix)
+                assert np.array_equal(d.view(np.uint32), g[f"{name}/ef{ef}_k{k}{suffix}/dists"].view(np.uint32))
+    for lab in g[f"{name}/deleted"]:
+        assert idx.set_deleted(int(lab), True) == 0
+    for ef in (10, 32, 100):
+        l, d, c = idx.search(q, 10, ef, mode=O.REFERENCE)
+        assert np.array_equal(l, g[f"{name}/ef{ef}_k10_del/labels"])
+        assert np.array_equal(d.view(np.uint32), g[f"{name}/ef{ef}_k10_del/dists"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name,space", [("bf_l2_d7", "l2"), ("bf_ip_d16", "ip"), ("bf_cos_d9", "cosine")])
+def test_oracle_bruteforce_matches_golden(name, space):
+    g = golden()
+    q = g[f"{name}/queries"]
+    bf = O.Bf(f"{GOLDEN}/{name}.bin", space, q.shape[1])
+    for k in (1, 10, 25):
+        l, d, c = bf.search(q, k)
+        assert np.array_equal(l, g[f"{name}/k{k}/labels"])
+        assert np.array_equal(d.view(np.uint32), g[f"{name}/k{k}/dists"].view(np.uint32))
+
+
+def test_oracle_search_vs_reference_fresh(tmp_path):
+    """Reference mode == reference knn_query; canonical mode agrees on almost all rows."""
+    hnswlib = ref_or_skip()
+    rng = np.random.default_rng(11)
+    for space, dim, M in (("l2", 32, 8), ("ip", 24, 12), ("cosine", 40, 16)):
+        x = rng.standard_normal((3000, dim)).astype(np.float32)
+        q = rng.standard_normal((300, dim)).astype(np.float32)
+        path = tmp_path / f"{space}.bin"
+        p = build_hnsw(path, x, space, M=M, efc=80)
+        idx = O.Hnsw(str(path), space, dim)
+        for ef in (10, 64):
+            p.set_ef(ef)
+            rl, rd = p.knn_query(q, k=10, num_threads=1)
+            ol, od, _ = idx.search(q, 10, ef, mode=O.REFERENCE)
+            assert np.array_equal(ol, rl)
+            assert np.array_equal(od.view(np.uint32), rd.view(np.uint32))
+            cl, cd, _ = idx.search(q, 10, ef, mode=O.CANONICAL)
+            assert np.mean(np.all(cl == rl, axis=1)) >= 0.999
+
+
+def test_oracle_bruteforce_vs_reference_fresh(tmp_path):
+    ref_or_skip()
+    rng = np.random.default_rng(12)
+    for space, dim in (("l2", 21), ("ip", 36), ("cosine", 13)):
+        x = rng.standard_normal((700, dim)).astype(np.float32)
+        q = rng.standard_normal((50, dim)).astype(np.float32)
+        p = build_bf(tmp_path / "bf.bin", x, space)
+        bf = O.Bf(str(tmp_path / "bf.bin"), space, dim)
+        rl, rd = p.knn_query(q, k=15)
+        ol, od, _ = bf.search(q, 15)
+        assert np.array_equal(ol, rl) and np.array_equal(od.view(np.uint32), rd.view(np.uint32))
+
+
+def test_oracle_load_errors(tmp_path):
+    with pytest.raises(RuntimeError, match="Cannot open file"):
+        O.Hnsw(str(tmp_path / "missing.bin"), "l2", 4)
+    bad = tmp_path / "bad.bin"
+    bad.write_bytes(b"\x00" * 40)
+    with pytest.raises(RuntimeError, match="corrupted"):
+        O.Hnsw(str(bad), "l2", 4)
