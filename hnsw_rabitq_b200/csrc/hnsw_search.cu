@@ -241,6 +241,10 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     int psize = 0, xsize = 0, hint_p = 0, hint_x = 0;
     const int xcap = (int)p.extra_cap;
     uint32_t status = 0;
+    // A disallowed entry point is queued with the sentinel distance FLT_MAX
+    // (hnswalg.h:336-337) and never evaluated, so the exact-key lookup cannot
+    // recognise it when the visited cache misses on it later: skip it by id.
+    uint32_t skip_id = INVALID_ID;
     if (bare || is_allowed(p, cur)) {
         float d0;
         if (!lane_distances<SPACE>(p, s, phase, cur, 1, lane, d0)) return false;
@@ -251,6 +255,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     } else {
         if (lane == 0) s.extra[0] = mkkey(__int_as_float(0x7f7fffff), cur);
         xsize = 1;
+        skip_id = cur;
     }
     if (lane == 0) s.vis[vis_slot(cur, p.log2_vis)] = cur;
     __syncwarp();
@@ -286,7 +291,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             if (__ballot_sync(FULL, valid) == 0) break;
             // duplicate ids within one list: keep the first occurrence
             unsigned peers = __match_any_sync(FULL, id);
-            bool fresh = valid && (__ffs(peers) - 1 == lane);
+            bool fresh = valid && (__ffs(peers) - 1 == lane) && id != skip_id;
             uint32_t slot = fresh ? vis_slot(id, p.log2_vis) : 0;
             if (fresh && s.vis[slot] == id) fresh = false;
             __syncwarp();

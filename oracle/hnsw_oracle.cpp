@@ -259,7 +259,7 @@ Hnsw* load_hnsw(const char* path, int space, uint64_t dim) {
 }
 
 struct Trace {
-    int64_t upper_hops = 0, upper_dists = 0, l0_expansions = 0, l0_dists = 0;
+    int64_t upper_hops = 0, upper_dists = 0, l0_expansions = 0, l0_dists = 0, ties = 0;
 };
 
 // Upper-layer greedy descent (hnswalg.h:1274-1302).  Shared by both modes.
@@ -298,30 +298,59 @@ struct CompareByFirst {
 };
 using HeapQ = std::priority_queue<std::pair<float, uint32_t>, std::vector<std::pair<float, uint32_t>>, CompareByFirst>;
 
-// Mode 0: the reference algorithm on the reference's own heap types.
+// Mode 0: the reference algorithm on the reference's own heap discipline:
+// std::priority_queue is push_heap / pop_heap over a vector with the same
+// comparator, used here directly so that the root's children can be read.
 // searchBaseLayerST (hnswalg.h:308-440) without a stop condition.
-HeapQ base_layer_reference(const Hnsw& h, uint32_t ep, const float* q, size_t ef, bool bare,
-                           const uint8_t* allow, std::vector<uint32_t>& vis, uint32_t tag, Trace& tr) {
-    HeapQ top, cand;
+//
+// Tie events: the only decisions on which mode 0 and mode 1 can differ are
+//  (a) a pop from either heap whose root ties one of its children (the heap
+//      then picks among equal distances by its internal layout, mode 1 by id),
+//  (b) the expansion of a candidate that had been evicted from
+//      top_candidates, which the stop test only allows when its distance
+//      equals lowerBound (mode 1 forgets evicted candidates).
+// They are counted in Trace::ties; a query without tie events returns the
+// same result in both modes.
+std::vector<std::pair<float, uint32_t>> base_layer_reference(const Hnsw& h, uint32_t ep, const float* q, size_t ef,
+                                                             bool bare, const uint8_t* allow,
+                                                             std::vector<uint32_t>& vis, uint32_t tag, Trace& tr) {
+    using P = std::pair<float, uint32_t>;
+    CompareByFirst cmp;
+    std::vector<P> top, cand;
+    std::unordered_map<uint32_t, int> in_top;
+    auto root_tied = [](const std::vector<P>& v) {
+        return (v.size() > 1 && v[1].first == v[0].first) || (v.size() > 2 && v[2].first == v[0].first);
+    };
+    auto push = [&](std::vector<P>& v, P e) {
+        v.push_back(e);
+        std::push_heap(v.begin(), v.end(), cmp);
+    };
+    auto pop = [&](std::vector<P>& v) {
+        if (root_tied(v)) tr.ties++;
+        std::pop_heap(v.begin(), v.end(), cmp);
+        v.pop_back();
+    };
     auto allowed = [&](uint32_t id) { return !h.deleted(id) && (!allow || allow[id]); };
     float lb;
     if (bare || allowed(ep)) {
         float d = dist(h.space, q, h.vec(ep), h.dim);
         tr.l0_dists++;
         lb = d;
-        top.emplace(d, ep);
-        cand.emplace(-d, ep);
+        push(top, {d, ep});
+        in_top[ep]++;
+        push(cand, {-d, ep});
     } else {
         lb = std::numeric_limits<float>::max();
-        cand.emplace(-lb, ep);
+        push(cand, {-lb, ep});
     }
     vis[ep] = tag;
     while (!cand.empty()) {
-        auto cp = cand.top();
+        P cp = cand.front();
         float cd = -cp.first;
         bool stop = bare ? (cd > lb) : (cd > lb && top.size() == ef);
         if (stop) break;
-        cand.pop();
+        if (cd == lb && !in_top.count(cp.second) && (bare || allowed(cp.second))) tr.ties++;
+        pop(cand);
         const uint32_t* ll = h.links0(cp.second);
         size_t size = Hnsw::count(ll);
         tr.l0_expansions++;
@@ -332,10 +361,17 @@ HeapQ base_layer_reference(const Hnsw& h, uint32_t ep, const float* q, size_t ef
             float d = dist(h.space, q, h.vec(c), h.dim);
             tr.l0_dists++;
             if (top.size() < ef || lb > d) {
-                cand.emplace(-d, c);
-                if (bare || allowed(c)) top.emplace(d, c);
-                while (top.size() > ef) top.pop();
-                if (!top.empty()) lb = top.top().first;
+                push(cand, {-d, c});
+                if (bare || allowed(c)) {
+                    push(top, {d, c});
+                    in_top[c]++;
+                }
+                while (top.size() > ef) {
+                    uint32_t gone = top.front().second;
+                    pop(top);
+                    if (--in_top[gone] == 0) in_top.erase(gone);
+                }
+                if (!top.empty()) lb = top.front().first;
             }
         }
     }
@@ -437,12 +473,20 @@ void search_one(const Hnsw& h, const float* q, size_t k, size_t ef, int mode, co
     tag++;
     if (tag == 0) { std::fill(vis.begin(), vis.end(), 0u); tag = 1; }
     if (mode == 0) {
-        HeapQ top = base_layer_reference(h, cur, q, ef2, bare, allow, vis, tag, tr);
-        while (top.size() > k) top.pop();
+        std::vector<std::pair<float, uint32_t>> top = base_layer_reference(h, cur, q, ef2, bare, allow, vis, tag, tr);
+        CompareByFirst cmp;
+        auto pop_top = [&] {
+            if ((top.size() > 1 && top[1].first == top[0].first) || (top.size() > 2 && top[2].first == top[0].first))
+                tr.ties++;
+            std::pop_heap(top.begin(), top.end(), cmp);
+            top.pop_back();
+        };
+        while (top.size() > k) pop_top();
         std::priority_queue<std::pair<float, uint64_t>> result;
         while (!top.empty()) {
-            result.emplace(top.top().first, h.label(top.top().second));
-            top.pop();
+            result.emplace(top.front().first, h.label(top.front().second));
+            std::pop_heap(top.begin(), top.end(), cmp);
+            top.pop_back();
         }
         out.res.resize(result.size());
         size_t n = result.size();
@@ -594,8 +638,9 @@ int orc_hnsw_set_deleted(void* p, uint64_t label, int flag) {
 // Batched searchKnn.  mode 0 = reference heaps, 1 = canonical pool.
 // allow: optional per-internal-id byte mask (the filter functor evaluated on
 // each node's label).  Outputs are closest first; counts[i] = results found.
-// trace (optional) receives 4 int64 per query: upper-layer link lists read,
-// upper-layer distances, level-0 expansions, level-0 distances.
+// trace (optional) receives 5 int64 per query: upper-layer link lists read,
+// upper-layer distances, level-0 expansions, level-0 distances, tie events
+// (mode 0 only; see base_layer_reference).
 int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t ef, int mode,
                     const uint8_t* allow, uint64_t* labels, float* dists, int32_t* counts,
                     int64_t* trace, int nthreads) {
@@ -621,10 +666,11 @@ int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t e
             dists[i * k + j] = j < r.size() ? r[j].first : std::numeric_limits<float>::infinity();
         }
         if (trace) {
-            trace[i * 4 + 0] = tr.upper_hops;
-            trace[i * 4 + 1] = tr.upper_dists;
-            trace[i * 4 + 2] = tr.l0_expansions;
-            trace[i * 4 + 3] = tr.l0_dists;
+            trace[i * 5 + 0] = tr.upper_hops;
+            trace[i * 5 + 1] = tr.upper_dists;
+            trace[i * 5 + 2] = tr.l0_expansions;
+            trace[i * 5 + 3] = tr.l0_dists;
+            trace[i * 5 + 4] = tr.ties;
         }
     });
     if (failed) { g_err = "cand error"; return -1; }

@@ -39,9 +39,10 @@ def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.99
     # identical work: upper-layer counters and level-0 expansions
     assert np.array_equal(gt[:, :3].astype(np.int64), ct[:, :3])
     assert np.all(gt[:, 3].astype(np.int64) >= ct[:, 3])
-    # against the reference algorithm (heap tie order)
-    rl, rd, rc = o.search(q, k, ef, mode=O.REFERENCE, allow=allow)
-    same, bad = compare_rows(gl, gd, rl, rd)
+    # against the reference algorithm (heap tie order): identical rows except
+    # where the reference run made a tie decision
+    rl, rd, rc, rt = o.search(q, k, ef, mode=O.REFERENCE, allow=allow, trace=True)
+    same, bad = compare_rows(gl, rl, rt[:, 4])
     assert same >= min_same and not bad, (same, bad[:5])
     return g
 
@@ -82,26 +83,37 @@ def test_parity_filter_and_deletes(tmp_path):
 
 
 def test_golden_fixtures():
+    """Against the reference's own recorded outputs.  Rows may differ only
+    where the reference run made a tie decision (the integer fixture is built
+    to have many); everything is bit-exact against the canonical oracle."""
     g = golden()
     cases = {"hnsw_l2_d16": "l2", "hnsw_ip_d20": "ip", "hnsw_cos_d12": "cosine", "hnsw_l2_d7_int": "l2"}
     for name, space in cases.items():
         q = g[f"{name}/queries"]
-        idx = gpu_index(f"{GOLDEN}/{name}.bin", space, q.shape[1])
+        path = f"{GOLDEN}/{name}.bin"
+        idx = gpu_index(path, space, q.shape[1])
+        o = O.Hnsw(path, space, q.shape[1])
+        even = (o.labels() % 2 == 0).astype(np.uint8)
+        min_same = 0.5 if name.endswith("_int") else 0.999
         for ef in (10, 32, 100):
             idx.set_ef(ef)
             for k in (1, 10):
-                for suffix, filt in (("", None), ("_even", lambda l: l % 2 == 0)):
+                for suffix, filt, allow in (("", None, None), ("_even", lambda l: l % 2 == 0, even)):
                     l, d = idx.knn_query(q, k=k, filter=filt)
-                    same, bad = compare_rows(l, d, g[f"{name}/ef{ef}_k{k}{suffix}/labels"],
-                                             g[f"{name}/ef{ef}_k{k}{suffix}/dists"])
-                    assert not bad and same >= 0.95, (name, ef, k, suffix, same, bad)
+                    cl, cd, _ = o.search(q, k, ef, mode=O.CANONICAL, allow=allow)
+                    assert np.array_equal(l, cl) and np.array_equal(d.view(np.uint32), cd.view(np.uint32))
+                    _, _, _, rt = o.search(q, k, ef, mode=O.REFERENCE, allow=allow, trace=True)
+                    same, bad = compare_rows(l, g[f"{name}/ef{ef}_k{k}{suffix}/labels"], rt[:, 4])
+                    assert not bad and same >= min_same, (name, ef, k, suffix, same, bad)
         for lab in g[f"{name}/deleted"]:
             idx.mark_deleted(int(lab))
+            o.set_deleted(int(lab), True)
         for ef in (10, 32, 100):
             idx.set_ef(ef)
             l, d = idx.knn_query(q, k=10)
-            same, bad = compare_rows(l, d, g[f"{name}/ef{ef}_k10_del/labels"], g[f"{name}/ef{ef}_k10_del/dists"])
-            assert not bad, (name, ef, bad)
+            _, _, _, rt = o.search(q, 10, ef, mode=O.REFERENCE, trace=True)
+            same, bad = compare_rows(l, g[f"{name}/ef{ef}_k10_del/labels"], rt[:, 4])
+            assert not bad and same >= min_same, (name, ef, bad)
             assert not np.isin(l, g[f"{name}/deleted"]).any()
 
 
@@ -178,3 +190,32 @@ def test_large_M_and_k(tmp_path):
     build_hnsw(tmp_path / "m32.bin", x, "l2", M=32, efc=100)
     check_parity(tmp_path / "m32.bin", "l2", q, 100, 150)
     check_parity(tmp_path / "m32.bin", "l2", q, 10, 400)
+
+
+def test_full_size_parity_1m():
+    """The 1M x 128 integer-valued workload (reference-built graph, M=16,
+    efc=200) at the operating points around recall 0.95: >= 99.9% of queries
+    return the reference's labels, and every other query traces to a tie."""
+    import os
+
+    from hnsw_rabitq_b200.datasets import gmm_1m_128
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cache = os.path.join(root, ".cache")
+    os.makedirs(cache, exist_ok=True)
+    path = os.path.join(cache, "gmm_1000000_128_M16_efc200.bin")
+    x, q = gmm_1m_128()
+    if not os.path.exists(path):
+        build_hnsw(path + ".tmp", x, "l2", M=16, efc=200, num_threads=os.cpu_count())
+        os.replace(path + ".tmp", path)
+    del x
+    qs = q[:3000]
+    g = gpu_index(path, "l2", 128)
+    o = O.Hnsw(path, "l2", 128)
+    for ef in (48, 64, 128):
+        g.set_ef(ef)
+        gl, gd = g.knn_query(qs, k=10)
+        cl, cd, _ = o.search(qs, 10, ef, mode=O.CANONICAL)
+        assert np.array_equal(gl, cl) and np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
+        rl, rd, _, rt = o.search(qs, 10, ef, mode=O.REFERENCE, trace=True)
+        same, bad = compare_rows(gl, rl, rt[:, 4])
+        assert same >= 0.999 and not bad, (ef, same, bad[:5])
