@@ -63,6 +63,8 @@ def parse():
     ap.add_argument("--target-recall", type=float, default=0.95)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", action="store_true", help="only run the timed loop (for ncu)")
+    ap.add_argument("--tie-order", default="reference", choices=["reference", "id"],
+                    help="reference: heap replay, results identical to hnswlib; id: ties by internal id")
     return ap.parse_args()
 
 
@@ -232,11 +234,14 @@ def run_ours(args, dist: Dist):
     torch.cuda.set_device(dev)
     x, q = workload(args.n, args.nq)
     path = ensure_index(x, dist)
-    gt = ground_truth(x, q)
+    gt = None if args.profile_steps else ground_truth(x, q)
     idx = Index("l2", 128)
     idx.device = dev
+    idx.tie_order = args.tie_order
     idx.load_index(path)
     info = idx._info()
+    if args.profile_steps and not args.ef:
+        raise SystemExit("--profile-steps needs --ef")
 
     # ---- operating point: smallest ef with recall@10 >= target
     sweep = []
@@ -256,7 +261,7 @@ def run_ours(args, dist: Dist):
             ef_star = EFS[-1]
     idx.set_ef(ef_star)
     lab, _ = idx.knn_query(q, k=10)
-    rec = recall(lab, gt)
+    rec = recall(lab, gt) if gt is not None else None
 
     # ---- device-resident timed loop
     lib = _capi.lib()
@@ -266,8 +271,9 @@ def run_ours(args, dist: Dist):
     dl = torch.empty((nq, k), dtype=torch.int64, device=f"cuda:{dev}")
     dd = torch.empty((nq, k), dtype=torch.float32, device=f"cuda:{dev}")
     dc = torch.empty((nq,), dtype=torch.int32, device=f"cuda:{dev}")
+    tie_flag = _capi.EXACT_TIES if args.tie_order == "reference" else 0
     opts = _capi.SearchOpts()
-    opts.flags = _capi.DEVICE_PTRS
+    opts.flags = _capi.DEVICE_PTRS | tie_flag
     opts.ef = ef_star
     opts.stream = stream.cuda_stream
 
@@ -306,6 +312,7 @@ def run_ours(args, dist: Dist):
     hd = torch.empty((nq, k), dtype=torch.float32).pin_memory()
     hc = torch.empty((nq,), dtype=torch.int32).pin_memory()
     eopts = _capi.SearchOpts()
+    eopts.flags = tie_flag
     eopts.ef = ef_star
 
     def e2e_step():
@@ -343,7 +350,8 @@ def run_ours(args, dist: Dist):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
                                    "HNSW M=16 efc=200, 10,000 queries, k=10",
-                       "method": "plain fp32 beam (exact reference semantics)", "ef": ef_star,
+                       "method": "plain fp32 beam, reference semantics, tie order: " + args.tie_order,
+                       "ef": ef_star,
                        "recall@10": round(rec, 5), "global_batch": nq, "parallelism": f"replicas x{dist.world}",
                        "l2_flush": "not needed: index data 640 MB > 126 MB L2",
                        "index_device_bytes": info.device_bytes},

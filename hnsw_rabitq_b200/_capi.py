@@ -18,6 +18,7 @@ ERR_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_LABEL, ERR_STATE, ERR_KERN
 SPACE_L2, SPACE_IP, SPACE_COSINE = 0, 1, 2
 DEVICE_PTRS = 0x1
 TRACE = 0x2
+EXACT_TIES = 0x4
 STATUS_TIMEOUT = 0x1
 STATUS_OVERFLOW = 0x2
 

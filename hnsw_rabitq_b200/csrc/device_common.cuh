@@ -244,6 +244,63 @@ __device__ __forceinline__ float dist_ip(const float* q, const float* x, int dim
     return __fsub_rn(1.0f, ip_scalar(q, x, dim));
 }
 
+// The dim % 16 == 0 distance split over a group of 4 lanes (a = lane & 3):
+// lane a keeps the reference's accumulators 4a .. 4a+3 (one float4 of each
+// 16-float chunk), so one LDS.128 per chunk per lane feeds 8 vectors per warp
+// instruction.  The cross-lane reduction reproduces the reference order
+// exactly: L2 sums the 16 accumulators left to right (space_l2.h:49-51), IP
+// applies GCC's _mm512_reduce_add_ps tree then 1 - x.  All 32 lanes must call
+// it (it shuffles); the result is valid in lanes with a == 0.
+template <int SPACE>
+__device__ __forceinline__ float group4_dist16(const float* __restrict__ q, const float* __restrict__ x, int n16,
+                                               int a) {
+    const float4* q4 = reinterpret_cast<const float4*>(q);
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+    float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+    for (int c = 0; c < n16; c++) {
+        float4 qv = q4[4 * c + a], xv = x4[4 * c + a];
+        if (SPACE == 0) {
+            float t0 = __fsub_rn(qv.x, xv.x), t1 = __fsub_rn(qv.y, xv.y), t2 = __fsub_rn(qv.z, xv.z),
+                  t3 = __fsub_rn(qv.w, xv.w);
+            c0 = __fmaf_rn(t0, t0, c0);
+            c1 = __fmaf_rn(t1, t1, c1);
+            c2 = __fmaf_rn(t2, t2, c2);
+            c3 = __fmaf_rn(t3, t3, c3);
+        } else {
+            c0 = __fmaf_rn(qv.x, xv.x, c0);
+            c1 = __fmaf_rn(qv.y, xv.y, c1);
+            c2 = __fmaf_rn(qv.z, xv.z, c2);
+            c3 = __fmaf_rn(qv.w, xv.w, c3);
+        }
+    }
+    if (SPACE == 0) {
+        // accumulators 4..15 from the three lanes to the right
+        float b0 = __shfl_down_sync(FULL, c0, 1), b1 = __shfl_down_sync(FULL, c1, 1);
+        float b2 = __shfl_down_sync(FULL, c2, 1), b3 = __shfl_down_sync(FULL, c3, 1);
+        float e0 = __shfl_down_sync(FULL, c0, 2), e1 = __shfl_down_sync(FULL, c1, 2);
+        float e2 = __shfl_down_sync(FULL, c2, 2), e3 = __shfl_down_sync(FULL, c3, 2);
+        float f0 = __shfl_down_sync(FULL, c0, 3), f1 = __shfl_down_sync(FULL, c1, 3);
+        float f2 = __shfl_down_sync(FULL, c2, 3), f3 = __shfl_down_sync(FULL, c3, 3);
+        float r = __fadd_rn(__fadd_rn(__fadd_rn(c0, c1), c2), c3);
+        r = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(r, b0), b1), b2), b3);
+        r = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(r, e0), e1), e2), e3);
+        r = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(r, f0), f1), f2), f3);
+        return r;
+    } else {
+        // T3[i] = a[i+8] + a[i]: lanes 0,1 pair with lanes 2,3
+        float u0 = __fadd_rn(__shfl_down_sync(FULL, c0, 2), c0);
+        float u1 = __fadd_rn(__shfl_down_sync(FULL, c1, 2), c1);
+        float u2 = __fadd_rn(__shfl_down_sync(FULL, c2, 2), c2);
+        float u3 = __fadd_rn(__shfl_down_sync(FULL, c3, 2), c3);
+        // T6[i] = T3[i+4] + T3[i]: lane 0 pairs with lane 1
+        float v0 = __fadd_rn(__shfl_down_sync(FULL, u0, 1), u0);
+        float v1 = __fadd_rn(__shfl_down_sync(FULL, u1, 1), u1);
+        float v2 = __fadd_rn(__shfl_down_sync(FULL, u2, 1), u2);
+        float v3 = __fadd_rn(__shfl_down_sync(FULL, u3, 1), u3);
+        return __fsub_rn(1.0f, __fadd_rn(__fadd_rn(v0, v2), __fadd_rn(v1, v3)));
+    }
+}
+
 template <int SPACE>
 __device__ __forceinline__ float distance(const float* q, const float* x, int dim) {
     if (SPACE == 0) return dist_l2(q, x, dim);

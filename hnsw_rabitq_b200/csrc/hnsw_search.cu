@@ -37,6 +37,7 @@
 
 #include "device_common.cuh"
 #include "hnsw_search.h"
+#include "ref_heap.h"
 
 namespace hnswgpu {
 
@@ -49,6 +50,10 @@ struct WarpSmem {
     uint64_t* pool;
     uint64_t* extra;
     uint32_t* vis;
+    uint64_t* topheap;   // tie-exact mode: replay of top_candidates
+    uint64_t* candheap;  // tie-exact mode: replay of candidate_set
+    uint64_t* accbuf;    // tie-exact mode: accepted keys of one chunk, link order
+    uint64_t* evbuf;     // tie-exact mode: keys evicted from top_candidates
 };
 
 __device__ __forceinline__ bool is_allowed(const SearchParams& p, uint32_t id) {
@@ -80,6 +85,50 @@ __device__ __forceinline__ int upper_bound_hi(const uint64_t* a, int n, uint32_t
         else hi = mid;
     }
     return lo;
+}
+
+// Insertion position of `key` (distance key dk, node id) in the sorted array
+// given cnt = upper_bound_hi(a, n, dk), walking back over the (rare) entries
+// that tie in distance.  Sets dup when the key is already present.
+__device__ __forceinline__ int insert_pos(const uint64_t* a, int cnt, uint32_t dk, uint32_t id, bool& dup) {
+    int pos = cnt;
+    while (pos > 0) {
+        uint64_t e = a[pos - 1];
+        if (khi(e) != dk) break;
+        uint32_t eid = kid(e);
+        if (eid == id) {
+            dup = true;
+            break;
+        }
+        if (eid < id) break;
+        pos--;
+    }
+    return pos;
+}
+
+// Remove the nev (<= 32) distinct keys ev[0..nev) (all present) from the
+// sorted array a[0, size), keeping the order of the rest.
+__device__ __forceinline__ void remove_keys(uint64_t* a, int& size, const uint64_t* ev, int nev, int lane) {
+    int myidx = lane < nev ? lower_bound_key(a, size, ev[lane] & KEY_MASK) : 0x7fffffff;
+    int minidx = myidx;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) minidx = min(minidx, __shfl_xor_sync(FULL, minidx, o));
+    for (int base = minidx; base < size; base += 32) {
+        int i = base + lane;
+        bool have = i < size;
+        uint64_t e = have ? a[i] : 0;
+        int before = 0;
+        bool gone = false;
+        for (int t = 0; t < nev; t++) {
+            int it = __shfl_sync(FULL, myidx, t);
+            before += (it < i);
+            gone |= (it == i);
+        }
+        __syncwarp();
+        if (have && !gone) a[i - before] = e;
+        __syncwarp();
+    }
+    size -= nev;
 }
 
 // First unexpanded entry at index >= hint, or -1.  Updates hint.
@@ -166,22 +215,36 @@ struct Counters {
 
 // Distances of `cnt` (<= 32) nodes held by lanes [0, cnt) (id per lane);
 // result returned in the owning lane.  False on a wait timeout.
-template <int SPACE>
+// Rows are staged `stage_slots` at a time.  For dim % 16 == 0 each group of
+// 4 lanes evaluates one staged row (8 rows per pass, group4_dist16); other
+// dimensions use one lane per row with the scalar-order routine.
+template <int SPACE, bool FAST16>
 __device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t id,
                                                int cnt, int lane, float& d) {
     d = __int_as_float(0x7f800000);
     for (int s0 = 0; s0 < cnt; s0 += (int)p.stage_slots) {
-        int n = min((int)p.stage_slots, cnt - s0);
-        bool mine = lane >= s0 && lane < s0 + n;
+        const int n = min((int)p.stage_slots, cnt - s0);
+        const bool mine = lane >= s0 && lane < s0 + n;
         if (!stage_rows(p, s, phase, mine, id, lane - s0, n, lane)) return false;
-        float dt = lane < n ? stage_dist<SPACE>(p, s, lane) : 0.f;
-        float got = __shfl_sync(FULL, dt, (lane - s0) & 31);
-        if (mine) d = got;
+        if (FAST16) {
+            const int a = lane & 3;
+            for (int g = 0; g < n; g += 8) {
+                const int v = min(g + (lane >> 2), n - 1);
+                float r = group4_dist16<SPACE>(s.q, s.stage + (size_t)v * p.stage_stride, (int)(p.dim >> 4), a);
+                const int rel = lane - s0 - g;  // this lane's row within the pass
+                float got = __shfl_sync(FULL, r, (rel & 7) << 2);
+                if (rel >= 0 && rel < 8 && mine) d = got;
+            }
+        } else {
+            float dt = lane < n ? stage_dist<SPACE>(p, s, lane) : 0.f;
+            float got = __shfl_sync(FULL, dt, (lane - s0) & 31);
+            if (mine) d = got;
+        }
     }
     return true;
 }
 
-template <int SPACE>
+template <int SPACE, bool FAST16, bool EXACT>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
                            Counters& ct) {
     const int dim = (int)p.dim;
@@ -204,7 +267,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     // ---- upper-layer greedy descent (hnswalg.h:1274-1302)
     uint32_t cur = p.ep;
     float curd;
-    if (!lane_distances<SPACE>(p, s, phase, cur, 1, lane, curd)) return false;
+    if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, curd)) return false;
     curd = __shfl_sync(FULL, curd, 0);
     ct.upper_dists += 1;
     const uint32_t up_stride = p.maxM + 1;
@@ -220,7 +283,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
                 int n = min(32, cnt - c0);
                 uint32_t id = lane < n ? row[1 + c0 + lane] : INVALID_ID;
                 float d;
-                if (!lane_distances<SPACE>(p, s, phase, id, n, lane, d)) return false;
+                if (!lane_distances<SPACE, FAST16>(p, s, phase, id, n, lane, d)) return false;
                 float m = lane < n ? d : __int_as_float(0x7f800000);
 #pragma unroll
                 for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, o));
@@ -245,22 +308,56 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     // (hnswalg.h:336-337) and never evaluated, so the exact-key lookup cannot
     // recognise it when the visited cache misses on it later: skip it by id.
     uint32_t skip_id = INVALID_ID;
+    const int pcap = (int)p.pool_cap;  // ef, or ef + 32 in tie-exact mode
+    int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
+    const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
     if (bare || is_allowed(p, cur)) {
         float d0;
-        if (!lane_distances<SPACE>(p, s, phase, cur, 1, lane, d0)) return false;
+        if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0)) return false;
         d0 = __shfl_sync(FULL, d0, 0);
         ct.l0_dists += 1;
         if (lane == 0) s.pool[0] = mkkey(d0, cur);
         psize = 1;
+        if (EXACT) {
+            if (lane == 0) {
+                s.topheap[0] = mkkey(d0, cur);
+                s.candheap[0] = mkkey(d0, cur);
+            }
+            tsz = csz = 1;
+        }
     } else {
-        if (lane == 0) s.extra[0] = mkkey(__int_as_float(0x7f7fffff), cur);
-        xsize = 1;
+        if (EXACT) {
+            if (lane == 0) s.candheap[0] = sentinel;
+            csz = 1;
+        } else {
+            if (lane == 0) s.extra[0] = sentinel;
+            xsize = 1;
+        }
         skip_id = cur;
     }
     if (lane == 0) s.vis[vis_slot(cur, p.log2_vis)] = cur;
     __syncwarp();
 
     while (true) {
+      uint32_t cid;
+      if (EXACT) {
+        // ---- next candidate: the reference's candidate_set.top() (hnswalg.h:343-359)
+        if (csz == 0) break;
+        const uint64_t c = s.candheap[0];
+        const uint32_t lbk = psize > 0 ? khi(s.pool[psize - 1]) : fkey(__int_as_float(0x7f7fffff));
+        const bool stop = bare ? (khi(c) > lbk) : (khi(c) > lbk && psize == (int)ef);
+        if (stop) break;
+        __syncwarp();
+        if (lane == 0) {
+            int n = csz;
+            ref_heap_pop(s.candheap, n, CandLess());
+            if (n > 0) prefetch_l2(p.links0 + (size_t)kid(s.candheap[0]) * p.maxM0);
+        }
+        csz--;
+        __syncwarp();
+        cid = kid(c);
+        ct.l0_exp += 1;
+      } else {
         int ip = find_unexpanded(s.pool, psize, hint_p, lane);
         int ix = bare ? -1 : find_unexpanded(s.extra, xsize, hint_x, lane);
         uint64_t kp = ip >= 0 ? (s.pool[ip] & KEY_MASK) : ~0ull;
@@ -275,8 +372,16 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             else s.pool[ip] = ck | EXP_BIT;
         }
         __syncwarp();
-        const uint32_t cid = kid(ck);
+        cid = kid(ck);
         ct.l0_exp += 1;
+        {
+            // the next expansion is most often the next unexpanded pool entry:
+            // start pulling its link row into L2 now
+            int h2 = hint_p;
+            int nx = find_unexpanded(s.pool, psize, h2, lane);
+            if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
+        }
+      }
         if (ct.l0_exp > p.max_expansions) {
             // only reachable after a candidate-list overflow (nodes dropped
             // from the list can be re-admitted); stop and flag the query
@@ -305,7 +410,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             int src = __fns(nmask, 0, lane + 1);  // lane holding the (lane)-th fresh id
             uint32_t cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
             float dc;
-            if (!lane_distances<SPACE>(p, s, phase, cid2, nnew, lane, dc)) return false;
+            if (!lane_distances<SPACE, FAST16>(p, s, phase, cid2, nnew, lane, dc)) return false;
             float d = __shfl_sync(FULL, dc, ci & 31);
             // ---- acceptance (closed form of the sequential test)
             uint32_t dk = fkey(d);
@@ -315,13 +420,11 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             uint64_t key = ((uint64_t)dk << 32) | id;
             int posP = 0, posX = 0, cntP = 0;
             if (live) {
-                posP = lower_bound_key(s.pool, psize, key);
-                if (posP < psize && (s.pool[posP] & KEY_MASK) == key) live = false;
-                if (live && !bare) {
-                    posX = lower_bound_key(s.extra, xsize, key);
-                    if (posX < xsize && (s.extra[posX] & KEY_MASK) == key) live = false;
-                }
-                if (live) cntP = upper_bound_hi(s.pool, psize, dk);
+                bool dup = false;
+                cntP = upper_bound_hi(s.pool, psize, dk);
+                posP = insert_pos(s.pool, cntP, dk, id, dup);
+                if (!bare && !dup) posX = insert_pos(s.extra, upper_bound_hi(s.extra, xsize, dk), dk, id, dup);
+                if (dup) live = false;
             }
             bool allowed = bare || (live && is_allowed(p, id));
             unsigned amask = __ballot_sync(FULL, live && allowed);
@@ -334,10 +437,44 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             bool accept = live && (uint32_t)(cntP + cntN) < ef;
             unsigned pmask = __ballot_sync(FULL, accept && allowed);
             unsigned xmask = bare ? 0u : __ballot_sync(FULL, accept && !allowed);
+            int nev = 0;
+            if (EXACT && (pmask | xmask)) {
+                // replay the reference's heap operations for the accepted
+                // neighbours in link order (hnswalg.h:398-429): every one
+                // enters candidate_set; allowed ones enter top_candidates,
+                // which then drops its top while it holds more than ef.
+                const unsigned amask2 = pmask | xmask;
+                if (accept) s.accbuf[__popc(amask2 & lanemask_lt())] = key | (allowed ? EXP_BIT : 0u);
+                __syncwarp();
+                const int na = __popc(amask2);
+                uint32_t ovf = 0;
+                if (lane == 0) {
+                    int cn = csz, tn = tsz;
+                    for (int t = 0; t < na; t++) {
+                        uint64_t e = s.accbuf[t];
+                        const bool al = ((uint32_t)e & EXP_BIT) != 0;
+                        e &= KEY_MASK;
+                        if (cn < (int)p.cand_cap) ref_heap_push(s.candheap, cn, e, CandLess());
+                        else ovf = 1;
+                        if (al) {
+                            ref_heap_push(s.topheap, tn, e, TopLess());
+                            if (tn > (int)ef) s.evbuf[nev++] = ref_heap_pop(s.topheap, tn, TopLess());
+                        }
+                    }
+                    csz = cn;
+                    tsz = tn;
+                }
+                csz = __shfl_sync(FULL, csz, 0);
+                tsz = __shfl_sync(FULL, tsz, 0);
+                nev = __shfl_sync(FULL, nev, 0);
+                if (__shfl_sync(FULL, ovf, 0)) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+                __syncwarp();
+            }
             if (pmask) {
-                int m = merge_sorted(s.pool, psize, (int)ef, pmask, key, posP, lane);
+                int m = merge_sorted(s.pool, psize, pcap, pmask, key, posP, lane);
                 hint_p = min(hint_p, m);
             }
+            if (EXACT && nev) remove_keys(s.pool, psize, s.evbuf, nev, lane);
             if (xmask) {
                 if (xsize + __popc(xmask) > xcap) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
                 int m = merge_sorted(s.extra, xsize, xcap, xmask, key, posX, lane);
@@ -351,8 +488,34 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         }
     }
 
-    // ---- results: the k smallest pool entries, ordered by (distance, label)
     const uint32_t k = p.k;
+    if (EXACT) {
+        // the reference pops top_candidates down to k (hnswalg.h:1314-1316);
+        // keep in the pool exactly the entries left in the heap
+        int tn = tsz;
+        if (lane == 0)
+            while (tn > (int)k) ref_heap_pop(s.topheap, tn, TopLess());
+        tn = __shfl_sync(FULL, tn, 0);
+        __syncwarp();
+        for (int t = lane; t < tn; t += 32) {
+            int pos = lower_bound_key(s.pool, psize, s.topheap[t] & KEY_MASK);
+            s.pool[pos] |= EXP_BIT;
+        }
+        __syncwarp();
+        int out = 0;
+        for (int base = 0; base < psize; base += 32) {
+            int i = base + lane;
+            bool keep = i < psize && ((uint32_t)s.pool[i] & EXP_BIT);
+            unsigned m = __ballot_sync(FULL, keep);
+            uint64_t e = keep ? (s.pool[i] & KEY_MASK) : 0;
+            __syncwarp();
+            if (keep) s.pool[out + __popc(m & lanemask_lt())] = e;
+            out += __popc(m);
+            __syncwarp();
+        }
+        psize = out;
+    }
+    // ---- results: the k smallest pool entries, ordered by (distance, label)
     const int kk = min((int)k, psize);
     uint64_t* olab = p.out_labels + (size_t)qi * k;
     float* odist = p.out_dists + (size_t)qi * k;
@@ -381,8 +544,8 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     return true;
 }
 
-template <int SPACE>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) hnsw_search_kernel(SearchParams p) {
+template <int SPACE, bool FAST16, bool EXACT>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base = smem + (size_t)warp * p.warp_smem;
@@ -393,6 +556,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) hnsw_search_kernel(Search
     s.pool = reinterpret_cast<uint64_t*>(base + p.off_pool);
     s.extra = reinterpret_cast<uint64_t*>(base + p.off_extra);
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
+    s.topheap = reinterpret_cast<uint64_t*>(base + p.off_top);
+    s.candheap = reinterpret_cast<uint64_t*>(base + p.off_cand);
+    s.accbuf = reinterpret_cast<uint64_t*>(base + p.off_acc);
+    s.evbuf = reinterpret_cast<uint64_t*>(base + p.off_ev);
     if (lane == 0) mbar_init(s.bar, 1);
     fence_mbar_init();
     __syncwarp();
@@ -403,11 +570,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) hnsw_search_kernel(Search
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE>(p, s, phase, qi, lane, ct)) {
+        if (!search_one<SPACE, FAST16, EXACT>(p, s, phase, qi, lane, ct)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
-            return;
+            break;
         }
         if (p.trace && lane == 0) {
             uint32_t* t = p.trace + (size_t)qi * 4;
@@ -415,6 +582,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32) hnsw_search_kernel(Search
             t[1] = ct.upper_dists;
             t[2] = ct.l0_exp;
             t[3] = ct.l0_dists;
+        }
+    }
+    // The last block to finish re-arms this launch's work counter, so the
+    // next launch that draws the same counter slot starts from zero.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(p.done_counter, 1u) == gridDim.x - 1) {
+            *p.work_counter = 0;
+            *p.done_counter = 0;
+            __threadfence();
         }
     }
 }
@@ -430,7 +608,15 @@ size_t warp_smem_layout(SearchParams& p) {
     off += (size_t)p.stage_slots * p.stage_stride * 4;
     off = (off + 7) & ~(size_t)7;
     p.off_pool = (uint32_t)off;
-    off += (size_t)p.ef * 8;
+    off += (size_t)p.pool_cap * 8;
+    p.off_top = (uint32_t)off;
+    off += p.exact ? ((size_t)p.ef + 1) * 8 : 0;
+    p.off_cand = (uint32_t)off;
+    off += p.exact ? (size_t)p.cand_cap * 8 : 0;
+    p.off_acc = (uint32_t)off;
+    off += p.exact ? 32 * 8 : 0;
+    p.off_ev = (uint32_t)off;
+    off += p.exact ? 32 * 8 : 0;
     p.off_extra = (uint32_t)off;
     off += (size_t)p.extra_cap * 8;
     off = (off + 15) & ~(size_t)15;
@@ -441,25 +627,48 @@ size_t warp_smem_layout(SearchParams& p) {
     return off;
 }
 
-cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
-    size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
-    const void* fn = space == 0 ? (const void*)hnsw_search_kernel<0> : (const void*)hnsw_search_kernel<1>;
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWarpsPerBlock * 32, smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+namespace {
+template <int SPACE, bool FAST16, bool EXACT>
+cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    // per-instantiation cache of the opt-in shared-memory size and occupancy
+    static int attr_smem = -1;
+    static size_t occ_smem = 0;
+    static int occ_per_sm = 0;
+    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT>;
+    const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
+    if ((int)smem > attr_smem) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_smem = (int)smem;
+    }
+    if (smem != occ_smem) {
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, fn, kWarpsPerBlock * 32, smem);
+        if (e != cudaSuccess) return e;
+        occ_smem = smem;
+    }
+    if (occ_per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t need = (p.nq + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    uint64_t blocks = (uint64_t)per_sm * (uint64_t)num_sms;
+    uint64_t blocks = (uint64_t)occ_per_sm * (uint64_t)num_sms;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    if (space == 0)
-        hnsw_search_kernel<0><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
-    else
-        hnsw_search_kernel<1><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_search_kernel<SPACE, FAST16, EXACT><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     return cudaGetLastError();
+}
+
+template <int SPACE, bool EXACT>
+cudaError_t launch_s(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    return p.fast16 ? launch_t<SPACE, true, EXACT>(p, num_sms, stream, blocks_out)
+                    : launch_t<SPACE, false, EXACT>(p, num_sms, stream, blocks_out);
+}
+}  // namespace
+
+cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (space == 0)
+        return p.exact ? launch_s<0, true>(p, num_sms, stream, blocks_out)
+                       : launch_s<0, false>(p, num_sms, stream, blocks_out);
+    return p.exact ? launch_s<1, true>(p, num_sms, stream, blocks_out)
+                   : launch_s<1, false>(p, num_sms, stream, blocks_out);
 }
 
 }  // namespace hnswgpu

@@ -28,16 +28,21 @@ struct SearchParams {
     uint32_t nq, q_stride, k, ef;
     uint32_t bare, normalize;
     uint32_t max_expansions;      // safety bound on level-0 expansions per query
+    uint32_t fast16;              // dim % 16 == 0: 4-lanes-per-row distance path
+    uint32_t exact;               // replay the reference's heaps (tie order exact)
+    uint32_t pool_cap;            // ef (canonical) or ef + 32 (tie-exact)
+    uint32_t cand_cap;            // tie-exact: candidate heap capacity
     // outputs
     uint64_t* out_labels;
     float* out_dists;
     int32_t* out_counts;
     uint32_t* trace;
-    uint32_t* work_counter;
+    uint32_t* work_counter;       // zero at launch; reset to zero by the last block
+    uint32_t* done_counter;       // blocks finished (same slot discipline)
     uint32_t* status;
     // per-warp shared memory layout
     uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
-    uint32_t off_query, off_stage, off_pool, off_extra, off_vis, warp_smem;
+    uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;
 };
 
 // Fills the off_* fields and warp_smem from the sizes; returns warp_smem.

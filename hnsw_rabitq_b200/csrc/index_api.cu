@@ -120,7 +120,7 @@ void init_common(hnswgpu_index* h, int device) {
     cuda_check(cudaSetDevice(device), "cudaSetDevice");
     cuda_check(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     cuda_check(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    h->counters.alloc(256);
+    h->counters.alloc(512);  // 256 (work, done) pairs, used round robin
     cuda_check(cudaMemset(h->counters.p, 0, h->counters.bytes()), "cudaMemset");
     h->status.alloc(1);
     cuda_check(cudaMemset(h->status.p, 0, 4), "cudaMemset");
@@ -180,7 +180,7 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
         throw ApiError(HNSWGPU_ERR_FORMAT,
                        "index layout does not match dim=" + std::to_string(dim) + " (" + corrupt + ")");
     if (maxM0 == 0 || maxM0 > 4096 || maxM > 4096) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "unsupported M");
-    if (cur > 0xfffffffeull) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "more than 2^32-2 elements");
+    if (cur > 0x7fffffffull) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "more than 2^31-1 elements");
     if (cur > 0 && (ep >= cur || maxlevel < 0)) throw ApiError(HNSWGPU_ERR_FORMAT, corrupt);
 
     h->space = space;
@@ -387,7 +387,7 @@ int guarded(F fn) {
 
 // One HNSW search launch on device buffers.
 void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
-              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st) {
+              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
     hnswgpu::SearchParams p{};
     p.vecs = h->vecs.p;
     p.links0 = h->links0.p;
@@ -417,10 +417,18 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     p.out_counts = dc;
     p.trace = dtrace;
     p.status = h->status.p;
-    p.stage_stride = h->row_floats + 4;
-    uint32_t slots = (uint32_t)((17u * 1024u) / (p.stage_stride * 4));
-    p.stage_slots = std::max(1u, std::min(32u, slots));
+    // Staging rows: the 4-lanes-per-row path reads 8 rows per LDS.128 pass, a
+    // row pad of 16 floats puts consecutive rows half a bank cycle apart
+    // (conflict-free quarter warps); the one-lane-per-row path wants 4.
+    p.fast16 = (h->dim % 16 == 0) ? 1u : 0u;
+    p.stage_stride = h->row_floats + (p.fast16 ? 16u : 4u);
+    uint32_t slots = (uint32_t)((9u * 1024u + 512u) / (p.stage_stride * 4));
+    p.stage_slots = std::max(1u, std::min(p.fast16 ? 16u : 32u, slots));
     p.extra_cap = p.bare ? 0u : std::max<uint32_t>(128u, 4u * p.ef);
+    p.exact = exact ? 1u : 0u;
+    p.pool_cap = exact ? p.ef + 32u : p.ef;
+    // the reference's candidate heap is never pruned; it peaks near 8 x ef
+    p.cand_cap = exact ? std::max<uint32_t>(256u, 10u * p.ef) : 0u;
     p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
     size_t ws = hnswgpu::warp_smem_layout(p);
     int max_optin = 0;
@@ -429,17 +437,21 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
         p.log2_vis--;
         ws = hnswgpu::warp_smem_layout(p);
     }
+    while (exact && ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin && p.cand_cap > 4u * p.ef) {
+        p.cand_cap -= p.ef;
+        ws = hnswgpu::warp_smem_layout(p);
+    }
     if (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
-    uint32_t slot = h->next_counter++ % (uint32_t)h->counters.n;
-    p.work_counter = h->counters.p + slot;
-    cuda_check(cudaMemsetAsync(p.work_counter, 0, 4, st), "cudaMemsetAsync");
+    uint32_t slot = h->next_counter++ % (uint32_t)(h->counters.n / 2);
+    p.work_counter = h->counters.p + 2 * slot;
+    p.done_counter = h->counters.p + 2 * slot + 1;
     cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
                "hnsw_search launch");
 }
 
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
-                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st) {
+                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
     if (h->is_bf) {
         hnswgpu::BfParams b{};
         b.vecs = h->vecs.p;
@@ -459,7 +471,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
         cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
                    "bf_search launch");
     } else {
-        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st);
+        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact);
     }
 }
 
@@ -590,6 +602,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         if (opts) o = *opts;
         const bool dev = (o.flags & HNSWGPU_DEVICE_PTRS) != 0;
         const bool want_trace = (o.flags & HNSWGPU_TRACE) && o.trace;
+        const bool exact = (o.flags & HNSWGPU_EXACT_TIES) != 0;
         const uint64_t ef = o.ef ? o.ef : h->ef;
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
         std::lock_guard<std::mutex> g(h->mu);
@@ -612,7 +625,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         }
         if (dev) {
             run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
-                       want_trace ? o.trace : nullptr, st);
+                       want_trace ? o.trace : nullptr, st, exact);
             return HNSWGPU_OK;
         }
         // host pointers: stage through the index's device I/O buffer
@@ -633,7 +646,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             dallow = h->allow.p;
         }
         cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st);
+        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact);
         cuda_check(cudaMemcpyAsync(out_labels, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");

@@ -100,7 +100,7 @@ class _GpuIndex:
         self._filter_cache = (filter, mask)
         return mask
 
-    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False):
+    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False, exact_ties: bool = False):
         self._require()
         q = _input_rows(data)
         if q.shape[1] != self.dim:
@@ -114,6 +114,8 @@ class _GpuIndex:
         counts = np.empty(nq, np.int32)
         opts = _capi.SearchOpts()
         opts.ef = int(ef)
+        if exact_ties:
+            opts.flags |= _capi.EXACT_TIES
         mask = self._allow_mask(filter)
         opts.allow = mask.ctypes.data if mask is not None else None
         tr = None
@@ -160,6 +162,10 @@ class Index(_GpuIndex):
     def __init__(self, space: str, dim: int):
         super().__init__(space, dim)
         self._default_ef = 10
+        # "reference": equal distances resolve exactly as hnswlib's heaps do
+        # (results identical to searchKnn); "id": ties break by internal id
+        # (identical except where distances tie exactly; faster).
+        self.tie_order = "reference"
 
     def __repr__(self):
         return f"<hnsw_rabitq_b200.Index(space='{self.space}', dim={self.dim})>"
@@ -222,17 +228,18 @@ class Index(_GpuIndex):
         """(labels uint64 [N, k], distances float32 [N, k]), closest first
         (bindings.cpp:612-697).  Raises RuntimeError when a query has fewer
         than k results, with the reference's message."""
-        labels, dists, counts, _ = self._search(data, k, filter)
+        labels, dists, counts, _ = self._search(data, k, filter, exact_ties=self.tie_order == "reference")
         if counts.size and counts.min() < k:
             raise RuntimeError(
                 "Cannot return the results in a contiguous 2D array. Probably ef or M is too small")
         return labels, dists
 
-    def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0):
+    def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0, tie_order: Optional[str] = None):
         """knn_query plus per-query work counters [upper link lists read,
         upper distances, level-0 expansions, level-0 distances] and counts;
         no exception for short results."""
-        return self._search(data, k, filter, ef=ef, trace=True)
+        order = tie_order or self.tie_order
+        return self._search(data, k, filter, ef=ef, trace=True, exact_ties=order == "reference")
 
 
 class BFIndex(_GpuIndex):

@@ -54,6 +54,10 @@ extern "C" {
                                      it they are host pointers and the call
                                      copies, launches and synchronises.         */
 #define HNSWGPU_TRACE 0x2u        /* write per-query work counters to `trace`   */
+#define HNSWGPU_EXACT_TIES 0x4u   /* HNSW: replay the reference's heap order so
+                                     that exact distance ties resolve as in
+                                     hnswlib (results identical to searchKnn);
+                                     without it ties break by internal id.     */
 
 /* kernel status bits (hnswgpu_search_opts.status / hnswgpu_get_status) */
 #define HNSWGPU_STATUS_TIMEOUT 0x1u   /* a bounded wait gave up; results invalid   */

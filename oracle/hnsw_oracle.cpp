@@ -259,7 +259,7 @@ Hnsw* load_hnsw(const char* path, int space, uint64_t dim) {
 }
 
 struct Trace {
-    int64_t upper_hops = 0, upper_dists = 0, l0_expansions = 0, l0_dists = 0, ties = 0;
+    int64_t upper_hops = 0, upper_dists = 0, l0_expansions = 0, l0_dists = 0, ties = 0, max_cand = 0;
 };
 
 // Upper-layer greedy descent (hnswalg.h:1274-1302).  Shared by both modes.
@@ -324,6 +324,7 @@ std::vector<std::pair<float, uint32_t>> base_layer_reference(const Hnsw& h, uint
     auto push = [&](std::vector<P>& v, P e) {
         v.push_back(e);
         std::push_heap(v.begin(), v.end(), cmp);
+        if (&v == &cand && (int64_t)v.size() > tr.max_cand) tr.max_cand = (int64_t)v.size();
     };
     auto pop = [&](std::vector<P>& v) {
         if (root_tied(v)) tr.ties++;
@@ -638,9 +639,9 @@ int orc_hnsw_set_deleted(void* p, uint64_t label, int flag) {
 // Batched searchKnn.  mode 0 = reference heaps, 1 = canonical pool.
 // allow: optional per-internal-id byte mask (the filter functor evaluated on
 // each node's label).  Outputs are closest first; counts[i] = results found.
-// trace (optional) receives 5 int64 per query: upper-layer link lists read,
+// trace (optional) receives 6 int64 per query: upper-layer link lists read,
 // upper-layer distances, level-0 expansions, level-0 distances, tie events
-// (mode 0 only; see base_layer_reference).
+// (mode 0 only; see base_layer_reference), largest candidate-heap size (mode 0).
 int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t ef, int mode,
                     const uint8_t* allow, uint64_t* labels, float* dists, int32_t* counts,
                     int64_t* trace, int nthreads) {
@@ -666,11 +667,12 @@ int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t e
             dists[i * k + j] = j < r.size() ? r[j].first : std::numeric_limits<float>::infinity();
         }
         if (trace) {
-            trace[i * 5 + 0] = tr.upper_hops;
-            trace[i * 5 + 1] = tr.upper_dists;
-            trace[i * 5 + 2] = tr.l0_expansions;
-            trace[i * 5 + 3] = tr.l0_dists;
-            trace[i * 5 + 4] = tr.ties;
+            trace[i * 6 + 0] = tr.upper_hops;
+            trace[i * 6 + 1] = tr.upper_dists;
+            trace[i * 6 + 2] = tr.l0_expansions;
+            trace[i * 6 + 3] = tr.l0_dists;
+            trace[i * 6 + 4] = tr.ties;
+            trace[i * 6 + 5] = tr.max_cand;
         }
     });
     if (failed) { g_err = "cand error"; return -1; }

@@ -18,6 +18,12 @@ def gpu_index(path, space, dim):
 
 
 def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.999):
+    """Both tie orders through the C ABI:
+    * tie_order="reference" (heap replay): labels, distances and counts
+      identical to the reference algorithm, same number of expansions;
+    * tie_order="id": bit-identical to the oracle's canonical mode, and equal
+      to the reference on every query whose reference run made no tie
+      decision."""
     dim = q.shape[1]
     g = gpu_index(path, space, dim)
     o = O.Hnsw(str(path), space, dim)
@@ -29,19 +35,23 @@ def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.99
     if allow_fn is not None:
         allow = np.array([1 if allow_fn(int(l)) else 0 for l in o.labels()], np.uint8)
     assert g.get_status() == 0
-    gl, gd, gc, gt = g.knn_query_traced(q, k, filter=allow_fn)
+    rl, rd, rc, rt = o.search(q, k, ef, mode=O.REFERENCE, allow=allow, trace=True)
+    # tie-exact mode == the reference
+    xl, xd, xc, xt = g.knn_query_traced(q, k, filter=allow_fn, tie_order="reference")
+    assert g.get_status() == 0, "candidate heap overflow or timeout"
+    assert np.array_equal(xc, rc)
+    assert np.array_equal(xl, rl), np.nonzero(~np.all(xl == rl, axis=1))[0][:10]
+    assert np.array_equal(xd.view(np.uint32), rd.view(np.uint32))
+    assert np.array_equal(xt[:, :3].astype(np.int64), rt[:, :3])
+    # id tie order == the canonical oracle
+    gl, gd, gc, gt = g.knn_query_traced(q, k, filter=allow_fn, tie_order="id")
     assert g.get_status() == 0, "candidate list overflow or timeout"
     cl, cd, cc, ct = o.search(q, k, ef, mode=O.CANONICAL, allow=allow, trace=True)
-    # bit-exact against the canonical oracle
     assert np.array_equal(gc, cc)
     assert np.array_equal(gl, cl), np.nonzero(~np.all(gl == cl, axis=1))[0][:10]
     assert np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
-    # identical work: upper-layer counters and level-0 expansions
     assert np.array_equal(gt[:, :3].astype(np.int64), ct[:, :3])
     assert np.all(gt[:, 3].astype(np.int64) >= ct[:, 3])
-    # against the reference algorithm (heap tie order): identical rows except
-    # where the reference run made a tie decision
-    rl, rd, rc, rt = o.search(q, k, ef, mode=O.REFERENCE, allow=allow, trace=True)
     same, bad = compare_rows(gl, rl, rt[:, 4])
     assert same >= min_same and not bad, (same, bad[:5])
     return g
@@ -83,9 +93,10 @@ def test_parity_filter_and_deletes(tmp_path):
 
 
 def test_golden_fixtures():
-    """Against the reference's own recorded outputs.  Rows may differ only
-    where the reference run made a tie decision (the integer fixture is built
-    to have many); everything is bit-exact against the canonical oracle."""
+    """Against the reference's own recorded outputs: the default (tie-exact)
+    mode reproduces them exactly, the integer fixture with its many ties
+    included; the id tie order is bit-exact against the canonical oracle and
+    differs from the recording only on queries with tie decisions."""
     g = golden()
     cases = {"hnsw_l2_d16": "l2", "hnsw_ip_d20": "ip", "hnsw_cos_d12": "cosine", "hnsw_l2_d7_int": "l2"}
     for name, space in cases.items():
@@ -94,26 +105,31 @@ def test_golden_fixtures():
         idx = gpu_index(path, space, q.shape[1])
         o = O.Hnsw(path, space, q.shape[1])
         even = (o.labels() % 2 == 0).astype(np.uint8)
-        min_same = 0.5 if name.endswith("_int") else 0.999
         for ef in (10, 32, 100):
             idx.set_ef(ef)
             for k in (1, 10):
                 for suffix, filt, allow in (("", None, None), ("_even", lambda l: l % 2 == 0, even)):
+                    ref_l = g[f"{name}/ef{ef}_k{k}{suffix}/labels"]
+                    ref_d = g[f"{name}/ef{ef}_k{k}{suffix}/dists"]
+                    idx.tie_order = "reference"
+                    l, d = idx.knn_query(q, k=k, filter=filt)
+                    assert np.array_equal(l, ref_l), (name, ef, k, suffix)
+                    assert np.array_equal(d.view(np.uint32), ref_d.view(np.uint32))
+                    idx.tie_order = "id"
                     l, d = idx.knn_query(q, k=k, filter=filt)
                     cl, cd, _ = o.search(q, k, ef, mode=O.CANONICAL, allow=allow)
                     assert np.array_equal(l, cl) and np.array_equal(d.view(np.uint32), cd.view(np.uint32))
                     _, _, _, rt = o.search(q, k, ef, mode=O.REFERENCE, allow=allow, trace=True)
-                    same, bad = compare_rows(l, g[f"{name}/ef{ef}_k{k}{suffix}/labels"], rt[:, 4])
-                    assert not bad and same >= min_same, (name, ef, k, suffix, same, bad)
+                    same, bad = compare_rows(l, ref_l, rt[:, 4])
+                    assert not bad, (name, ef, k, suffix, same, bad)
+        idx.tie_order = "reference"
         for lab in g[f"{name}/deleted"]:
             idx.mark_deleted(int(lab))
-            o.set_deleted(int(lab), True)
         for ef in (10, 32, 100):
             idx.set_ef(ef)
             l, d = idx.knn_query(q, k=10)
-            _, _, _, rt = o.search(q, 10, ef, mode=O.REFERENCE, trace=True)
-            same, bad = compare_rows(l, g[f"{name}/ef{ef}_k10_del/labels"], rt[:, 4])
-            assert not bad and same >= min_same, (name, ef, bad)
+            assert np.array_equal(l, g[f"{name}/ef{ef}_k10_del/labels"])
+            assert np.array_equal(d.view(np.uint32), g[f"{name}/ef{ef}_k10_del/dists"].view(np.uint32))
             assert not np.isin(l, g[f"{name}/deleted"]).any()
 
 
@@ -194,8 +210,9 @@ def test_large_M_and_k(tmp_path):
 
 def test_full_size_parity_1m():
     """The 1M x 128 integer-valued workload (reference-built graph, M=16,
-    efc=200) at the operating points around recall 0.95: >= 99.9% of queries
-    return the reference's labels, and every other query traces to a tie."""
+    efc=200) at the operating points around recall 0.95: the default
+    tie-exact mode returns the reference's labels and distances for every
+    query; the id tie order differs only on queries with tie decisions."""
     import os
 
     from hnsw_rabitq_b200.datasets import gmm_1m_128
@@ -213,9 +230,13 @@ def test_full_size_parity_1m():
     o = O.Hnsw(path, "l2", 128)
     for ef in (48, 64, 128):
         g.set_ef(ef)
+        rl, rd, _, rt = o.search(qs, 10, ef, mode=O.REFERENCE, trace=True)
+        g.tie_order = "reference"
+        xl, xd = g.knn_query(qs, k=10)
+        assert np.array_equal(xl, rl) and np.array_equal(xd.view(np.uint32), rd.view(np.uint32))
+        g.tie_order = "id"
         gl, gd = g.knn_query(qs, k=10)
         cl, cd, _ = o.search(qs, 10, ef, mode=O.CANONICAL)
         assert np.array_equal(gl, cl) and np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
-        rl, rd, _, rt = o.search(qs, 10, ef, mode=O.REFERENCE, trace=True)
         same, bad = compare_rows(gl, rl, rt[:, 4])
-        assert same >= 0.999 and not bad, (ef, same, bad[:5])
+        assert same >= 0.995 and not bad, (ef, same, bad[:5])
