@@ -17,7 +17,11 @@ constexpr unsigned FULL = 0xffffffffu;
 constexpr uint32_t INVALID_ID = 0xffffffffu;
 constexpr uint32_t EXP_BIT = 0x80000000u;                 // "expanded" flag in a key's id field
 constexpr uint64_t KEY_MASK = ~(uint64_t)EXP_BIT;         // key without the flag
-constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 26;            // bounded mbarrier wait
+// Bounded mbarrier wait: each try_wait may suspend the thread for up to
+// MBAR_SUSPEND_NS (it wakes as soon as the phase completes), at most
+// MBAR_SPIN_LIMIT times -- a few seconds in total before giving up.
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 16;
+constexpr uint32_t MBAR_SUSPEND_NS = 50000;
 
 // ------------------------------------------------------------------ keys
 // Order-preserving map of a float to uint32 (monotone on all non-NaN values).
@@ -68,10 +72,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(addr), "r"(parity)
+            : "r"(addr), "r"(parity), "r"(MBAR_SUSPEND_NS)
             : "memory");
         if (done) return true;
     }
@@ -244,6 +248,9 @@ __device__ __forceinline__ float dist_ip(const float* q, const float* x, int dim
     return __fsub_rn(1.0f, ip_scalar(q, x, dim));
 }
 
+template <int SPACE>
+__device__ __forceinline__ float group4_reduce(float c0, float c1, float c2, float c3);
+
 // The dim % 16 == 0 distance split over a group of 4 lanes (a = lane & 3):
 // lane a keeps the reference's accumulators 4a .. 4a+3 (one float4 of each
 // 16-float chunk), so one LDS.128 per chunk per lane feeds 8 vectors per warp
@@ -273,6 +280,13 @@ __device__ __forceinline__ float group4_dist16(const float* __restrict__ q, cons
             c3 = __fmaf_rn(qv.w, xv.w, c3);
         }
     }
+    return group4_reduce<SPACE>(c0, c1, c2, c3);
+}
+
+// Cross-lane reduction of group4_dist16: lane a of a 4-lane group holds the
+// reference's accumulators 4a .. 4a+3.
+template <int SPACE>
+__device__ __forceinline__ float group4_reduce(float c0, float c1, float c2, float c3) {
     if (SPACE == 0) {
         // accumulators 4..15 from the three lanes to the right
         float b0 = __shfl_down_sync(FULL, c0, 1), b1 = __shfl_down_sync(FULL, c1, 1);

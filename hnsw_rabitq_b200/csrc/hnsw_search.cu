@@ -151,13 +151,15 @@ __device__ __forceinline__ int find_unexpanded(const uint64_t* a, int n, int& hi
 // size), keeping at most cap entries.  Returns the smallest insertion index.
 __device__ __forceinline__ int merge_sorted(uint64_t* a, int& size, int cap, unsigned amask, uint64_t key, int pos,
                                             int lane) {
+    // `key` may carry EXP_BIT (inserted already expanded); order ignores it
+    const uint64_t kc = key & KEY_MASK;
     int na = __popc(amask);
     bool mine = (amask >> lane) & 1u;
     int rank = 0;
     for (unsigned m = amask; m; m &= m - 1) {
         int src = __ffs(m) - 1;
-        uint64_t k2 = shfl64(key, src);
-        rank += (k2 < key);
+        uint64_t k2 = shfl64(kc, src);
+        rank += (k2 < kc);
     }
     int mpos = mine ? pos : 0x7fffffff;
 #pragma unroll
@@ -173,7 +175,7 @@ __device__ __forceinline__ int merge_sorted(uint64_t* a, int& size, int cap, uns
             int sh = 0;
             for (unsigned m = amask; m; m &= m - 1) {
                 int src = __ffs(m) - 1;
-                uint64_t k2 = shfl64(key, src);
+                uint64_t k2 = shfl64(kc, src);
                 sh += (k2 < em);
             }
             __syncwarp();
@@ -213,6 +215,31 @@ struct Counters {
     uint32_t upper_hops, upper_dists, l0_exp, l0_dists;
 };
 
+// Optional per-phase cycle accounting (compile with -DHNSWGPU_PHASE_TIMING;
+// the shipped library is built without it).  Phases: 0 query setup,
+// 1 upper-layer descent, 2 candidate selection, 3 link row + visited cache,
+// 4 staging wait, 5 distance arithmetic, 6 acceptance, 7 heap replay,
+// 8 pool / list maintenance, 9 result output.
+#ifdef HNSWGPU_PHASE_TIMING
+struct PhaseClock {
+    long long last = 0;
+    long long acc[10] = {0};
+    __device__ void start() { last = clock64(); }
+    __device__ void mark(int i) {
+        long long t = clock64();
+        acc[i] += t - last;
+        last = t;
+    }
+};
+#define PT_MARK(i) pc.mark(i)
+#else
+struct PhaseClock {
+    __device__ void start() {}
+    __device__ void mark(int) {}
+};
+#define PT_MARK(i)
+#endif
+
 // Distances of `cnt` (<= 32) nodes held by lanes [0, cnt) (id per lane);
 // result returned in the owning lane.  False on a wait timeout.
 // Rows are staged `stage_slots` at a time.  For dim % 16 == 0 each group of
@@ -220,12 +247,13 @@ struct Counters {
 // dimensions use one lane per row with the scalar-order routine.
 template <int SPACE, bool FAST16>
 __device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t id,
-                                               int cnt, int lane, float& d) {
+                                               int cnt, int lane, float& d, PhaseClock& pc) {
     d = __int_as_float(0x7f800000);
     for (int s0 = 0; s0 < cnt; s0 += (int)p.stage_slots) {
         const int n = min((int)p.stage_slots, cnt - s0);
         const bool mine = lane >= s0 && lane < s0 + n;
         if (!stage_rows(p, s, phase, mine, id, lane - s0, n, lane)) return false;
+        PT_MARK(4);
         if (FAST16) {
             const int a = lane & 3;
             for (int g = 0; g < n; g += 8) {
@@ -240,13 +268,305 @@ __device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& 
             float got = __shfl_sync(FULL, dt, (lane - s0) & 31);
             if (mine) d = got;
         }
+        PT_MARK(5);
+    }
+    return true;
+}
+
+// ------------------------------------------------------------------------
+// Pipelined level-0 beam for the common case (no deletes, no filter,
+// dim % 16 == 0, maxM0 <= 32).  Same decisions as the general loop; the
+// difference is scheduling: as soon as the acceptance of the current
+// expansion is known, the next candidate is fixed (id tie order: the first
+// unexpanded of pool + accepted; tie-exact order: the candidate heap's top,
+// predicted whenever its distance is unique), and its link row, visited-cache
+// update and first TMA batch are issued before the pool merge / heap replay
+// of the current expansion, which then run under that memory latency.
+struct Fetch {
+    uint32_t id;     // this lane's neighbour id (link order), or INVALID_ID
+    bool fresh;      // evaluated now (missed in the visited cache)
+    unsigned nmask;  // fresh lanes
+    int nnew;        // number of fresh lanes
+    uint32_t cid2;   // id of the lane-th fresh neighbour (lanes < nnew)
+    int n0;          // rows of the first staging batch in flight
+};
+
+__device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, uint32_t c, int lane, Fetch& f) {
+    const uint32_t* lrow = p.links0 + (size_t)c * p.maxM0;
+    const uint32_t id = lane < (int)p.maxM0 ? __ldg(lrow + lane) : INVALID_ID;
+    bool fresh = id != INVALID_ID;
+    if (!p.links_unique) {
+        unsigned peers = __match_any_sync(FULL, id);
+        fresh = fresh && (__ffs(peers) - 1 == lane);
+    }
+    const uint32_t slot = fresh ? vis_slot(id, p.log2_vis) : 0;
+    if (fresh && s.vis[slot] == id) fresh = false;
+    __syncwarp();
+    if (fresh) s.vis[slot] = id;
+    f.id = id;
+    f.fresh = fresh;
+    f.nmask = __ballot_sync(FULL, fresh);
+    f.nnew = __popc(f.nmask);
+    const int src = (int)__fns(f.nmask, 0, lane + 1);
+    f.cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
+    f.n0 = min((int)p.stage_slots, f.nnew);
+    if (f.n0 > 0) {
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)f.n0 * p.row_bytes);
+        __syncwarp();
+        if (lane < f.n0)
+            bulk_g2s(s.stage + (size_t)lane * p.stage_stride, p.vecs + (size_t)f.cid2 * p.row_floats, p.row_bytes,
+                     s.bar);
+    }
+}
+
+// Distances of the staged rows [0, n) into the compacted lanes [s0, s0 + n).
+template <int SPACE>
+__device__ __forceinline__ void batch_dist(const SearchParams& p, const WarpSmem& s, const float4* qr, int n, int s0,
+                                           int lane, float& dc) {
+    const int a = lane & 3;
+    const int n16 = (int)(p.dim >> 4);
+    for (int g = 0; g < n; g += 8) {
+        const int v = min(g + (lane >> 2), n - 1);
+        const float4* x4 = reinterpret_cast<const float4*>(s.stage + (size_t)v * p.stage_stride);
+        float r;
+        if (n16 <= 8) {
+            // query chunks held in registers (qr[c] = this lane's float4 of chunk c)
+            float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                if (c < n16) {
+                    const float4 qv = qr[c], xv = x4[4 * c + a];
+                    if (SPACE == 0) {
+                        float t0 = __fsub_rn(qv.x, xv.x), t1 = __fsub_rn(qv.y, xv.y), t2 = __fsub_rn(qv.z, xv.z),
+                              t3 = __fsub_rn(qv.w, xv.w);
+                        c0 = __fmaf_rn(t0, t0, c0);
+                        c1 = __fmaf_rn(t1, t1, c1);
+                        c2 = __fmaf_rn(t2, t2, c2);
+                        c3 = __fmaf_rn(t3, t3, c3);
+                    } else {
+                        c0 = __fmaf_rn(qv.x, xv.x, c0);
+                        c1 = __fmaf_rn(qv.y, xv.y, c1);
+                        c2 = __fmaf_rn(qv.z, xv.z, c2);
+                        c3 = __fmaf_rn(qv.w, xv.w, c3);
+                    }
+                }
+            }
+            r = group4_reduce<SPACE>(c0, c1, c2, c3);
+        } else {
+            r = group4_dist16<SPACE>(s.q, reinterpret_cast<const float*>(x4), n16, a);
+        }
+        const int t = lane - s0 - g;  // compacted index of this lane within the pass
+        const float got = __shfl_sync(FULL, r, (t & 7) << 2);
+        if (t >= 0 && t < 8 && t + g < n) dc = got;
+    }
+}
+
+// Distances of all fresh neighbours of a fetched list; result in the owning
+// (link-order) lane.
+template <int SPACE>
+__device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem& s, uint32_t& phase, const Fetch& f,
+                                                const float4* qr, int lane, float& d, PhaseClock& pc) {
+    float dc = __int_as_float(0x7f800000);
+    if (f.n0 > 0) {
+        const bool ok = mbar_wait(s.bar, phase);
+        phase ^= 1u;
+        if (!__all_sync(FULL, ok)) return false;
+        PT_MARK(4);
+        batch_dist<SPACE>(p, s, qr, f.n0, 0, lane, dc);
+        PT_MARK(5);
+    }
+    for (int s0 = f.n0; s0 < f.nnew; s0 += (int)p.stage_slots) {
+        const int n = min((int)p.stage_slots, f.nnew - s0);
+        const bool mine = lane >= s0 && lane < s0 + n;
+        if (!stage_rows(p, s, phase, mine, f.cid2, lane - s0, n, lane)) return false;
+        PT_MARK(4);
+        batch_dist<SPACE>(p, s, qr, n, s0, lane, dc);
+        PT_MARK(5);
+    }
+    const int ci = __popc(f.nmask & lanemask_lt());
+    d = __shfl_sync(FULL, dc, ci & 31);
+    return true;
+}
+
+template <int SPACE, bool EXACT>
+__device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
+                               PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
+                               uint32_t& status) {
+    const int ef = (int)p.ef;
+    const int pcap = (int)p.pool_cap;
+    int hint_p = 0, csz = 0;
+    // the entry point is pushed and popped at once (hnswalg.h:325-359)
+    if (lane == 0) {
+        s.pool[0] = mkkey(d0, ep) | (EXACT ? 0u : EXP_BIT);
+        if (EXACT) s.topheap[0] = mkkey(d0, ep);
+    }
+    psize = 1;
+    tsz = EXACT ? 1 : 0;
+    __syncwarp();
+    Fetch f;
+    fetch_links(p, s, ep, lane, f);
+    ct.l0_exp += 1;
+    PT_MARK(3);
+    while (true) {
+        ct.l0_dists += f.nnew;
+        float d;
+        if (!fetch_distances<SPACE>(p, s, phase, f, qr, lane, d, pc)) return false;
+        // ---- acceptance (closed form of hnswalg.h:395 over the link order)
+        const uint32_t dk = fkey(d);
+        const bool full = psize == ef;
+        const uint32_t lbk = full ? khi(s.pool[psize - 1]) : 0xffffffffu;
+        bool live = f.fresh && !(full && dk >= lbk);
+        uint64_t key = ((uint64_t)dk << 32) | f.id;
+        int posP = 0, cntP = 0;
+        if (live) {
+            bool dup = false;
+            cntP = upper_bound_hi(s.pool, psize, dk);
+            posP = insert_pos(s.pool, cntP, dk, f.id, dup);
+            if (dup) live = false;
+        }
+        const unsigned amask = __ballot_sync(FULL, live);
+        int cntN = 0;
+        for (unsigned m = amask; m; m &= m - 1) {
+            const int src2 = __ffs(m) - 1;
+            const uint32_t dk2 = __shfl_sync(FULL, dk, src2);
+            cntN += (src2 < lane && dk2 <= dk);
+        }
+        const bool accept = live && cntP + cntN < ef;
+        const unsigned pmask = __ballot_sync(FULL, accept);
+        PT_MARK(6);
+        // ---- the next candidate
+        uint64_t kmin = accept ? key : ~0ull;  // smallest accepted key
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            uint64_t other = shfl64(kmin, lane ^ o);
+            kmin = other < kmin ? other : kmin;
+        }
+        bool have_next = false, spec = false;
+        uint32_t next = INVALID_ID;
+        if (!EXACT) {
+            int ip = find_unexpanded(s.pool, psize, hint_p, lane);
+            const uint64_t kp = ip >= 0 ? (s.pool[ip] & KEY_MASK) : ~0ull;
+            if (kp != ~0ull || kmin != ~0ull) {
+                have_next = true;
+                if (kmin < kp) {
+                    next = (uint32_t)kmin;
+                    if (accept && key == kmin) key |= EXP_BIT;  // inserted already expanded
+                } else {
+                    next = kid(kp);
+                    __syncwarp();
+                    if (lane == 0) s.pool[ip] |= EXP_BIT;
+                    __syncwarp();
+                }
+            }
+        } else {
+            // candidate_set after this expansion's pushes: its top is the
+            // smallest of the current heap top and the accepted keys; when
+            // that distance is unique the heap layout cannot matter
+            const uint64_t r0 = csz > 0 ? s.candheap[0] : ~0ull;
+            const uint32_t r0d = khi(r0);
+            const bool r0tie = (csz > 1 && khi(s.candheap[1]) == r0d) || (csz > 2 && khi(s.candheap[2]) == r0d);
+            const uint32_t ad = khi(kmin);
+            const uint32_t nd = min(r0d, ad);
+            const int acount = __popc(__ballot_sync(FULL, accept && dk == nd));
+            const int mult = (csz > 0 && r0d == nd ? 1 + (r0tie ? 1 : 0) : 0) + acount;
+            if ((csz > 0 || kmin != ~0ull) && mult == 1) {
+                spec = true;
+                next = r0d == nd && csz > 0 ? kid(r0) : (uint32_t)kmin;
+            }
+        }
+        Fetch fn;
+        if (have_next || spec) fetch_links(p, s, next, lane, fn);
+        PT_MARK(2);
+        // ---- bookkeeping of this expansion, under the latency of the next fetch
+        int nev = 0;
+        if (EXACT && pmask) {
+            if (accept) s.accbuf[__popc(pmask & lanemask_lt())] = key;
+            __syncwarp();
+            const int na = __popc(pmask);
+            uint32_t ovf = 0;
+            if (lane == 0) {
+                int cn = csz, tn = tsz;
+                for (int t = 0; t < na; t++) {
+                    const uint64_t e = s.accbuf[t];
+                    if (cn < (int)p.cand_cap) ref_heap_push(s.candheap, cn, e, CandLess());
+                    else ovf = 1;
+                    ref_heap_push(s.topheap, tn, e, TopLess());
+                    if (tn > ef) s.evbuf[nev++] = ref_heap_pop(s.topheap, tn, TopLess());
+                }
+                csz = cn;
+                tsz = tn;
+            }
+            csz = __shfl_sync(FULL, csz, 0);
+            tsz = __shfl_sync(FULL, tsz, 0);
+            nev = __shfl_sync(FULL, nev, 0);
+            if (__shfl_sync(FULL, ovf, 0)) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+            __syncwarp();
+            PT_MARK(7);
+        }
+        if (pmask) {
+            const int m = merge_sorted(s.pool, psize, pcap, pmask, key, posP, lane);
+            hint_p = min(hint_p, m);
+        }
+        if (EXACT && nev) remove_keys(s.pool, psize, s.evbuf, nev, lane);
+        if (!EXACT) {
+            // the expansion after `next` is most often the first unexpanded
+            // entry now: pull its link row into L2 while `next` runs
+            int h2 = hint_p;
+            const int nx = find_unexpanded(s.pool, psize, h2, lane);
+            if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
+        }
+        PT_MARK(8);
+        if (EXACT) {
+            // the reference's loop head: top of candidate_set vs lowerBound
+            bool go = false;
+            uint32_t top_id = INVALID_ID;
+            if (csz > 0) {
+                const uint64_t c = s.candheap[0];
+                const uint32_t lb = khi(s.pool[psize - 1]);
+                go = !(khi(c) > lb);
+                top_id = kid(c);
+            }
+            if (!go) {
+                if (spec && fn.n0 > 0) {  // drain the unused copies
+                    mbar_wait(s.bar, phase);
+                    phase ^= 1u;
+                }
+                break;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                int n = csz;
+                ref_heap_pop(s.candheap, n, CandLess());
+                if (n > 0) prefetch_l2(p.links0 + (size_t)kid(s.candheap[0]) * p.maxM0);
+            }
+            csz--;
+            __syncwarp();
+            if (spec && top_id != next) {
+                // cannot happen when the prediction holds; recover by refetching
+                status |= HNSWGPU_STATUS_TIMEOUT_BIT;
+                if (fn.n0 > 0) {
+                    mbar_wait(s.bar, phase);
+                    phase ^= 1u;
+                }
+                spec = false;
+            }
+            if (!spec) fetch_links(p, s, top_id, lane, fn);
+        } else if (!have_next) {
+            break;
+        }
+        f = fn;
+        ct.l0_exp += 1;
+        PT_MARK(2);
     }
     return true;
 }
 
 template <int SPACE, bool FAST16, bool EXACT>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
-                           Counters& ct) {
+                           Counters& ct, PhaseClock& pc) {
+    pc.start();
     const int dim = (int)p.dim;
     const uint32_t ef = p.ef;
     // ---- query row (normalised for the cosine space)
@@ -264,10 +584,11 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     const uint32_t nvis = 1u << p.log2_vis;
     for (uint32_t i = lane; i < nvis; i += 32) s.vis[i] = INVALID_ID;
 
+    PT_MARK(0);
     // ---- upper-layer greedy descent (hnswalg.h:1274-1302)
     uint32_t cur = p.ep;
     float curd;
-    if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, curd)) return false;
+    if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, curd, pc)) return false;
     curd = __shfl_sync(FULL, curd, 0);
     ct.upper_dists += 1;
     const uint32_t up_stride = p.maxM + 1;
@@ -283,7 +604,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
                 int n = min(32, cnt - c0);
                 uint32_t id = lane < n ? row[1 + c0 + lane] : INVALID_ID;
                 float d;
-                if (!lane_distances<SPACE, FAST16>(p, s, phase, id, n, lane, d)) return false;
+                if (!lane_distances<SPACE, FAST16>(p, s, phase, id, n, lane, d, pc)) return false;
                 float m = lane < n ? d : __int_as_float(0x7f800000);
 #pragma unroll
                 for (int o = 16; o; o >>= 1) m = fminf(m, __shfl_xor_sync(FULL, m, o));
@@ -299,6 +620,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         }
     }
 
+    PT_MARK(1);
     // ---- level-0 beam (hnswalg.h:308-440)
     const bool bare = p.bare != 0;
     int psize = 0, xsize = 0, hint_p = 0, hint_x = 0;
@@ -311,9 +633,24 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     const int pcap = (int)p.pool_cap;  // ef, or ef + 32 in tie-exact mode
     int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
     const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
+    const bool pipe = FAST16 && bare && p.maxM0 <= 32;
+    if (pipe) {
+        float d0;
+        if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0, pc)) return false;
+        d0 = __shfl_sync(FULL, d0, 0);
+        ct.l0_dists += 1;
+        if (lane == 0) s.vis[vis_slot(cur, p.log2_vis)] = cur;
+        float4 qr[8];
+        const int n16 = (int)(p.dim >> 4);
+        const float4* q4 = reinterpret_cast<const float4*>(s.q);
+#pragma unroll
+        for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+        if (!base_pipelined<SPACE, EXACT>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status)) return false;
+    } else {
     if (bare || is_allowed(p, cur)) {
         float d0;
-        if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0)) return false;
+        if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0, pc)) return false;
         d0 = __shfl_sync(FULL, d0, 0);
         ct.l0_dists += 1;
         if (lane == 0) s.pool[0] = mkkey(d0, cur);
@@ -382,6 +719,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
         }
       }
+        PT_MARK(2);
         if (ct.l0_exp > p.max_expansions) {
             // only reachable after a candidate-list overflow (nodes dropped
             // from the list can be re-admitted); stop and flag the query
@@ -403,6 +741,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             if (fresh) s.vis[slot] = id;
             unsigned nmask = __ballot_sync(FULL, fresh);
             int nnew = __popc(nmask);
+            PT_MARK(3);
             if (nnew == 0) continue;
             ct.l0_dists += nnew;
             // compact the fresh ids to lanes [0, nnew), evaluate, route back
@@ -410,7 +749,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             int src = __fns(nmask, 0, lane + 1);  // lane holding the (lane)-th fresh id
             uint32_t cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
             float dc;
-            if (!lane_distances<SPACE, FAST16>(p, s, phase, cid2, nnew, lane, dc)) return false;
+            if (!lane_distances<SPACE, FAST16>(p, s, phase, cid2, nnew, lane, dc, pc)) return false;
             float d = __shfl_sync(FULL, dc, ci & 31);
             // ---- acceptance (closed form of the sequential test)
             uint32_t dk = fkey(d);
@@ -437,6 +776,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             bool accept = live && (uint32_t)(cntP + cntN) < ef;
             unsigned pmask = __ballot_sync(FULL, accept && allowed);
             unsigned xmask = bare ? 0u : __ballot_sync(FULL, accept && !allowed);
+            PT_MARK(6);
             int nev = 0;
             if (EXACT && (pmask | xmask)) {
                 // replay the reference's heap operations for the accepted
@@ -469,6 +809,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
                 nev = __shfl_sync(FULL, nev, 0);
                 if (__shfl_sync(FULL, ovf, 0)) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
                 __syncwarp();
+                PT_MARK(7);
             }
             if (pmask) {
                 int m = merge_sorted(s.pool, psize, pcap, pmask, key, posP, lane);
@@ -485,8 +826,11 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
                 xsize = upper_bound_hi(s.extra, xsize, khi(s.pool[psize - 1]));
                 hint_x = min(hint_x, xsize);
             }
+            PT_MARK(8);
         }
     }
+    PT_MARK(2);
+    }  // general loop
 
     const uint32_t k = p.k;
     if (EXACT) {
@@ -541,11 +885,12 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         p.out_counts[qi] = kk;
         if (status) atomicOr(p.status, status);
     }
+    PT_MARK(9);
     return true;
 }
 
 template <int SPACE, bool FAST16, bool EXACT>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) hnsw_search_kernel(SearchParams p) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base = smem + (size_t)warp * p.warp_smem;
@@ -564,13 +909,14 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) hnsw_search_kernel(Sea
     fence_mbar_init();
     __syncwarp();
     uint32_t phase = 0;
+    PhaseClock pc;
     while (true) {
         uint32_t qi = 0;
         if (lane == 0) qi = atomicAdd(p.work_counter, 1u);
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE, FAST16, EXACT>(p, s, phase, qi, lane, ct)) {
+        if (!search_one<SPACE, FAST16, EXACT>(p, s, phase, qi, lane, ct, pc)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
@@ -584,6 +930,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) hnsw_search_kernel(Sea
             t[3] = ct.l0_dists;
         }
     }
+#ifdef HNSWGPU_PHASE_TIMING
+    if (lane == 0 && p.phase_cycles)
+        for (int i = 0; i < 10; i++) atomicAdd(p.phase_cycles + i, (unsigned long long)pc.acc[i]);
+#endif
     // The last block to finish re-arms this launch's work counter, so the
     // next launch that draws the same counter slot starts from zero.
     __syncthreads();

@@ -7,7 +7,14 @@
 
 namespace hnswgpu {
 
-constexpr int kWarpsPerBlock = 4;
+#ifndef HNSWGPU_WPB
+#define HNSWGPU_WPB 1
+#endif
+#ifndef HNSWGPU_MINB
+#define HNSWGPU_MINB 16
+#endif
+constexpr int kWarpsPerBlock = HNSWGPU_WPB;  // independent query warps per CTA
+constexpr int kMinBlocks = HNSWGPU_MINB;     // launch bound: resident CTAs per SM
 constexpr uint32_t HNSWGPU_STATUS_TIMEOUT_BIT = 0x1u;
 constexpr uint32_t HNSWGPU_STATUS_OVERFLOW_BIT = 0x2u;
 
@@ -29,6 +36,7 @@ struct SearchParams {
     uint32_t bare, normalize;
     uint32_t max_expansions;      // safety bound on level-0 expansions per query
     uint32_t fast16;              // dim % 16 == 0: 4-lanes-per-row distance path
+    uint32_t links_unique;        // no level-0 list repeats an id (checked at load)
     uint32_t exact;               // replay the reference's heaps (tie order exact)
     uint32_t pool_cap;            // ef (canonical) or ef + 32 (tie-exact)
     uint32_t cand_cap;            // tie-exact: candidate heap capacity
@@ -40,6 +48,7 @@ struct SearchParams {
     uint32_t* work_counter;       // zero at launch; reset to zero by the last block
     uint32_t* done_counter;       // blocks finished (same slot discipline)
     uint32_t* status;
+    unsigned long long* phase_cycles;  // 10 counters, profiling builds only (may be null)
     // per-warp shared memory layout
     uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
     uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;

@@ -93,6 +93,7 @@ struct hnswgpu_index {
     std::vector<uint64_t> labels;
     std::unordered_map<uint64_t, uint32_t> lookup;
     std::vector<uint32_t> deleted;  // host copy of the bitmap
+    bool links_unique = true;       // no level-0 list repeats an id
     uint64_t num_deleted = 0;
     DevBuf<float> vecs;
     DevBuf<uint32_t> links0, upper_off, upper_links, deleted_bits;
@@ -233,6 +234,22 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
             h->lookup[lab] = (uint32_t)i;
         }
     }
+    // level-0 lists that repeat an id (hnswlib never writes one) need the
+    // kernel's per-list duplicate check
+    {
+        std::vector<uint32_t> stamp(cur, 0xffffffffu);
+        h->links_unique = true;
+        for (uint64_t i = 0; i < cur && h->links_unique; i++)
+            for (uint64_t j = 0; j < maxM0; j++) {
+                uint32_t v = hl[i * maxM0 + j];
+                if (v == 0xffffffffu) break;
+                if (stamp[v] == (uint32_t)i) {
+                    h->links_unique = false;
+                    break;
+                }
+                stamp[v] = (uint32_t)i;
+            }
+    }
     // upper levels (hnswalg.h:795-809)
     std::vector<uint32_t> hoff(cur, 0xffffffffu);
     std::vector<int> level(cur, 0);
@@ -366,6 +383,10 @@ uint32_t next_pow2_log2(uint64_t v) {
     return l;
 }
 
+#ifdef HNSWGPU_PHASE_TIMING
+unsigned long long* g_phase_buf = nullptr;
+#endif
+
 int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
@@ -421,6 +442,7 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     // row pad of 16 floats puts consecutive rows half a bank cycle apart
     // (conflict-free quarter warps); the one-lane-per-row path wants 4.
     p.fast16 = (h->dim % 16 == 0) ? 1u : 0u;
+    p.links_unique = h->links_unique ? 1u : 0u;
     p.stage_stride = h->row_floats + (p.fast16 ? 16u : 4u);
     uint32_t slots = (uint32_t)((9u * 1024u + 512u) / (p.stage_stride * 4));
     p.stage_slots = std::max(1u, std::min(p.fast16 ? 16u : 32u, slots));
@@ -443,6 +465,15 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     }
     if (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
+#ifdef HNSWGPU_PHASE_TIMING
+    static unsigned long long* phase_buf = nullptr;
+    if (!phase_buf) {
+        cuda_check(cudaMalloc((void**)&phase_buf, 10 * sizeof(unsigned long long)), "cudaMalloc");
+        cuda_check(cudaMemset(phase_buf, 0, 10 * sizeof(unsigned long long)), "cudaMemset");
+    }
+    p.phase_cycles = phase_buf;
+    g_phase_buf = phase_buf;
+#endif
     uint32_t slot = h->next_counter++ % (uint32_t)(h->counters.n / 2);
     p.work_counter = h->counters.p + 2 * slot;
     p.done_counter = h->counters.p + 2 * slot + 1;
@@ -676,5 +707,17 @@ int hnswgpu_get_status(hnswgpu_index* h, uint32_t* out_bits) {
         return HNSWGPU_OK;
     });
 }
+
+#ifdef HNSWGPU_PHASE_TIMING
+// Profiling builds only: per-phase cycle totals of all searches since the
+// last call (10 counters), cleared on read.
+HNSWGPU_API int hnswgpu_phase_cycles(unsigned long long* out) {
+    if (!g_phase_buf) return fail(HNSWGPU_ERR_ARG, "no search ran");
+    cudaDeviceSynchronize();
+    cudaMemcpy(out, g_phase_buf, 10 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    cudaMemset(g_phase_buf, 0, 10 * sizeof(unsigned long long));
+    return HNSWGPU_OK;
+}
+#endif
 
 }  // extern "C"
