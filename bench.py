@@ -46,7 +46,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CACHE = os.path.join(ROOT, ".cache")
-EFS = [10, 16, 24, 32, 48, 64, 96, 128, 192, 256, 320, 400]
+EFS = [10, 16, 24, 32, 40, 44, 48, 52, 56, 64, 80, 96, 128, 192, 256, 320, 400]
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -339,7 +339,7 @@ def run_ours(args, dist: Dist):
             per_launch = bytes_per_q * nq
             achieved = per_launch / (ms_step / 1e3) / 1e9
             roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                    "frac": round(achieved / peak, 4), "traffic": committed_traffic(ef_star),
+                    "frac": round(achieved / peak, 4), "traffic": committed_traffic(args.tie_order, ef_star),
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                     else "fallback 6.65 TB/s",
                     "algorithmic_bytes_per_query": round(bytes_per_q, 1)}
@@ -366,16 +366,15 @@ def run_ours(args, dist: Dist):
     return out
 
 
-def committed_traffic(ef):
+def committed_traffic(tie_order, ef):
     """DRAM bytes per launch of hnsw_search_kernel from the committed ncu
-    summary (profiles/), for the same ef, or None."""
+    summary (profiles/), for the same tie order and ef, or None."""
     p = os.path.join(ROOT, "profiles", "hnsw_search_gmm1m_traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        v = d.get(str(ef))
-        return v
-    except (OSError, ValueError):
+        return d.get(tie_order, {}).get(str(ef))
+    except (OSError, ValueError, AttributeError):
         return None
 
 

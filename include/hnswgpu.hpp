@@ -1,0 +1,208 @@
+// hnswgpu.hpp -- header-only C++ classes over the C ABI (hnswgpu.h) with the
+// shape of hnswlib's query API, so that C++ code written against hnswlib
+// 0.9.0 switches by changing the namespace and the space type:
+//
+//   hnswlib::L2Space space(dim);                    hnswgpu::L2Space space(dim);
+//   auto* a = new hnswlib::HierarchicalNSW<float>(  auto* a = new hnswgpu::HierarchicalNSW<float>(
+//       &space, "index.bin");                           &space, "index.bin");
+//   a->setEf(64);                                   a->setEf(64);
+//   auto pq = a->searchKnn(q, 10, &filter);         auto pq = a->searchKnn(q, 10, &filter);
+//
+// Replaced interfaces: HierarchicalNSW load constructor, setEf, searchKnn,
+// searchKnnCloserFirst, markDelete / unmarkDelete (hnswlib/hnswalg.h:78-86,
+// 173-175, 852-927, 1269-1323; hnswlib/hnswlib.h:186-221), BruteforceSearch
+// load constructor and searchKnn (hnswlib/bruteforce.h:35-43, 106-125),
+// BaseFilterFunctor (hnswlib/hnswlib.h:128-132).  Errors are thrown as
+// std::runtime_error with the reference's messages.  Index construction
+// (addPoint) stays with hnswlib: build and save there, load here.
+#pragma once
+#include <cstdint>
+#include <queue>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "hnswgpu.h"
+
+namespace hnswgpu {
+
+typedef size_t labeltype;
+
+// Same contract as hnswlib::BaseFilterFunctor: true = the label may be
+// returned.  The GPU path evaluates it once per search call for every label
+// of the index (the reference calls it per candidate).
+class BaseFilterFunctor {
+ public:
+    virtual bool operator()(labeltype) { return true; }
+    virtual ~BaseFilterFunctor() {}
+};
+
+class SpaceInterface {
+ public:
+    virtual int space_kind() const = 0;
+    virtual size_t dim() const = 0;
+    size_t get_data_size() const { return dim() * sizeof(float); }
+    virtual ~SpaceInterface() {}
+};
+
+class L2Space : public SpaceInterface {
+    size_t dim_;
+
+ public:
+    explicit L2Space(size_t dim) : dim_(dim) {}
+    int space_kind() const override { return HNSWGPU_SPACE_L2; }
+    size_t dim() const override { return dim_; }
+};
+
+class InnerProductSpace : public SpaceInterface {
+    size_t dim_;
+
+ public:
+    explicit InnerProductSpace(size_t dim) : dim_(dim) {}
+    int space_kind() const override { return HNSWGPU_SPACE_IP; }
+    size_t dim() const override { return dim_; }
+};
+
+// The Python binding's "cosine" space: inner product with queries
+// normalised on the way in (stored vectors are expected normalised).
+class CosineSpace : public SpaceInterface {
+    size_t dim_;
+
+ public:
+    explicit CosineSpace(size_t dim) : dim_(dim) {}
+    int space_kind() const override { return HNSWGPU_SPACE_COSINE; }
+    size_t dim() const override { return dim_; }
+};
+
+namespace detail {
+inline void check(int rc) {
+    if (rc != HNSWGPU_OK) throw std::runtime_error(hnswgpu_last_error());
+}
+
+class IndexBase {
+ protected:
+    hnswgpu_index* h_ = nullptr;
+    size_t dim_ = 0;
+    uint32_t flags_ = 0;
+
+    std::vector<uint8_t> mask(BaseFilterFunctor* f) const {
+        std::vector<uint8_t> m;
+        if (!f) return m;
+        hnswgpu_info info;
+        check(hnswgpu_get_info(h_, &info));
+        std::vector<uint64_t> labels(info.count);
+        if (info.count) check(hnswgpu_get_labels(h_, labels.data()));
+        m.resize(info.count);
+        for (size_t i = 0; i < labels.size(); i++) m[i] = (*f)((labeltype)labels[i]) ? 1 : 0;
+        return m;
+    }
+
+ public:
+    IndexBase() = default;
+    IndexBase(const IndexBase&) = delete;
+    IndexBase& operator=(const IndexBase&) = delete;
+    ~IndexBase() {
+        if (h_) hnswgpu_free(h_);
+    }
+
+    // Batched search (an extension): nq queries, closest-first rows of k
+    // labels / distances, counts[i] = results found (rest: UINT64_MAX / +inf).
+    void searchKnnBatch(const float* queries, size_t nq, size_t k, labeltype* labels, float* dists,
+                        int32_t* counts, BaseFilterFunctor* f = nullptr) const {
+        std::vector<uint8_t> m = mask(f);
+        hnswgpu_search_opts o{};
+        o.flags = flags_;
+        o.allow = f ? m.data() : nullptr;
+        static_assert(sizeof(labeltype) == sizeof(uint64_t), "labeltype must be 64-bit");
+        check(hnswgpu_search(h_, queries, nq, k, &o, reinterpret_cast<uint64_t*>(labels), dists, counts));
+    }
+
+    // hnswlib's searchKnn: a max-heap of (distance, label), farthest on top.
+    std::priority_queue<std::pair<float, labeltype>> searchKnn(const void* query, size_t k,
+                                                               BaseFilterFunctor* f = nullptr) const {
+        std::vector<labeltype> l(k);
+        std::vector<float> d(k);
+        int32_t c = 0;
+        searchKnnBatch(static_cast<const float*>(query), 1, k, l.data(), d.data(), &c, f);
+        std::priority_queue<std::pair<float, labeltype>> out;
+        for (int32_t i = 0; i < c; i++) out.emplace(d[i], l[i]);
+        return out;
+    }
+
+    // AlgorithmInterface::searchKnnCloserFirst (hnswlib/hnswlib.h:203-221).
+    std::vector<std::pair<float, labeltype>> searchKnnCloserFirst(const void* query, size_t k,
+                                                                  BaseFilterFunctor* f = nullptr) const {
+        auto pq = searchKnn(query, k, f);
+        std::vector<std::pair<float, labeltype>> r(pq.size());
+        size_t n = pq.size();
+        while (!pq.empty()) {
+            r[--n] = pq.top();
+            pq.pop();
+        }
+        return r;
+    }
+
+    size_t getCurrentElementCount() const {
+        hnswgpu_info info;
+        check(hnswgpu_get_info(h_, &info));
+        return info.count;
+    }
+    size_t getMaxElements() const {
+        hnswgpu_info info;
+        check(hnswgpu_get_info(h_, &info));
+        return info.max_elements;
+    }
+    hnswgpu_index* handle() const { return h_; }
+};
+}  // namespace detail
+
+template <typename dist_t = float>
+class HierarchicalNSW : public detail::IndexBase {
+    static_assert(sizeof(dist_t) == sizeof(float), "the GPU path computes float distances");
+
+ public:
+    // HierarchicalNSW(SpaceInterface*, location, nmslib, max_elements,
+    // allow_replace_deleted) -- loads a file written by saveIndex.
+    HierarchicalNSW(const SpaceInterface* s, const std::string& location, bool nmslib = false,
+                    size_t max_elements = 0, bool allow_replace_deleted = false, int device = 0) {
+        (void)nmslib;
+        (void)allow_replace_deleted;
+        dim_ = s->dim();
+        flags_ = HNSWGPU_EXACT_TIES;
+        detail::check(hnswgpu_load_hnsw(location.c_str(), s->space_kind(), dim_, max_elements, device, &h_));
+    }
+
+    void setEf(size_t ef) { detail::check(hnswgpu_set_ef(h_, ef)); }
+    size_t getEf() const {
+        hnswgpu_info info;
+        detail::check(hnswgpu_get_info(h_, &info));
+        return info.ef;
+    }
+    // true (default): equal distances resolve exactly as hnswlib's heaps do;
+    // false: ties break by internal id (faster, identical without ties).
+    void setReferenceTieOrder(bool on) { flags_ = on ? HNSWGPU_EXACT_TIES : 0u; }
+
+    void markDelete(labeltype label) { detail::check(hnswgpu_mark_deleted(h_, label)); }
+    void unmarkDelete(labeltype label) { detail::check(hnswgpu_unmark_deleted(h_, label)); }
+    size_t getDeletedCount() const {
+        hnswgpu_info info;
+        detail::check(hnswgpu_get_info(h_, &info));
+        return info.num_deleted;
+    }
+};
+
+template <typename dist_t = float>
+class BruteforceSearch : public detail::IndexBase {
+    static_assert(sizeof(dist_t) == sizeof(float), "the GPU path computes float distances");
+
+ public:
+    // BruteforceSearch(SpaceInterface*, location) -- loads a file written by
+    // BruteforceSearch::saveIndex.
+    BruteforceSearch(const SpaceInterface* s, const std::string& location, int device = 0) {
+        dim_ = s->dim();
+        detail::check(hnswgpu_load_bf(location.c_str(), s->space_kind(), dim_, device, &h_));
+    }
+};
+
+}  // namespace hnswgpu

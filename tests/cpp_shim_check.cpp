@@ -1,0 +1,69 @@
+// Drives the C++ shim (include/hnswgpu.hpp) the way hnswlib's own C++ tests
+// drive hnswlib (tests/cpp/searchKnnCloserFirst_test.cpp,
+// tests/cpp/searchKnnWithFilter_test.cpp): prints the closest-first results
+// of searchKnn for every query so the Python side can compare them with the
+// reference's recorded outputs, and checks closer-first ordering, filter
+// functors and delete marks.  Usage: cpp_shim_check index.bin queries.f32 dim nq k ef
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+
+#include "hnswgpu.hpp"
+
+struct PickNothing : public hnswgpu::BaseFilterFunctor {
+    bool operator()(hnswgpu::labeltype) override { return false; }
+};
+struct PickDivisible : public hnswgpu::BaseFilterFunctor {
+    size_t div;
+    explicit PickDivisible(size_t d) : div(d) {}
+    bool operator()(hnswgpu::labeltype l) override { return l % div == 0; }
+};
+
+int main(int argc, char** argv) {
+    if (argc != 7) return 2;
+    const char* path = argv[1];
+    size_t dim = atoi(argv[3]), nq = atoi(argv[4]), k = atoi(argv[5]), ef = atoi(argv[6]);
+    std::vector<float> q(nq * dim);
+    FILE* f = fopen(argv[2], "rb");
+    if (!f || fread(q.data(), 4, q.size(), f) != q.size()) return 3;
+    fclose(f);
+    hnswgpu::L2Space space(dim);
+    auto* alg = new hnswgpu::HierarchicalNSW<float>(&space, path);
+    alg->setEf(ef);
+    for (size_t i = 0; i < nq; i++) {
+        auto pq = alg->searchKnn(q.data() + i * dim, k);
+        auto cf = alg->searchKnnCloserFirst(q.data() + i * dim, k);
+        if (cf.size() != pq.size()) return 4;
+        // closer first == the heap popped into reverse order
+        for (size_t j = cf.size(); j-- > 0;) {
+            if (cf[j] != pq.top()) return 5;
+            pq.pop();
+        }
+        for (auto& r : cf) printf("%llu %.9g ", (unsigned long long)r.second, r.first);
+        printf("\n");
+    }
+    PickNothing none;
+    if (!alg->searchKnn(q.data(), k, &none).empty()) return 6;
+    PickDivisible d3(3);
+    for (auto& r : alg->searchKnnCloserFirst(q.data(), k, &d3))
+        if (r.second % 3) return 7;
+    auto first = alg->searchKnnCloserFirst(q.data(), 1)[0].second;
+    alg->markDelete(first);
+    for (auto& r : alg->searchKnnCloserFirst(q.data(), k))
+        if (r.second == first) return 8;
+    try {
+        alg->markDelete(first);
+        return 9;
+    } catch (const std::runtime_error&) {
+    }
+    alg->unmarkDelete(first);
+    if (alg->searchKnnCloserFirst(q.data(), 1)[0].second != first) return 10;
+    try {
+        hnswgpu::HierarchicalNSW<float> bad(&space, "/nonexistent/index.bin");
+        return 11;
+    } catch (const std::runtime_error& e) {
+        if (std::string(e.what()) != "Cannot open file") return 12;
+    }
+    delete alg;
+    return 0;
+}
