@@ -50,6 +50,7 @@ SIGNATURES = {
     "hnswgpu_unmark_deleted": (C.c_int, [P, U64]),
     "hnswgpu_search": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_get_status": (C.c_int, [P, C.POINTER(U32)]),
+    "hnswgpu_search_noalloc": (C.c_int, [P, P, U64, U64, U64, U32, P, P, P, P, P]),
 }
 
 _lib = None

@@ -1013,6 +1013,28 @@ cudaError_t launch_s(const SearchParams& p, int num_sms, cudaStream_t stream, in
 }
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Fixed scratch for hnswgpu_search_noalloc: the search kernel's work counter,
+// finished-CTA counter and status word, in a file-scope device array instead
+// of memory allocated per index.  Every GPU that loads the library holds these
+// 256 bytes until the process exits; all calls on a device share them.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocScratchWords];
+
+cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
+    // Resolved once per device, with that device current: in host code the
+    // symbol's name is only a host-side stand-in, not a device address.
+    static uint32_t* addr[kMaxDevices] = {nullptr};
+    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+    if (!addr[device]) {
+        void* ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[device] = static_cast<uint32_t*>(ptr);
+    }
+    *out = addr[device];
+    return cudaSuccess;
+}
+
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
     if (space == 0)
         return p.exact ? launch_s<0, true>(p, num_sms, stream, blocks_out)

@@ -54,6 +54,13 @@ struct SearchParams {
     uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;
 };
 
+// Scratch of hnswgpu_search_noalloc: words [0] work counter, [1] finished-CTA
+// counter, [2] status bits; 64 words = 256 bytes.
+constexpr int kNoallocScratchWords = 64;
+constexpr int kMaxDevices = 64;
+// Device address of the fixed scratch on `device`, which must be current.
+cudaError_t noalloc_scratch_address(int device, uint32_t** out);
+
 // Fills the off_* fields and warp_smem from the sizes; returns warp_smem.
 size_t warp_smem_layout(SearchParams& p);
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out);

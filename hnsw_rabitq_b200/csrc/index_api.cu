@@ -406,9 +406,11 @@ int guarded(F fn) {
     }
 }
 
-// One HNSW search launch on device buffers.
-void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
-              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
+// Launch parameters of one HNSW search on device buffers (no allocation;
+// work_counter / done_counter / status are left for the caller to set).
+hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef,
+                                  const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace,
+                                  bool exact) {
     hnswgpu::SearchParams p{};
     p.vecs = h->vecs.p;
     p.links0 = h->links0.p;
@@ -437,7 +439,6 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     p.out_dists = dd;
     p.out_counts = dc;
     p.trace = dtrace;
-    p.status = h->status.p;
     // Staging rows: the 4-lanes-per-row path reads 8 rows per LDS.128 pass, a
     // row pad of 16 floats puts consecutive rows half a bank cycle apart
     // (conflict-free quarter warps); the one-lane-per-row path wants 4.
@@ -465,6 +466,14 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     }
     if (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
+    return p;
+}
+
+// One HNSW search launch on device buffers, scratch from the index.
+void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
+              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
+    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact);
+    p.status = h->status.p;
 #ifdef HNSWGPU_PHASE_TIMING
     static unsigned long long* phase_buf = nullptr;
     if (!phase_buf) {
@@ -690,6 +699,44 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             cudaStreamSynchronize(st);
             return fail(HNSWGPU_ERR_KERNEL, "search kernel timed out waiting for a copy");
         }
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint64_t nq, uint64_t k, uint64_t ef,
+                           uint32_t flags, const uint8_t* d_allow, uint64_t* d_labels, float* d_dists,
+                           int32_t* d_counts, void* stream) {
+    return guarded([&] {
+        if (!h || h->is_bf) return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc needs an HNSW index");
+        if (k == 0 || (nq && (!d_queries || !d_labels || !d_dists || !d_counts)))
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        // The fixed scratch holds one 32-bit work counter: it hands out query
+        // indices, so a call may carry at most 2^31 queries.
+        if (nq > 0x7fffffffull || k > 0xffffffffull)
+            return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc: nq must be < 2^31 (fixed 256-byte scratch)");
+        if (flags & ~(uint32_t)HNSWGPU_EXACT_TIES)
+            return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc: only HNSWGPU_EXACT_TIES may be set");
+        cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
+        if (nq == 0) return HNSWGPU_OK;
+        cudaStream_t st = (cudaStream_t)stream;
+        if (h->count == 0) {
+            cuda_check(cudaMemsetAsync(d_counts, 0, nq * 4, st), "cudaMemsetAsync");
+            cuda_check(cudaMemsetAsync(d_labels, 0xff, nq * k * 8, st), "cudaMemsetAsync");
+            cuda_check(cudaMemsetAsync(d_dists, 0x7f, nq * k * 4, st), "cudaMemsetAsync");
+            return HNSWGPU_OK;
+        }
+        uint32_t* scratch = nullptr;
+        cuda_check(hnswgpu::noalloc_scratch_address(h->device, &scratch), "cudaGetSymbolAddress");
+        hnswgpu::SearchParams p = hnsw_params(h, d_queries, nq, k, ef ? ef : h->ef, d_allow, d_labels, d_dists,
+                                              d_counts, nullptr, (flags & HNSWGPU_EXACT_TIES) != 0);
+        p.work_counter = scratch + 0;
+        p.done_counter = scratch + 1;
+        p.status = scratch + 2;
+        // counters and status must start at zero: clear what a previous call
+        // (or an interrupted one) may have left
+        cuda_check(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), st), "cudaMemsetAsync");
+        cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
+                   "hnsw_search launch");
         return HNSWGPU_OK;
     });
 }

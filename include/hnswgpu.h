@@ -161,6 +161,29 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
                    const hnswgpu_search_opts* opts, uint64_t* out_labels, float* out_dists,
                    int32_t* out_counts);
 
+/* HNSW search that allocates no memory, for callers that cannot call
+ * cudaMalloc: code running under a device-memory budget it does not own (a
+ * framework's caching allocator or a serving process that reserves all of its
+ * memory up front and treats any later allocation as a failure), and code
+ * that must not risk the implicit device synchronisation an allocation or
+ * free can cause.  It has no counterpart in the reference.
+ *
+ * Same search as hnswgpu_search with HNSWGPU_DEVICE_PTRS: queries, outputs and
+ * the optional allow mask are device pointers, `ef` 0 means the index's ef,
+ * flags may only hold HNSWGPU_EXACT_TIES; the call is asynchronous on `stream`.
+ * The kernel's scratch (work counter, finished-CTA counter, status word) is a
+ * fixed 256-byte array in the library's device image instead of per-index
+ * memory; nq >= 2^31 is rejected.  Every GPU that loads the library holds that
+ * array until the process exits.  The first call on a device resolves the
+ * array's device address (cudaGetSymbolAddress with that device current): make
+ * it before any stream capture.  All calls on a device share the array, so
+ * calls that overlap on the GPU (other streams, or a graph replay while
+ * another call runs) race and must not be issued; each call clears the
+ * counters before its launch.  Status bits are not reported by this call. */
+HNSWGPU_API int hnswgpu_search_noalloc(const hnswgpu_index* index, const float* d_queries, uint64_t nq, uint64_t k,
+                                       uint64_t ef, uint32_t flags, const uint8_t* d_allow, uint64_t* d_labels,
+                                       float* d_dists, int32_t* d_counts, void* stream);
+
 /* OR of the kernel status bits raised by searches on this index since the
  * last call (synchronises the index's stream); clears them. */
 HNSWGPU_API int hnswgpu_get_status(hnswgpu_index* index, uint32_t* out_bits);
