@@ -19,6 +19,7 @@ SPACE_L2, SPACE_IP, SPACE_COSINE = 0, 1, 2
 DEVICE_PTRS = 0x1
 TRACE = 0x2
 EXACT_TIES = 0x4
+PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
 STATUS_TIMEOUT = 0x1
 STATUS_OVERFLOW = 0x2
 
@@ -33,7 +34,8 @@ class Info(C.Structure):
 
 
 class SearchOpts(C.Structure):
-    _fields_ = [("flags", U32), ("reserved0", U32), ("ef", U64), ("allow", P), ("trace", P), ("stream", P)]
+    _fields_ = [("flags", U32), ("precision", U32), ("ef", U64), ("allow", P), ("trace", P), ("stream", P),
+                ("rerank", U32), ("reserved1", U32)]
 
 
 SIGNATURES = {
@@ -43,6 +45,7 @@ SIGNATURES = {
     "hnswgpu_load_bf": (C.c_int, [C.c_char_p, C.c_int, U64, C.c_int, C.POINTER(P)]),
     "hnswgpu_create_bf": (C.c_int, [C.c_int, U64, P, P, U64, U64, C.c_int, C.POINTER(P)]),
     "hnswgpu_free": (C.c_int, [P]),
+    "hnswgpu_build_traversal_copy": (C.c_int, [P, U32]),
     "hnswgpu_get_info": (C.c_int, [P, C.POINTER(Info)]),
     "hnswgpu_set_ef": (C.c_int, [P, U64]),
     "hnswgpu_get_labels": (C.c_int, [P, P]),

@@ -31,8 +31,11 @@
 // broken by internal id; on the same index the kernel therefore returns the
 // reference's labels except where distances tie exactly (the oracle's
 // "canonical" mode computes exactly this kernel's result).
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -55,6 +58,49 @@ struct WarpSmem {
     uint64_t* accbuf;    // tie-exact mode: accepted keys of one chunk, link order
     uint64_t* evbuf;     // tie-exact mode: keys evicted from top_candidates
 };
+
+// Optional self-checks (compile with -DHNSWGPU_BOUNDS_CHECK; the shipped
+// library is built without them): every staging copy and staged-row read is
+// checked against the warp's shared-memory layout and the source buffer; the
+// first violation is recorded in g_dbg and the access is skipped (a skipped
+// copy completes its bytes on the mbarrier so the wait stays consistent).
+#ifdef HNSWGPU_BOUNDS_CHECK
+__device__ unsigned long long g_dbg[8];
+__device__ __forceinline__ bool dbg_ok(bool cond, unsigned code, unsigned long long a, unsigned long long b) {
+    if (cond) return true;
+    if (atomicCAS(&g_dbg[0], 0ull, (unsigned long long)code) == 0ull) {
+        g_dbg[1] = a;
+        g_dbg[2] = b;
+        g_dbg[3] = blockIdx.x;
+    }
+    return false;
+}
+__device__ __forceinline__ void mbar_complete_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+#define DBG_OK(cond, code, a, b) dbg_ok((cond), (code), (unsigned long long)(a), (unsigned long long)(b))
+#else
+#define DBG_OK(cond, code, a, b) true
+#endif
+
+// Staging copy with the optional checks: dst must lie in this warp's staging
+// region [stage, pool), src inside [base, base + nrows * row_bytes).
+__device__ __forceinline__ void stage_copy(const SearchParams& p, const WarpSmem& s, void* dst, const void* base,
+                                           uint64_t row, uint64_t nrows, uint32_t row_bytes, unsigned code) {
+    const unsigned char* dp = static_cast<const unsigned char*>(dst);
+    const unsigned char* lo = reinterpret_cast<const unsigned char*>(s.stage);
+    const unsigned char* hi = reinterpret_cast<const unsigned char*>(s.pool);
+    const bool ok = DBG_OK(dp >= lo && dp + row_bytes <= hi && ((uintptr_t)dp & 15) == 0 && (row_bytes & 15) == 0,
+                           code, dp - lo, row_bytes) &&
+                    DBG_OK(row < nrows, code + 1, row, nrows);
+    if (ok) {
+        bulk_g2s(dst, static_cast<const unsigned char*>(base) + row * row_bytes, row_bytes, s.bar);
+    } else {
+#ifdef HNSWGPU_BOUNDS_CHECK
+        mbar_complete_tx(s.bar, row_bytes);
+#endif
+    }
+}
 
 __device__ __forceinline__ bool is_allowed(const SearchParams& p, uint32_t id) {
     if (p.deleted_bits && ((p.deleted_bits[id >> 5] >> (id & 31)) & 1u)) return false;
@@ -199,8 +245,7 @@ __device__ __forceinline__ bool stage_rows(const SearchParams& p, WarpSmem& s, u
     __syncwarp();
     if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)cnt * p.row_bytes);
     __syncwarp();
-    if (mine)
-        bulk_g2s(s.stage + (size_t)slot * p.stage_stride, p.vecs + (size_t)id * p.row_floats, p.row_bytes, s.bar);
+    if (mine) stage_copy(p, s, s.stage + (size_t)slot * p.stage_stride, p.vecs, id, p.count, p.row_bytes, 10);
     bool ok = mbar_wait(s.bar, phase);
     phase ^= 1u;
     return __all_sync(FULL, ok);
@@ -214,6 +259,8 @@ __device__ __forceinline__ float stage_dist(const SearchParams& p, const WarpSme
 struct Counters {
     uint32_t upper_hops, upper_dists, l0_exp, l0_dists;
 };
+
+
 
 // Optional per-phase cycle accounting (compile with -DHNSWGPU_PHASE_TIMING;
 // the shipped library is built without it).  Phases: 0 query setup,
@@ -282,6 +329,37 @@ __device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& 
 // predicted whenever its distance is unique), and its link row, visited-cache
 // update and first TMA batch are issued before the pool merge / heap replay
 // of the current expansion, which then run under that memory latency.
+// Where the rows of one staging batch come from: the float32 rows, or the
+// low-precision traversal copy.
+struct RowSrc {
+    const unsigned char* base;
+    uint32_t row_bytes;    // bytes per row in global memory (= bytes copied)
+    uint32_t stage_bytes;  // staging stride
+    uint32_t slots;        // rows per batch
+};
+
+template <int PREC>
+__device__ __forceinline__ RowSrc trav_src(const SearchParams& p) {
+    if (PREC == 0) return RowSrc{reinterpret_cast<const unsigned char*>(p.vecs), p.row_bytes, p.stage_stride * 4,
+                                 p.stage_slots};
+    return RowSrc{p.tvecs, p.trow_bytes, p.tstage_bytes, p.tslots};
+}
+
+__device__ __forceinline__ bool stage_src(const SearchParams& p, WarpSmem& s, uint32_t& phase, const RowSrc& r,
+                                          bool mine, uint32_t id, int slot, int cnt, int lane) {
+    if (cnt == 0) return true;
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)cnt * r.row_bytes);
+    __syncwarp();
+    if (mine)
+        stage_copy(p, s, reinterpret_cast<unsigned char*>(s.stage) + (size_t)slot * r.stage_bytes, r.base, id,
+                   p.count, r.row_bytes, 20);
+    bool ok = mbar_wait(s.bar, phase);
+    phase ^= 1u;
+    return __all_sync(FULL, ok);
+}
+
 struct Fetch {
     uint32_t id;     // this lane's neighbour id (link order), or INVALID_ID
     bool fresh;      // evaluated now (missed in the visited cache)
@@ -291,7 +369,9 @@ struct Fetch {
     int n0;          // rows of the first staging batch in flight
 };
 
+template <int PREC>
 __device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, uint32_t c, int lane, Fetch& f) {
+    const RowSrc rs = trav_src<PREC>(p);
     const uint32_t* lrow = p.links0 + (size_t)c * p.maxM0;
     const uint32_t id = lane < (int)p.maxM0 ? __ldg(lrow + lane) : INVALID_ID;
     bool fresh = id != INVALID_ID;
@@ -309,15 +389,94 @@ __device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, 
     f.nnew = __popc(f.nmask);
     const int src = (int)__fns(f.nmask, 0, lane + 1);
     f.cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
-    f.n0 = min((int)p.stage_slots, f.nnew);
+    f.n0 = min((int)rs.slots, f.nnew);
     if (f.n0 > 0) {
         fence_proxy_async_smem();
         __syncwarp();
-        if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)f.n0 * p.row_bytes);
+        if (lane == 0) mbar_arrive_expect_tx(s.bar, (uint32_t)f.n0 * rs.row_bytes);
         __syncwarp();
         if (lane < f.n0)
-            bulk_g2s(s.stage + (size_t)lane * p.stage_stride, p.vecs + (size_t)f.cid2 * p.row_floats, p.row_bytes,
-                     s.bar);
+            stage_copy(p, s, reinterpret_cast<unsigned char*>(s.stage) + (size_t)lane * rs.stage_bytes, rs.base,
+                       f.cid2, p.count, rs.row_bytes, 30);
+    }
+}
+
+// Approximate distances from staged low-precision rows [0, n) into the
+// compacted lanes [s0, s0 + n): 4 lanes per row over 16-byte chunks, fp32
+// accumulation in any order (these distances only steer the beam; returned
+// distances come from the float32 re-rank).
+template <int SPACE, int PREC>
+__device__ __forceinline__ void batch_dist_lowp(const SearchParams& p, const WarpSmem& s, int n, int s0, int lane,
+                                                float& dc) {
+    const int a = lane & 3;
+    const int nch = (int)(p.trow_bytes - (PREC == 2 ? 16u : 0u)) / 16;  // 16-byte chunks of data
+    const float4* q4 = reinterpret_cast<const float4*>(s.q);
+    const unsigned char* stage = reinterpret_cast<const unsigned char*>(s.stage);
+    for (int g = 0; g < n; g += 8) {
+        const int v = min(g + (lane >> 2), n - 1);
+        const unsigned char* row = stage + (size_t)v * p.tstage_bytes;
+        if (!DBG_OK(row + p.trow_bytes <= reinterpret_cast<const unsigned char*>(s.pool) && v >= 0, 40,
+                    (size_t)v * p.tstage_bytes, n))
+            row = stage;
+        const uint4* r16 = reinterpret_cast<const uint4*>(row);
+        float acc = 0.f;
+        float sc = 1.f;
+        if (PREC == 2) sc = *reinterpret_cast<const float*>(row + p.trow_bytes - 16);
+        for (int c = a; c < nch; c += 4) {
+            const uint4 raw = r16[c];
+            const uint32_t w[4] = {raw.x, raw.y, raw.z, raw.w};
+            if (PREC == 1) {
+                // 8 bf16 = elements 8c .. 8c+7
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const float4 qv = q4[2 * c + h];
+                    const float x0 = __uint_as_float(w[2 * h] << 16), x1 = __uint_as_float(w[2 * h] & 0xffff0000u);
+                    const float x2 = __uint_as_float(w[2 * h + 1] << 16),
+                                x3 = __uint_as_float(w[2 * h + 1] & 0xffff0000u);
+                    if (SPACE == 0) {
+                        float t0 = qv.x - x0, t1 = qv.y - x1, t2 = qv.z - x2, t3 = qv.w - x3;
+                        acc = fmaf(t0, t0, acc);
+                        acc = fmaf(t1, t1, acc);
+                        acc = fmaf(t2, t2, acc);
+                        acc = fmaf(t3, t3, acc);
+                    } else {
+                        acc = fmaf(qv.x, x0, acc);
+                        acc = fmaf(qv.y, x1, acc);
+                        acc = fmaf(qv.z, x2, acc);
+                        acc = fmaf(qv.w, x3, acc);
+                    }
+                }
+            } else {
+                // 16 e4m3 = elements 16c .. 16c+15
+#pragma unroll
+                for (int h = 0; h < 4; h++) {
+                    const float4 qv = q4[4 * c + h];
+                    const __half2 lo = __half2(__nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[h] & 0xffffu), __NV_E4M3));
+                    const __half2 hi = __half2(__nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[h] >> 16), __NV_E4M3));
+                    const float2 xa = __half22float2(lo), xb = __half22float2(hi);
+                    if (SPACE == 0) {
+                        float t0 = fmaf(sc, xa.x, -qv.x), t1 = fmaf(sc, xa.y, -qv.y), t2 = fmaf(sc, xb.x, -qv.z),
+                              t3 = fmaf(sc, xb.y, -qv.w);
+                        acc = fmaf(t0, t0, acc);
+                        acc = fmaf(t1, t1, acc);
+                        acc = fmaf(t2, t2, acc);
+                        acc = fmaf(t3, t3, acc);
+                    } else {
+                        acc = fmaf(qv.x, xa.x, acc);
+                        acc = fmaf(qv.y, xa.y, acc);
+                        acc = fmaf(qv.z, xb.x, acc);
+                        acc = fmaf(qv.w, xb.y, acc);
+                    }
+                }
+            }
+        }
+        acc += __shfl_xor_sync(FULL, acc, 1);
+        acc += __shfl_xor_sync(FULL, acc, 2);
+        float r = acc;
+        if (SPACE != 0) r = 1.0f - (PREC == 2 ? sc * acc : acc);
+        const int t = lane - s0 - g;
+        const float got = __shfl_sync(FULL, r, (t & 7) << 2);
+        if (t >= 0 && t < 8 && t + g < n) dc = got;
     }
 }
 
@@ -330,6 +489,10 @@ __device__ __forceinline__ void batch_dist(const SearchParams& p, const WarpSmem
     for (int g = 0; g < n; g += 8) {
         const int v = min(g + (lane >> 2), n - 1);
         const float4* x4 = reinterpret_cast<const float4*>(s.stage + (size_t)v * p.stage_stride);
+        if (!DBG_OK(reinterpret_cast<const unsigned char*>(x4) + p.row_bytes <=
+                        reinterpret_cast<const unsigned char*>(s.pool),
+                    50, (size_t)v * p.stage_stride * 4, n))
+            x4 = reinterpret_cast<const float4*>(s.stage);
         float r;
         if (n16 <= 8) {
             // query chunks held in registers (qr[c] = this lane's float4 of chunk c)
@@ -365,24 +528,27 @@ __device__ __forceinline__ void batch_dist(const SearchParams& p, const WarpSmem
 
 // Distances of all fresh neighbours of a fetched list; result in the owning
 // (link-order) lane.
-template <int SPACE>
+template <int SPACE, int PREC>
 __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem& s, uint32_t& phase, const Fetch& f,
                                                 const float4* qr, int lane, float& d, PhaseClock& pc) {
     float dc = __int_as_float(0x7f800000);
+    const RowSrc rs = trav_src<PREC>(p);
     if (f.n0 > 0) {
         const bool ok = mbar_wait(s.bar, phase);
         phase ^= 1u;
         if (!__all_sync(FULL, ok)) return false;
         PT_MARK(4);
-        batch_dist<SPACE>(p, s, qr, f.n0, 0, lane, dc);
+        if (PREC == 0) batch_dist<SPACE>(p, s, qr, f.n0, 0, lane, dc);
+        else batch_dist_lowp<SPACE, PREC>(p, s, f.n0, 0, lane, dc);
         PT_MARK(5);
     }
-    for (int s0 = f.n0; s0 < f.nnew; s0 += (int)p.stage_slots) {
-        const int n = min((int)p.stage_slots, f.nnew - s0);
+    for (int s0 = f.n0; s0 < f.nnew; s0 += (int)rs.slots) {
+        const int n = min((int)rs.slots, f.nnew - s0);
         const bool mine = lane >= s0 && lane < s0 + n;
-        if (!stage_rows(p, s, phase, mine, f.cid2, lane - s0, n, lane)) return false;
+        if (!stage_src(p, s, phase, rs, mine, f.cid2, lane - s0, n, lane)) return false;
         PT_MARK(4);
-        batch_dist<SPACE>(p, s, qr, n, s0, lane, dc);
+        if (PREC == 0) batch_dist<SPACE>(p, s, qr, n, s0, lane, dc);
+        else batch_dist_lowp<SPACE, PREC>(p, s, n, s0, lane, dc);
         PT_MARK(5);
     }
     const int ci = __popc(f.nmask & lanemask_lt());
@@ -390,7 +556,7 @@ __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem&
     return true;
 }
 
-template <int SPACE, bool EXACT>
+template <int SPACE, bool EXACT, int PREC>
 __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
                                PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
                                uint32_t& status) {
@@ -406,13 +572,13 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
     tsz = EXACT ? 1 : 0;
     __syncwarp();
     Fetch f;
-    fetch_links(p, s, ep, lane, f);
+    fetch_links<PREC>(p, s, ep, lane, f);
     ct.l0_exp += 1;
     PT_MARK(3);
     while (true) {
         ct.l0_dists += f.nnew;
         float d;
-        if (!fetch_distances<SPACE>(p, s, phase, f, qr, lane, d, pc)) return false;
+        if (!fetch_distances<SPACE, PREC>(p, s, phase, f, qr, lane, d, pc)) return false;
         // ---- acceptance (closed form of hnswalg.h:395 over the link order)
         const uint32_t dk = fkey(d);
         const bool full = psize == ef;
@@ -477,7 +643,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             }
         }
         Fetch fn;
-        if (have_next || spec) fetch_links(p, s, next, lane, fn);
+        if (have_next || spec) fetch_links<PREC>(p, s, next, lane, fn);
         PT_MARK(2);
         // ---- bookkeeping of this expansion, under the latency of the next fetch
         int nev = 0;
@@ -552,7 +718,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
                 }
                 spec = false;
             }
-            if (!spec) fetch_links(p, s, top_id, lane, fn);
+            if (!spec) fetch_links<PREC>(p, s, top_id, lane, fn);
         } else if (!have_next) {
             break;
         }
@@ -563,7 +729,57 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT>
+// Exact re-rank after a low-precision beam: the best `rerank` pool entries
+// (ordered by approximate distance) get their float32 rows staged (staging
+// area + the now idle visited cache) and their distances recomputed in the
+// reference's summation order; the pool is then re-sorted by the exact
+// (distance, id) keys, so the k returned distances are bit-exact.
+template <int SPACE>
+__device__ bool rerank_fp32(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, const float4* qr,
+                            int& psize) {
+    const int R = min(psize, (int)p.rerank);
+    const RowSrc rs{reinterpret_cast<const unsigned char*>(p.vecs), p.row_bytes, p.stage_stride * 4, p.rr_slots};
+#ifdef HNSWGPU_BOUNDS_CHECK
+    for (int r = lane; r < psize; r += 32)
+        for (int t = 0; t < psize; t++)
+            if (t != r) DBG_OK(kid(s.pool[t]) != kid(s.pool[r]), 120, kid(s.pool[r]), (t << 16) | r);
+    __syncwarp();
+#endif
+    for (int b = 0; b < R; b += (int)rs.slots) {
+        const int nb = min((int)rs.slots, R - b);
+        uint32_t id = lane < nb ? kid(s.pool[b + lane]) : 0u;
+        if (!DBG_OK(id < p.count && b + lane < (int)p.pool_cap, 70, id, b + lane)) id = 0;
+        if (!stage_src(p, s, phase, rs, lane < nb, id, lane, nb, lane)) return false;
+        float dc = 0.f;
+        batch_dist<SPACE>(p, s, qr, nb, 0, lane, dc);
+        __syncwarp();
+        if (lane < nb) s.pool[b + lane] = mkkey(dc, id);
+        __syncwarp();
+    }
+#ifdef HNSWGPU_BOUNDS_CHECK
+    for (int r = lane; r < R; r += 32)
+        for (int t = 0; t < R; t++)
+            if (t != r) DBG_OK(s.pool[t] != s.pool[r], 130, s.pool[r], (t << 16) | r);
+    __syncwarp();
+#endif
+    // rank by counting; the staging area is free again and holds the result
+    uint64_t* tmp = reinterpret_cast<uint64_t*>(s.stage);
+    for (int r = lane; r < R; r += 32) {
+        const uint64_t kr = s.pool[r];
+        int rank = 0;
+        for (int t = 0; t < R; t++) rank += s.pool[t] < kr;
+        if (DBG_OK(rank < R && reinterpret_cast<unsigned char*>(tmp + rank + 1) <= reinterpret_cast<unsigned char*>(s.pool),
+                   60, rank, R))
+            tmp[rank] = kr;
+    }
+    __syncwarp();
+    for (int r = lane; r < R; r += 32) s.pool[r] = tmp[r];
+    __syncwarp();
+    psize = R;
+    return true;
+}
+
+template <int SPACE, bool FAST16, bool EXACT, int PREC>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
                            Counters& ct, PhaseClock& pc) {
     pc.start();
@@ -636,7 +852,17 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     const bool pipe = FAST16 && bare && p.maxM0 <= 32;
     if (pipe) {
         float d0;
-        if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0, pc)) return false;
+        if (PREC == 0) {
+            if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0, pc)) return false;
+        } else {
+            // every pool key of a low-precision beam must come from the same
+            // (approximate) arithmetic: a node re-reached after a visited-cache
+            // miss is recognised by its exact (distance, id) key
+            const RowSrc rs = trav_src<PREC>(p);
+            if (!stage_src(p, s, phase, rs, lane == 0, cur, 0, 1, lane)) return false;
+            d0 = 0.f;
+            batch_dist_lowp<SPACE, PREC>(p, s, 1, 0, lane, d0);
+        }
         d0 = __shfl_sync(FULL, d0, 0);
         ct.l0_dists += 1;
         if (lane == 0) s.vis[vis_slot(cur, p.log2_vis)] = cur;
@@ -646,7 +872,9 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
 #pragma unroll
         for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
-        if (!base_pipelined<SPACE, EXACT>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status)) return false;
+        if (!base_pipelined<SPACE, EXACT, PREC>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status))
+            return false;
+        if (PREC != 0 && !rerank_fp32<SPACE>(p, s, phase, lane, qr, psize)) return false;
     } else {
     if (bare || is_allowed(p, cur)) {
         float d0;
@@ -865,17 +1093,21 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     float* odist = p.out_dists + (size_t)qi * k;
     for (int r = lane; r < kk; r += 32) {
         uint64_t e = s.pool[r];
+        if (!DBG_OK(kid(e) < p.count, 80 + (PREC << 2), kid(e), r)) e = 0;
         uint32_t dk = khi(e);
         uint64_t lab = p.labels[kid(e)];
         int st = r;
         while (st > 0 && khi(s.pool[st - 1]) == dk) st--;
         int below = 0;
         for (int t = st; t < kk && khi(s.pool[t]) == dk; t++) {
-            uint64_t lt = p.labels[kid(s.pool[t])];
+            const uint32_t tid = kid(s.pool[t]);
+            uint64_t lt = DBG_OK(tid < p.count, 90, tid, t) ? p.labels[tid] : 0;
             if (t != r && (lt < lab || (lt == lab && t < r))) below++;
         }
-        olab[st + below] = lab;
-        odist[st + below] = funkey(dk);
+        if (DBG_OK(st + below < kk, 100, st + below, kk)) {
+            olab[st + below] = lab;
+            odist[st + below] = funkey(dk);
+        }
     }
     for (int r = kk + lane; r < (int)k; r += 32) {
         olab[r] = ~0ull;
@@ -889,7 +1121,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT>
+template <int SPACE, bool FAST16, bool EXACT, int PREC>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -916,7 +1148,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_k
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE, FAST16, EXACT>(p, s, phase, qi, lane, ct, pc)) {
+        if (!search_one<SPACE, FAST16, EXACT, PREC>(p, s, phase, qi, lane, ct, pc)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
@@ -954,8 +1186,15 @@ size_t warp_smem_layout(SearchParams& p) {
     p.off_query = (uint32_t)off;
     off += (size_t)p.row_floats * 4;
     off = (off + 15) & ~(size_t)15;
+    // staging area followed by the visited cache: after the beam the two
+    // together stage the float32 rows of the re-rank
     p.off_stage = (uint32_t)off;
-    off += (size_t)p.stage_slots * p.stage_stride * 4;
+    size_t stage = (size_t)p.stage_slots * p.stage_stride * 4;
+    if (p.prec) stage = std::max(stage, (size_t)p.tslots * p.tstage_bytes);
+    off += (stage + 15) & ~(size_t)15;
+    p.off_vis = (uint32_t)off;
+    off += ((size_t)1 << p.log2_vis) * 4;
+    p.rr_slots = p.prec ? (uint32_t)std::min<size_t>(32, (off - p.off_stage) / ((size_t)p.stage_stride * 4)) : 0;
     off = (off + 7) & ~(size_t)7;
     p.off_pool = (uint32_t)off;
     off += (size_t)p.pool_cap * 8;
@@ -969,22 +1208,19 @@ size_t warp_smem_layout(SearchParams& p) {
     off += p.exact ? 32 * 8 : 0;
     p.off_extra = (uint32_t)off;
     off += (size_t)p.extra_cap * 8;
-    off = (off + 15) & ~(size_t)15;
-    p.off_vis = (uint32_t)off;
-    off += ((size_t)1 << p.log2_vis) * 4;
     off = (off + 127) & ~(size_t)127;
     p.warp_smem = (uint32_t)off;
     return off;
 }
 
 namespace {
-template <int SPACE, bool FAST16, bool EXACT>
+template <int SPACE, bool FAST16, bool EXACT, int PREC>
 cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
     // per-instantiation cache of the opt-in shared-memory size and occupancy
     static int attr_smem = -1;
     static size_t occ_smem = 0;
     static int occ_per_sm = 0;
-    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT>;
+    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC>;
     const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
     if ((int)smem > attr_smem) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1002,16 +1238,32 @@ cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, in
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    hnsw_search_kernel<SPACE, FAST16, EXACT><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     return cudaGetLastError();
 }
 
 template <int SPACE, bool EXACT>
 cudaError_t launch_s(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
-    return p.fast16 ? launch_t<SPACE, true, EXACT>(p, num_sms, stream, blocks_out)
-                    : launch_t<SPACE, false, EXACT>(p, num_sms, stream, blocks_out);
+    return p.fast16 ? launch_t<SPACE, true, EXACT, 0>(p, num_sms, stream, blocks_out)
+                    : launch_t<SPACE, false, EXACT, 0>(p, num_sms, stream, blocks_out);
+}
+
+template <int SPACE>
+cudaError_t launch_lowp(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    // low-precision traversal: dim % 16 == 0, id tie order (checked by the host)
+    return p.prec == 1 ? launch_t<SPACE, true, false, 1>(p, num_sms, stream, blocks_out)
+                       : launch_t<SPACE, true, false, 2>(p, num_sms, stream, blocks_out);
 }
 }  // namespace
+
+#ifdef HNSWGPU_BOUNDS_CHECK
+cudaError_t read_debug_record(unsigned long long* out) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_dbg, sizeof(unsigned long long) * 8);
+    if (e != cudaSuccess) return e;
+    unsigned long long z[8] = {0};
+    return cudaMemcpyToSymbol(g_dbg, z, sizeof(z));
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // Fixed scratch for hnswgpu_search_noalloc: the search kernel's work counter,
@@ -1036,6 +1288,8 @@ cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
 }
 
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (p.prec) return space == 0 ? launch_lowp<0>(p, num_sms, stream, blocks_out)
+                                  : launch_lowp<1>(p, num_sms, stream, blocks_out);
     if (space == 0)
         return p.exact ? launch_s<0, true>(p, num_sms, stream, blocks_out)
                        : launch_s<0, false>(p, num_sms, stream, blocks_out);

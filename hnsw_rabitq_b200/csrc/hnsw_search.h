@@ -49,6 +49,14 @@ struct SearchParams {
     uint32_t* done_counter;       // blocks finished (same slot discipline)
     uint32_t* status;
     unsigned long long* phase_cycles;  // 10 counters, profiling builds only (may be null)
+    // low-precision traversal (prec 1 = bf16, 2 = fp8 e4m3 + per-row scale)
+    uint32_t prec;
+    const unsigned char* tvecs;  // traversal rows, tstride bytes apart
+    uint32_t trow_bytes;         // bytes copied per traversal row (16-multiple)
+    uint32_t tstage_bytes;       // staging stride of a traversal row
+    uint32_t tslots;             // traversal rows per staging batch
+    uint32_t rerank;             // best candidates re-ranked with fp32 distances
+    uint32_t rr_slots;           // fp32 rows per re-rank staging batch
     // per-warp shared memory layout
     uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
     uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;
@@ -63,6 +71,14 @@ cudaError_t noalloc_scratch_address(int device, uint32_t** out);
 
 // Fills the off_* fields and warp_smem from the sizes; returns warp_smem.
 size_t warp_smem_layout(SearchParams& p);
+
+// Low-precision traversal copies (quantize.cu).  Row layouts:
+//   bf16: dim x bf16, zero padded to a 16-byte multiple;
+//   fp8 : dim x e4m3 (value / scale, scale = max|x| / 448), zero padded to a
+//         16-byte multiple, then 16 bytes holding the float scale.
+uint32_t traversal_row_bytes(uint32_t prec, uint32_t dim);
+cudaError_t launch_quantize_rows(const float* src, uint32_t count, uint32_t dim, uint32_t src_stride, uint32_t prec,
+                                 unsigned char* dst, cudaStream_t stream);
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out);
 
 }  // namespace hnswgpu

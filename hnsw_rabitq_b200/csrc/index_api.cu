@@ -19,6 +19,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <memory>
@@ -105,10 +106,11 @@ struct hnswgpu_index {
     DevBuf<unsigned char> io;  // host-pointer calls: queries + outputs
     DevBuf<uint8_t> allow;
     DevBuf<float> bf_norms;    // brute force: per-row helper values
+    DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
     std::mutex mu;
     uint64_t device_bytes() const {
         return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
-               dlabels.bytes() + bf_norms.bytes();
+               dlabels.bytes() + bf_norms.bytes() + tcopy[1].bytes() + tcopy[2].bytes();
     }
 };
 
@@ -406,11 +408,22 @@ int guarded(F fn) {
     }
 }
 
+void ensure_traversal_copy(hnswgpu_index* h, uint32_t prec) {
+    if (prec != 1 && prec != 2) throw ApiError(HNSWGPU_ERR_ARG, "precision must be HNSWGPU_PREC_BF16 or _FP8");
+    if (h->tcopy[prec].p || h->count == 0) return;
+    const uint32_t rb = hnswgpu::traversal_row_bytes(prec, (uint32_t)h->dim);
+    h->tcopy[prec].alloc(h->count * rb);
+    cuda_check(hnswgpu::launch_quantize_rows(h->vecs.p, (uint32_t)h->count, (uint32_t)h->dim, h->row_floats, prec,
+                                             h->tcopy[prec].p, h->stream),
+               "quantize launch");
+    cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+}
+
 // Launch parameters of one HNSW search on device buffers (no allocation;
 // work_counter / done_counter / status are left for the caller to set).
 hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef,
                                   const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace,
-                                  bool exact) {
+                                  bool exact, uint32_t prec = 0, uint32_t rerank = 0) {
     hnswgpu::SearchParams p{};
     p.vecs = h->vecs.p;
     p.links0 = h->links0.p;
@@ -453,6 +466,27 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     // the reference's candidate heap is never pruned; it peaks near 8 x ef
     p.cand_cap = exact ? std::max<uint32_t>(256u, 10u * p.ef) : 0u;
     p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
+    if (prec) {
+        if (!p.fast16 || !p.bare || p.maxM0 > 32 || exact)
+            throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
+                           "low-precision traversal needs dim % 16 == 0, maxM0 <= 32, no filter / deletes and the id "
+                           "tie order");
+        if (!h->tcopy[prec].p) throw ApiError(HNSWGPU_ERR_ARG, "traversal copy not built");
+        p.prec = prec;
+        p.tvecs = h->tcopy[prec].p;
+        p.trow_bytes = hnswgpu::traversal_row_bytes(prec, (uint32_t)h->dim);
+        // staging stride: a multiple of 64 bytes with an odd count of 64-byte
+        // units, so the two rows a quarter warp reads hit disjoint bank halves
+        uint32_t st = (p.trow_bytes + 63) / 64;
+        if ((st & 1) == 0) st++;
+        p.tstage_bytes = st * 64;
+        p.tslots = prec == 2 ? 32u : 16u;
+        p.stage_slots = 8;  // float32 rows: upper-layer descent and re-rank batches
+        p.rerank = (uint32_t)std::max<uint64_t>(k, rerank ? std::min<uint64_t>(rerank, p.ef) : p.ef);
+#ifdef HNSWGPU_BOUNDS_CHECK
+        if (getenv("HNSWGPU_DEBUG_NO_RERANK")) p.rerank = 0;
+#endif
+    }
     size_t ws = hnswgpu::warp_smem_layout(p);
     int max_optin = 0;
     cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
@@ -471,8 +505,10 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
 
 // One HNSW search launch on device buffers, scratch from the index.
 void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
-              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
-    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact);
+              uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact, uint32_t prec,
+              uint32_t rerank) {
+    if (prec) ensure_traversal_copy(h, prec);
+    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank);
     p.status = h->status.p;
 #ifdef HNSWGPU_PHASE_TIMING
     static unsigned long long* phase_buf = nullptr;
@@ -491,7 +527,8 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
 }
 
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
-                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact) {
+                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
+                uint32_t prec = 0, uint32_t rerank = 0) {
     if (h->is_bf) {
         hnswgpu::BfParams b{};
         b.vecs = h->vecs.p;
@@ -511,11 +548,17 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
         cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
                    "bf_search launch");
     } else {
-        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact);
+        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank);
     }
 }
 
 }  // namespace
+
+#ifdef HNSWGPU_BOUNDS_CHECK
+namespace hnswgpu {
+cudaError_t read_debug_record(unsigned long long* out);
+}
+#endif
 
 extern "C" {
 
@@ -560,6 +603,16 @@ int hnswgpu_create_bf(int space, uint64_t dim, const float* data, const uint64_t
         init_common(h.get(), device);
         create_bf_from_rows(h.get(), space, dim, data, labels, n, max_elements);
         *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_build_traversal_copy(hnswgpu_index* h, uint32_t precision) {
+    return guarded([&] {
+        if (!h || h->is_bf) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        ensure_traversal_copy(h, precision);
         return HNSWGPU_OK;
     });
 }
@@ -665,7 +718,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         }
         if (dev) {
             run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
-                       want_trace ? o.trace : nullptr, st, exact);
+                       want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank);
             return HNSWGPU_OK;
         }
         // host pointers: stage through the index's device I/O buffer
@@ -686,7 +739,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             dallow = h->allow.p;
         }
         cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact);
+        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact, o.precision, o.rerank);
         cuda_check(cudaMemcpyAsync(out_labels, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
@@ -754,6 +807,14 @@ int hnswgpu_get_status(hnswgpu_index* h, uint32_t* out_bits) {
         return HNSWGPU_OK;
     });
 }
+
+#ifdef HNSWGPU_BOUNDS_CHECK
+// Self-checking builds only: first recorded violation (code, a, b, block).
+HNSWGPU_API int hnswgpu_debug_record(unsigned long long* out) {
+    cudaDeviceSynchronize();
+    return hnswgpu::read_debug_record(out) == cudaSuccess ? HNSWGPU_OK : HNSWGPU_ERR_CUDA;
+}
+#endif
 
 #ifdef HNSWGPU_PHASE_TIMING
 // Profiling builds only: per-phase cycle totals of all searches since the

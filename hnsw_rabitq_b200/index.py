@@ -22,6 +22,7 @@ import numpy as np
 from . import _capi
 
 _SPACES = {"l2": _capi.SPACE_L2, "ip": _capi.SPACE_IP, "cosine": _capi.SPACE_COSINE}
+_PRECISIONS = {"fp32": _capi.PREC_FP32, "bf16": _capi.PREC_BF16, "fp8": _capi.PREC_FP8}
 
 
 def _input_rows(data) -> np.ndarray:
@@ -100,7 +101,8 @@ class _GpuIndex:
         self._filter_cache = (filter, mask)
         return mask
 
-    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False, exact_ties: bool = False):
+    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False, exact_ties: bool = False,
+                precision: str = "fp32", rerank: int = 0):
         self._require()
         q = _input_rows(data)
         if q.shape[1] != self.dim:
@@ -114,7 +116,9 @@ class _GpuIndex:
         counts = np.empty(nq, np.int32)
         opts = _capi.SearchOpts()
         opts.ef = int(ef)
-        if exact_ties:
+        opts.precision = _PRECISIONS[precision]
+        opts.rerank = int(rerank)
+        if exact_ties and opts.precision == _capi.PREC_FP32:
             opts.flags |= _capi.EXACT_TIES
         mask = self._allow_mask(filter)
         opts.allow = mask.ctypes.data if mask is not None else None
@@ -166,6 +170,11 @@ class Index(_GpuIndex):
         # (results identical to searchKnn); "id": ties break by internal id
         # (identical except where distances tie exactly; faster).
         self.tie_order = "reference"
+        # traversal copy: "fp32" (the reference's search), or "bf16" / "fp8"
+        # (approximate beam over a low-precision copy, then the best `rerank`
+        # candidates, default ef, re-ranked with exact float32 distances)
+        self.precision = "fp32"
+        self.rerank = 0
 
     def __repr__(self):
         return f"<hnsw_rabitq_b200.Index(space='{self.space}', dim={self.dim})>"
@@ -228,18 +237,23 @@ class Index(_GpuIndex):
         """(labels uint64 [N, k], distances float32 [N, k]), closest first
         (bindings.cpp:612-697).  Raises RuntimeError when a query has fewer
         than k results, with the reference's message."""
-        labels, dists, counts, _ = self._search(data, k, filter, exact_ties=self.tie_order == "reference")
+        labels, dists, counts, _ = self._search(data, k, filter, exact_ties=self.tie_order == "reference",
+                                                precision=self.precision, rerank=self.rerank)
         if counts.size and counts.min() < k:
             raise RuntimeError(
                 "Cannot return the results in a contiguous 2D array. Probably ef or M is too small")
         return labels, dists
 
-    def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0, tie_order: Optional[str] = None):
+    def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0, tie_order: Optional[str] = None,
+                         precision: Optional[str] = None, rerank: Optional[int] = None):
         """knn_query plus per-query work counters [upper link lists read,
         upper distances, level-0 expansions, level-0 distances] and counts;
         no exception for short results."""
         order = tie_order or self.tie_order
-        return self._search(data, k, filter, ef=ef, trace=True, exact_ties=order == "reference")
+        prec = precision or self.precision
+        rr = self.rerank if rerank is None else rerank
+        return self._search(data, k, filter, ef=ef, trace=True, exact_ties=order == "reference", precision=prec,
+                            rerank=rr)
 
 
 class BFIndex(_GpuIndex):

@@ -84,7 +84,11 @@ typedef struct hnswgpu_info {
 
 typedef struct hnswgpu_search_opts {
     uint32_t flags;            /* HNSWGPU_DEVICE_PTRS | HNSWGPU_TRACE           */
-    uint32_t reserved0;
+    uint32_t precision;        /* HNSW traversal copy: HNSWGPU_PREC_FP32 (the
+                                  reference's search), _BF16 or _FP8; the
+                                  low-precision forms re-rank the best
+                                  `rerank` candidates with exact FP32
+                                  distances before returning k.                */
     uint64_t ef;               /* 0: use the index's ef_ (setEf)               */
     const uint8_t* allow;      /* optional per-internal-id byte mask: nonzero =
                                   the filter functor accepts that node's label.
@@ -95,7 +99,14 @@ typedef struct hnswgpu_search_opts {
                                   level-0 expansions, level-0 distances.
                                   Same memory kind as the queries.            */
     void* stream;              /* cudaStream_t; NULL = the index's own stream  */
+    uint32_t rerank;           /* low precision: candidates re-ranked (0: ef)  */
+    uint32_t reserved1;
 } hnswgpu_search_opts;
+
+/* traversal precisions (hnswgpu_search_opts.precision) */
+#define HNSWGPU_PREC_FP32 0u
+#define HNSWGPU_PREC_BF16 1u      /* bf16 copy of every vector                  */
+#define HNSWGPU_PREC_FP8 2u       /* e4m3 copy with one fp32 scale per vector   */
 
 /* Message of this thread's last failure ("" if none). */
 HNSWGPU_API const char* hnswgpu_last_error(void);
@@ -125,6 +136,13 @@ HNSWGPU_API int hnswgpu_load_bf(const char* path, int space, uint64_t dim, int d
  * does (python_bindings/bindings.cpp:241-248, 790-800). */
 HNSWGPU_API int hnswgpu_create_bf(int space, uint64_t dim, const float* data, const uint64_t* labels, uint64_t n,
                                   uint64_t max_elements, int device, hnswgpu_index** out);
+
+/* Build (once) the low-precision traversal copy of an HNSW index's vectors
+ * (precision HNSWGPU_PREC_BF16 or HNSWGPU_PREC_FP8), derived on the GPU from
+ * the resident float32 rows.  Searches with that precision build it on first
+ * use; calling this first keeps the allocation out of the timed path.  No
+ * counterpart in the reference (which searches float32 only). */
+HNSWGPU_API int hnswgpu_build_traversal_copy(hnswgpu_index* index, uint32_t precision);
 
 /* Release the index and its device memory. */
 HNSWGPU_API int hnswgpu_free(hnswgpu_index* index);
