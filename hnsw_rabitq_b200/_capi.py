@@ -19,6 +19,11 @@ SPACE_L2, SPACE_IP, SPACE_COSINE = 0, 1, 2
 DEVICE_PTRS = 0x1
 TRACE = 0x2
 EXACT_TIES = 0x4
+LEARNED_STOP = 0x8
+EXACT_SCAN = 0x10
+TERM_FEATURES = 6
+TERM_HIDDEN = 64
+TERM_PARAMS = 4685
 PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
 STATUS_TIMEOUT = 0x1
 STATUS_OVERFLOW = 0x2
@@ -38,6 +43,11 @@ class SearchOpts(C.Structure):
                 ("rerank", U32), ("reserved1", U32)]
 
 
+class TermTrainOpts(C.Structure):
+    _fields_ = [("epochs", U32), ("batch", U32), ("lr", C.c_float), ("pos_weight", C.c_float),
+                ("weight_decay", C.c_float), ("reserved", U32), ("seed", U64)]
+
+
 SIGNATURES = {
     "hnswgpu_last_error": (C.c_char_p, []),
     "hnswgpu_version": (C.c_char_p, []),
@@ -54,6 +64,11 @@ SIGNATURES = {
     "hnswgpu_search": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_get_status": (C.c_int, [P, C.POINTER(U32)]),
     "hnswgpu_search_noalloc": (C.c_int, [P, P, U64, U64, U64, U32, P, P, P, P, P]),
+    "hnswgpu_set_termination_model": (C.c_int, [P, P, U32, C.c_float]),
+    "hnswgpu_search_checkpoints": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), U32, U32, P, P, P, P, P, P]),
+    "hnswgpu_term_train": (C.c_int, [C.c_int, P, P, U64, C.POINTER(TermTrainOpts), P, P]),
+    "hnswgpu_term_loss_grad": (C.c_int, [C.c_int, P, P, P, U64, C.c_float, P, P]),
+    "hnswgpu_term_logits": (C.c_int, [C.c_int, P, P, U64, P]),
 }
 
 _lib = None

@@ -32,6 +32,7 @@
 // reference's labels except where distances tie exactly (the oracle's
 // "canonical" mode computes exactly this kernel's result).
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
@@ -41,6 +42,7 @@
 #include "device_common.cuh"
 #include "hnsw_search.h"
 #include "ref_heap.h"
+#include "term_mlp.cuh"
 
 namespace hnswgpu {
 
@@ -556,11 +558,13 @@ __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem&
     return true;
 }
 
-template <int SPACE, bool EXACT, int PREC>
+template <int SPACE, bool EXACT, int PREC, int TERM>
 __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
                                PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
-                               uint32_t& status) {
+                               uint32_t& status, uint32_t qi, float qn) {
     const int ef = (int)p.ef;
+    const int kq = (int)p.k;
+    uint32_t last_change = 0, nckpt = 0;  // learned termination state
     const int pcap = (int)p.pool_cap;
     int hint_p = 0, csz = 0;
     // the entry point is pushed and popped at once (hnswalg.h:325-359)
@@ -601,6 +605,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         }
         const bool accept = live && cntP + cntN < ef;
         const unsigned pmask = __ballot_sync(FULL, accept);
+        if (TERM && __any_sync(FULL, accept && cntP + cntN < kq)) last_change = ct.l0_exp;
         PT_MARK(6);
         // ---- the next candidate
         uint64_t kmin = accept ? key : ~0ull;  // smallest accepted key
@@ -610,12 +615,13 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             kmin = other < kmin ? other : kmin;
         }
         bool have_next = false, spec = false;
-        uint32_t next = INVALID_ID;
+        uint32_t next = INVALID_ID, next_dk = 0xffffffffu;
         if (!EXACT) {
             int ip = find_unexpanded(s.pool, psize, hint_p, lane);
             const uint64_t kp = ip >= 0 ? (s.pool[ip] & KEY_MASK) : ~0ull;
             if (kp != ~0ull || kmin != ~0ull) {
                 have_next = true;
+                next_dk = khi(kmin < kp ? kmin : kp);
                 if (kmin < kp) {
                     next = (uint32_t)kmin;
                     if (accept && key == kmin) key |= EXP_BIT;  // inserted already expanded
@@ -684,6 +690,33 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
         }
         PT_MARK(8);
+        if (TERM && have_next && ct.l0_exp % p.term_period == 0) {
+            // checkpoint: features of the state after this expansion
+            const int kk = min(kq, psize);
+            const float d1 = funkey(khi(s.pool[0]));
+            const float dk = funkey(khi(s.pool[kk - 1]));
+            const float dn = funkey(next_dk);
+            float fe[kTermFeatures];
+            term_features((float)ct.l0_exp, d1, dk, dn, d0, qn, (float)(ct.l0_exp - last_change),
+                          1.0f / (float)p.term_period, fe);
+            if (TERM == 1) {
+                if (nckpt < p.term_max_ckpt) {
+                    const size_t row = (size_t)qi * p.term_max_ckpt + nckpt;
+                    if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
+                    for (int i = lane; i < kq; i += 32)
+                        p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+                }
+                nckpt++;
+            } else if (term_logit(p.term_model, fe, lane) > p.term_logit) {
+                // confident that the top-k is final: drain the prefetched
+                // expansion and stop
+                if (fn.n0 > 0) {
+                    mbar_wait(s.bar, phase);
+                    phase ^= 1u;
+                }
+                break;
+            }
+        }
         if (EXACT) {
             // the reference's loop head: top of candidate_set vs lowerBound
             bool go = false;
@@ -726,6 +759,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         ct.l0_exp += 1;
         PT_MARK(2);
     }
+    if (TERM == 1 && lane == 0) p.ckpt_count[qi] = min(nckpt, p.term_max_ckpt);
     return true;
 }
 
@@ -779,7 +813,7 @@ __device__ bool rerank_fp32(const SearchParams& p, WarpSmem& s, uint32_t& phase,
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
                            Counters& ct, PhaseClock& pc) {
     pc.start();
@@ -871,8 +905,15 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         const float4* q4 = reinterpret_cast<const float4*>(s.q);
 #pragma unroll
         for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float qn = 0.f;
+        if (TERM) {  // |q|^2, a feature of the termination network
+            for (uint32_t i = lane; i < p.dim; i += 32) qn = fmaf(s.q[i], s.q[i], qn);
+#pragma unroll
+            for (int o = 16; o; o >>= 1) qn += __shfl_xor_sync(FULL, qn, o);
+        }
         __syncwarp();
-        if (!base_pipelined<SPACE, EXACT, PREC>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status))
+        if (!base_pipelined<SPACE, EXACT, PREC, TERM>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status,
+                                                      qi, qn))
             return false;
         if (PREC != 0 && !rerank_fp32<SPACE>(p, s, phase, lane, qr, psize)) return false;
     } else {
@@ -1121,7 +1162,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1148,7 +1189,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_k
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE, FAST16, EXACT, PREC>(p, s, phase, qi, lane, ct, pc)) {
+        if (!search_one<SPACE, FAST16, EXACT, PREC, TERM>(p, s, phase, qi, lane, ct, pc)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
@@ -1214,13 +1255,13 @@ size_t warp_smem_layout(SearchParams& p) {
 }
 
 namespace {
-template <int SPACE, bool FAST16, bool EXACT, int PREC>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0>
 cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
     // per-instantiation cache of the opt-in shared-memory size and occupancy
     static int attr_smem = -1;
     static size_t occ_smem = 0;
     static int occ_per_sm = 0;
-    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC>;
+    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM>;
     const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
     if ((int)smem > attr_smem) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1238,7 +1279,7 @@ cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, in
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -1253,6 +1294,19 @@ cudaError_t launch_lowp(const SearchParams& p, int num_sms, cudaStream_t stream,
     // low-precision traversal: dim % 16 == 0, id tie order (checked by the host)
     return p.prec == 1 ? launch_t<SPACE, true, false, 1>(p, num_sms, stream, blocks_out)
                        : launch_t<SPACE, true, false, 2>(p, num_sms, stream, blocks_out);
+}
+// learned termination (id tie order, pipelined beam; checked by the host)
+template <int SPACE, int TERM>
+cudaError_t launch_term_p(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    return p.prec == 0   ? launch_t<SPACE, true, false, 0, TERM>(p, num_sms, stream, blocks_out)
+           : p.prec == 1 ? launch_t<SPACE, true, false, 1, TERM>(p, num_sms, stream, blocks_out)
+                         : launch_t<SPACE, true, false, 2, TERM>(p, num_sms, stream, blocks_out);
+}
+
+template <int SPACE>
+cudaError_t launch_term(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    return p.term_mode == 1 ? launch_term_p<SPACE, 1>(p, num_sms, stream, blocks_out)
+                            : launch_term_p<SPACE, 2>(p, num_sms, stream, blocks_out);
 }
 }  // namespace
 
@@ -1288,6 +1342,8 @@ cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
 }
 
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (p.term_mode) return space == 0 ? launch_term<0>(p, num_sms, stream, blocks_out)
+                                       : launch_term<1>(p, num_sms, stream, blocks_out);
     if (p.prec) return space == 0 ? launch_lowp<0>(p, num_sms, stream, blocks_out)
                                   : launch_lowp<1>(p, num_sms, stream, blocks_out);
     if (space == 0)

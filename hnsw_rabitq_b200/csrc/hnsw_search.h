@@ -14,6 +14,38 @@ namespace hnswgpu {
 #define HNSWGPU_MINB 16
 #endif
 constexpr int kWarpsPerBlock = HNSWGPU_WPB;  // independent query warps per CTA
+// Early-termination network: kTermFeatures -> kTermHidden -> kTermHidden -> 1.
+constexpr int kTermFeatures = 6;
+constexpr int kTermHidden = 64;
+// Packed float32 parameters, in this order:
+//   mu[6], inv_sigma[6] (feature standardisation),
+//   W1[64][6], b1[64], W2[64][64], b2[64], w3[64], b3[1].
+constexpr int kTermOffMu = 0;
+constexpr int kTermOffInvSigma = kTermOffMu + kTermFeatures;
+constexpr int kTermOffW1 = kTermOffInvSigma + kTermFeatures;
+constexpr int kTermOffB1 = kTermOffW1 + kTermHidden * kTermFeatures;
+constexpr int kTermOffW2 = kTermOffB1 + kTermHidden;
+constexpr int kTermOffB2 = kTermOffW2 + kTermHidden * kTermHidden;
+constexpr int kTermOffW3 = kTermOffB2 + kTermHidden;
+constexpr int kTermOffB3 = kTermOffW3 + kTermHidden;
+constexpr int kTermParams = kTermOffB3 + 1;
+// Inference form (device): float mu[6], inv_sigma[6], b1[64], b2[64], b3,
+// pad[3] (kTermPackedFloats floats), then half W1[64][6], W2[64][64], w3[64].
+constexpr int kTermPackedFloats = 2 * kTermFeatures + 2 * kTermHidden + 4;
+constexpr int kTermPackedHalves = kTermHidden * kTermFeatures + kTermHidden * kTermHidden + kTermHidden;
+constexpr size_t kTermPackedBytes = (size_t)kTermPackedFloats * 4 + (size_t)kTermPackedHalves * 2;
+// Convert the float32 parameter vector (kTermParams) into the inference form.
+void pack_term_model(const float* params, unsigned char* out);
+// Training side (term_train.cu), host pointers, current device:
+// mean loss and its gradient over n samples;
+cudaError_t term_loss_grad(const float* params, const float* feats, const float* labels, uint64_t n,
+                           float pos_weight, float* out_loss, float* out_grad);
+// Adam over shuffled mini-batches, params updated in place;
+cudaError_t term_train(const float* feats, const float* labels, uint64_t n, float* params, uint32_t epochs,
+                       uint32_t batch, float lr, float pos_weight, float weight_decay, uint64_t seed,
+                       float* out_epoch_loss);
+// logits of the search's in-warp inference (fp16 weights) for n feature rows.
+cudaError_t term_logits(const float* params, const float* feats, uint64_t n, float* out);
 constexpr int kMinBlocks = HNSWGPU_MINB;     // launch bound: resident CTAs per SM
 constexpr uint32_t HNSWGPU_STATUS_TIMEOUT_BIT = 0x1u;
 constexpr uint32_t HNSWGPU_STATUS_OVERFLOW_BIT = 0x2u;
@@ -49,6 +81,15 @@ struct SearchParams {
     uint32_t* done_counter;       // blocks finished (same slot discipline)
     uint32_t* status;
     unsigned long long* phase_cycles;  // 10 counters, profiling builds only (may be null)
+    // learned early termination (mode 1 = record checkpoints, 2 = stop early)
+    uint32_t term_mode;
+    uint32_t term_period;        // expansions between checkpoints (T)
+    uint32_t term_max_ckpt;      // checkpoint rows per query (trace mode)
+    float* ckpt_feat;            // trace: nq x max_ckpt x kTermFeatures
+    uint32_t* ckpt_ids;          // trace: nq x max_ckpt x k internal ids of the current top-k
+    uint32_t* ckpt_count;        // trace: checkpoints written per query
+    const float* term_model;     // learned: packed network (see term_model_layout)
+    float term_logit;            // learned: stop when the network's logit exceeds this
     // low-precision traversal (prec 1 = bf16, 2 = fp8 e4m3 + per-row scale)
     uint32_t prec;
     const unsigned char* tvecs;  // traversal rows, tstride bytes apart

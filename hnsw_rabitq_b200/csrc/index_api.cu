@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -33,6 +34,9 @@
 #include "bf_search.h"
 #include "device_common.cuh"
 #include "hnsw_search.h"
+
+static_assert(HNSWGPU_TERM_PARAMS == hnswgpu::kTermParams, "termination parameter count");
+static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feature count");
 
 namespace {
 
@@ -107,6 +111,9 @@ struct hnswgpu_index {
     DevBuf<uint8_t> allow;
     DevBuf<float> bf_norms;    // brute force: per-row helper values
     DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
+    DevBuf<unsigned char> term_model;  // learned termination: packed network
+    uint32_t term_period = 0;
+    float term_logit = 0.f;
     std::mutex mu;
     uint64_t device_bytes() const {
         return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
@@ -503,12 +510,44 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     return p;
 }
 
+// Learned-termination settings of one launch (mode 1: record checkpoints,
+// 2: stop early with the index's network).
+struct TermCfg {
+    uint32_t mode = 0, period = 0, max_ckpt = 0;
+    float* feat = nullptr;
+    uint32_t* ids = nullptr;
+    uint32_t* count = nullptr;
+};
+
+void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg* t) {
+    if (!t || !t->mode) return;
+    if (!p.fast16 || !p.bare || p.maxM0 > 32 || p.exact)
+        throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
+                       "learned termination needs dim % 16 == 0, maxM0 <= 32, no filter / deletes and the id tie "
+                       "order");
+    p.term_mode = t->mode;
+    if (t->mode == 1) {
+        if (t->period == 0) throw ApiError(HNSWGPU_ERR_ARG, "checkpoint period must be > 0");
+        p.term_period = t->period;
+        p.term_max_ckpt = t->max_ckpt;
+        p.ckpt_feat = t->feat;
+        p.ckpt_ids = t->ids;
+        p.ckpt_count = t->count;
+    } else {
+        if (!h->term_model.p) throw ApiError(HNSWGPU_ERR_STATE, "no termination model set");
+        p.term_period = h->term_period;
+        p.term_model = reinterpret_cast<const float*>(h->term_model.p);
+        p.term_logit = h->term_logit;
+    }
+}
+
 // One HNSW search launch on device buffers, scratch from the index.
 void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
               uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact, uint32_t prec,
-              uint32_t rerank) {
+              uint32_t rerank, const TermCfg* term) {
     if (prec) ensure_traversal_copy(h, prec);
     hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank);
+    apply_term(h, p, term);
     p.status = h->status.p;
 #ifdef HNSWGPU_PHASE_TIMING
     static unsigned long long* phase_buf = nullptr;
@@ -528,8 +567,10 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
 
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
-                uint32_t prec = 0, uint32_t rerank = 0) {
-    if (h->is_bf) {
+                uint32_t prec = 0, uint32_t rerank = 0, const TermCfg* term = nullptr, bool scan = false) {
+    if (scan && !h->is_bf && h->num_deleted)
+        throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "HNSWGPU_EXACT_SCAN: the index has deleted elements");
+    if (h->is_bf || scan) {
         hnswgpu::BfParams b{};
         b.vecs = h->vecs.p;
         b.labels = h->dlabels.p;
@@ -548,7 +589,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
         cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
                    "bf_search launch");
     } else {
-        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank);
+        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank, term);
     }
 }
 
@@ -696,6 +737,10 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         const bool dev = (o.flags & HNSWGPU_DEVICE_PTRS) != 0;
         const bool want_trace = (o.flags & HNSWGPU_TRACE) && o.trace;
         const bool exact = (o.flags & HNSWGPU_EXACT_TIES) != 0;
+        const bool scan = (o.flags & HNSWGPU_EXACT_SCAN) != 0;
+        TermCfg term;
+        if (o.flags & HNSWGPU_LEARNED_STOP) term.mode = 2;
+        if (scan && term.mode) return fail(HNSWGPU_ERR_ARG, "HNSWGPU_EXACT_SCAN excludes HNSWGPU_LEARNED_STOP");
         const uint64_t ef = o.ef ? o.ef : h->ef;
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
         std::lock_guard<std::mutex> g(h->mu);
@@ -718,7 +763,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         }
         if (dev) {
             run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
-                       want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank);
+                       want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank, &term, scan);
             return HNSWGPU_OK;
         }
         // host pointers: stage through the index's device I/O buffer
@@ -739,7 +784,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             dallow = h->allow.p;
         }
         cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact, o.precision, o.rerank);
+        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact, o.precision, o.rerank, &term, scan);
         cuda_check(cudaMemcpyAsync(out_labels, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
@@ -790,6 +835,128 @@ int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint6
         cuda_check(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), st), "cudaMemsetAsync");
         cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
                    "hnsw_search launch");
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_set_termination_model(hnswgpu_index* h, const float* params, uint32_t period, float logit_threshold) {
+    return guarded([&] {
+        if (!h || h->is_bf) return fail(HNSWGPU_ERR_ARG, "a termination model needs an HNSW index");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (!params) {
+            cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+            h->term_model.release();
+            return HNSWGPU_OK;
+        }
+        if (period == 0) return fail(HNSWGPU_ERR_ARG, "period must be > 0");
+        for (int i = 0; i < hnswgpu::kTermParams; i++)
+            if (!std::isfinite(params[i])) return fail(HNSWGPU_ERR_ARG, "termination model has non-finite values");
+        std::vector<unsigned char> packed(hnswgpu::kTermPackedBytes);
+        hnswgpu::pack_term_model(params, packed.data());
+        h->term_model.ensure(packed.size());
+        // ordered after every search already queued on the index's stream
+        cuda_check(cudaMemcpyAsync(h->term_model.p, packed.data(), packed.size(), cudaMemcpyHostToDevice, h->stream),
+                   "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        h->term_period = period;
+        h->term_logit = logit_threshold;
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t k,
+                               const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt, float* out_feat,
+                               uint32_t* out_ids, uint32_t* out_nckpt, uint64_t* out_labels, float* out_dists,
+                               int32_t* out_counts) {
+    return guarded([&] {
+        if (!h || h->is_bf || k == 0 || period == 0)
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (nq && (!queries || !out_labels || !out_dists || !out_counts || !out_nckpt ||
+                   (max_ckpt && (!out_feat || !out_ids))))
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (nq > 0xffffffffull || k > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "batch too large");
+        hnswgpu_search_opts o{};
+        if (opts) o = *opts;
+        if (o.flags & ~(uint32_t)HNSWGPU_TRACE)
+            return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_checkpoints: host pointers and the id tie order only");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (nq == 0 || h->count == 0) return fail(HNSWGPU_ERR_ARG, "empty batch or index");
+        const uint64_t ef = o.ef ? o.ef : h->ef;
+        cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
+        const size_t rows = (size_t)nq * max_ckpt;
+        DevBuf<float> dq, dd, df;
+        DevBuf<uint64_t> dl;
+        DevBuf<int32_t> dc;
+        DevBuf<uint32_t> di, dn;
+        dq.alloc(nq * h->dim);
+        dl.alloc(nq * k);
+        dd.alloc(nq * k);
+        dc.alloc(nq);
+        dn.alloc(nq);
+        df.alloc(rows * hnswgpu::kTermFeatures);
+        di.alloc(rows * k);
+        cuda_check(cudaMemcpyAsync(dq.p, queries, nq * h->dim * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        TermCfg term;
+        term.mode = 1;
+        term.period = period;
+        term.max_ckpt = max_ckpt;
+        term.feat = df.p;
+        term.ids = di.p;
+        term.count = dn.p;
+        run_hnsw(h, dq.p, nq, k, ef, nullptr, dl.p, dd.p, dc.p, nullptr, st, false, o.precision, o.rerank, &term);
+        cuda_check(cudaMemcpyAsync(out_labels, dl.p, nq * k * 8, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_dists, dd.p, nq * k * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_counts, dc.p, nq * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_nckpt, dn.p, nq * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        if (rows) {
+            cuda_check(cudaMemcpyAsync(out_feat, df.p, rows * hnswgpu::kTermFeatures * 4, cudaMemcpyDeviceToHost, st),
+                       "cudaMemcpyAsync");
+            cuda_check(cudaMemcpyAsync(out_ids, di.p, rows * k * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        }
+        uint32_t status = 0;
+        cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (status & HNSWGPU_STATUS_TIMEOUT) {
+            cudaMemsetAsync(h->status.p, 0, 4, st);
+            cudaStreamSynchronize(st);
+            return fail(HNSWGPU_ERR_KERNEL, "search kernel timed out waiting for a copy");
+        }
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_term_train(int device, const float* feats, const float* labels, uint64_t n,
+                       const hnswgpu_term_train_opts* opts, float* params, float* out_epoch_loss) {
+    return guarded([&] {
+        if (!feats || !labels || !params || !opts || n == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (n > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "too many samples");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        cuda_check(hnswgpu::term_train(feats, labels, n, params, opts->epochs, opts->batch, opts->lr,
+                                       opts->pos_weight, opts->weight_decay, opts->seed, out_epoch_loss),
+                   "termination training");
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_term_loss_grad(int device, const float* params, const float* feats, const float* labels, uint64_t n,
+                           float pos_weight, float* out_loss, float* out_grad) {
+    return guarded([&] {
+        if (!feats || !labels || !params || !out_loss || !out_grad || n == 0)
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        cuda_check(hnswgpu::term_loss_grad(params, feats, labels, n, pos_weight, out_loss, out_grad),
+                   "termination gradient");
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_term_logits(int device, const float* params, const float* feats, uint64_t n, float* out_logits) {
+    return guarded([&] {
+        if (!params || (n && (!feats || !out_logits))) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        cuda_check(hnswgpu::term_logits(params, feats, n, out_logits), "termination inference");
         return HNSWGPU_OK;
     });
 }

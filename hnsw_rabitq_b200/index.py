@@ -101,8 +101,7 @@ class _GpuIndex:
         self._filter_cache = (filter, mask)
         return mask
 
-    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False, exact_ties: bool = False,
-                precision: str = "fp32", rerank: int = 0):
+    def _queries(self, data, k: int):
         self._require()
         q = _input_rows(data)
         if q.shape[1] != self.dim:
@@ -110,6 +109,11 @@ class _GpuIndex:
         k = int(k)
         if k <= 0:
             raise RuntimeError("k must be positive")
+        return q, k
+
+    def _search(self, data, k: int, filter, ef: int = 0, trace: bool = False, exact_ties: bool = False,
+                precision: str = "fp32", rerank: int = 0, flags: int = 0):
+        q, k = self._queries(data, k)
         nq = q.shape[0]
         labels = np.empty((nq, k), np.uint64)
         dists = np.empty((nq, k), np.float32)
@@ -118,7 +122,8 @@ class _GpuIndex:
         opts.ef = int(ef)
         opts.precision = _PRECISIONS[precision]
         opts.rerank = int(rerank)
-        if exact_ties and opts.precision == _capi.PREC_FP32:
+        opts.flags = int(flags)
+        if exact_ties and opts.precision == _capi.PREC_FP32 and not flags & _capi.LEARNED_STOP:
             opts.flags |= _capi.EXACT_TIES
         mask = self._allow_mask(filter)
         opts.allow = mask.ctypes.data if mask is not None else None
@@ -175,6 +180,11 @@ class Index(_GpuIndex):
         # candidates, default ef, re-ranked with exact float32 distances)
         self.precision = "fp32"
         self.rerank = 0
+        # learned early termination: when True (and a model is set with
+        # set_termination_model), knn_query ends each query's beam as soon as
+        # the network judges its top-k final; ef is the cap (id tie order)
+        self.learned_stop = False
+        self._term_model = None
 
     def __repr__(self):
         return f"<hnsw_rabitq_b200.Index(space='{self.space}', dim={self.dim})>"
@@ -232,20 +242,70 @@ class Index(_GpuIndex):
         self._require()
         _capi.check(_capi.lib().hnswgpu_unmark_deleted(self._h, int(label)))
 
+    # -- learned early termination
+    def set_termination_model(self, model) -> None:
+        """Install a trained ``learned.TerminationModel`` (or None to remove
+        it) on the GPU index."""
+        self._require()
+        if model is None:
+            _capi.check(_capi.lib().hnswgpu_set_termination_model(self._h, None, 0, 0.0))
+            self._term_model = None
+            return
+        p = np.ascontiguousarray(model.params, dtype=np.float32)
+        if p.shape != (_capi.TERM_PARAMS,):
+            raise ValueError(f"termination parameters must have shape ({_capi.TERM_PARAMS},)")
+        _capi.check(_capi.lib().hnswgpu_set_termination_model(self._h, _ptr(p), int(model.period),
+                                                              float(model.threshold)))
+        self._term_model = model
+
+    def _flags(self, learned: Optional[bool]) -> int:
+        use = self.learned_stop if learned is None else learned
+        return _capi.LEARNED_STOP if use else 0
+
+    def search_checkpoints(self, data, k: int, ef: int = 0, period: int = 4, max_ckpt: int = 128,
+                           precision: Optional[str] = None, rerank: Optional[int] = None):
+        """The id-tie-order search, recording every `period` level-0
+        expansions the termination features and the internal ids of the
+        current top-k.  Returns a dict with feat [nq, max_ckpt, 6], ids
+        [nq, max_ckpt, k] (uint32, 0xffffffff = none), nckpt [nq], labels,
+        dists, counts."""
+        q, k = self._queries(data, k)
+        nq = q.shape[0]
+        out = dict(feat=np.zeros((nq, max_ckpt, _capi.TERM_FEATURES), np.float32),
+                   ids=np.full((nq, max_ckpt, k), 0xffffffff, np.uint32), nckpt=np.zeros(nq, np.uint32),
+                   labels=np.empty((nq, k), np.uint64), dists=np.empty((nq, k), np.float32),
+                   counts=np.empty(nq, np.int32))
+        opts = _capi.SearchOpts()
+        opts.ef = int(ef)
+        opts.precision = _PRECISIONS[precision or self.precision]
+        opts.rerank = int(self.rerank if rerank is None else rerank)
+        _capi.check(_capi.lib().hnswgpu_search_checkpoints(
+            self._h, _ptr(q), nq, k, C.byref(opts), int(period), int(max_ckpt), _ptr(out["feat"]),
+            _ptr(out["ids"]), _ptr(out["nckpt"]), _ptr(out["labels"]), _ptr(out["dists"]), _ptr(out["counts"])))
+        return out
+
+    def knn_query_exact(self, data, k: int = 1, filter: Optional[Callable[[int], bool]] = None):
+        """Exact k-NN by an exhaustive GPU scan of the index's vectors (the
+        ground truth of recall measurements): (labels, distances)."""
+        labels, dists, counts, _ = self._search(data, k, filter, flags=_capi.EXACT_SCAN)
+        return labels, dists
+
     # -- search
     def knn_query(self, data, k: int = 1, num_threads: int = -1, filter: Optional[Callable[[int], bool]] = None):
         """(labels uint64 [N, k], distances float32 [N, k]), closest first
         (bindings.cpp:612-697).  Raises RuntimeError when a query has fewer
         than k results, with the reference's message."""
         labels, dists, counts, _ = self._search(data, k, filter, exact_ties=self.tie_order == "reference",
-                                                precision=self.precision, rerank=self.rerank)
+                                                precision=self.precision, rerank=self.rerank,
+                                                flags=self._flags(None))
         if counts.size and counts.min() < k:
             raise RuntimeError(
                 "Cannot return the results in a contiguous 2D array. Probably ef or M is too small")
         return labels, dists
 
     def knn_query_traced(self, data, k: int = 1, filter=None, ef: int = 0, tie_order: Optional[str] = None,
-                         precision: Optional[str] = None, rerank: Optional[int] = None):
+                         precision: Optional[str] = None, rerank: Optional[int] = None,
+                         learned: Optional[bool] = None):
         """knn_query plus per-query work counters [upper link lists read,
         upper distances, level-0 expansions, level-0 distances] and counts;
         no exception for short results."""
@@ -253,7 +313,7 @@ class Index(_GpuIndex):
         prec = precision or self.precision
         rr = self.rerank if rerank is None else rerank
         return self._search(data, k, filter, ef=ef, trace=True, exact_ties=order == "reference", precision=prec,
-                            rerank=rr)
+                            rerank=rr, flags=self._flags(learned))
 
 
 class BFIndex(_GpuIndex):

@@ -1,0 +1,212 @@
+"""Learned early termination of the HNSW level-0 beam.
+
+The reference's beam (hnswlib/hnswalg.h:368-440) runs until its candidate
+queue is exhausted, so every query pays for the hardest query's ef.  Here a
+small network decides per query when the top-k has stopped changing:
+
+1. ``Index.search_checkpoints`` runs the search (ef = the cap) and records,
+   every `period` level-0 expansions, a 6-feature description of the beam and
+   the current top-k (GPU kernel, the same feature code the search uses);
+2. each checkpoint is labelled 1 when stopping there loses nothing: its top-k
+   already holds as many true neighbours (exact GPU scan) as the beam's final
+   answer;
+3. the 6 -> 64 -> 64 -> 1 network is trained on the GPU (forward / backward /
+   Adam kernels of libhnswgpu, float32 master weights);
+4. the stop threshold on the logit is calibrated on held-out queries by
+   running the learned search itself (fp16 weights, in-warp inference) and
+   keeping the earliest stop whose recall@k meets the target.
+
+With the model installed (``Index.set_termination_model``) and
+``Index.learned_stop = True``, ``knn_query`` stops each query at the first
+checkpoint whose logit exceeds the threshold; ef is the fallback cap.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _capi
+
+N_PARAMS = _capi.TERM_PARAMS
+F, H = _capi.TERM_FEATURES, _capi.TERM_HIDDEN
+OFF_MU, OFF_INV_SIGMA = 0, F
+OFF_W1 = 2 * F
+OFF_B1 = OFF_W1 + H * F
+OFF_W2 = OFF_B1 + H
+OFF_B2 = OFF_W2 + H * H
+OFF_W3 = OFF_B2 + H
+OFF_B3 = OFF_W3 + H
+_NONE = 0xffffffff
+
+
+@dataclass
+class TerminationModel:
+    """A trained network plus how it is applied."""
+    params: np.ndarray            # float32 [HNSWGPU_TERM_PARAMS]
+    period: int = 4               # expansions between checkpoints
+    threshold: float = 0.0        # stop when logit > threshold
+    ef_cap: int = 128             # ef of the learned search (the fallback cap)
+    precision: str = "fp32"       # traversal precision it was trained with
+    rerank: int = 0
+    info: dict = field(default_factory=dict)
+
+    def save(self, path: str) -> None:
+        meta = dict(period=self.period, threshold=self.threshold, ef_cap=self.ef_cap, precision=self.precision,
+                    rerank=self.rerank, info=self.info)
+        np.savez(path, params=self.params, meta=json.dumps(meta))
+
+    @staticmethod
+    def load(path: str) -> "TerminationModel":
+        z = np.load(path)
+        meta = json.loads(str(z["meta"]))
+        return TerminationModel(params=z["params"].astype(np.float32), **meta)
+
+
+def init_params(feats: np.ndarray, seed: int = 0) -> np.ndarray:
+    """He-initialised parameters; mu / inv_sigma standardise `feats`."""
+    feats = np.asarray(feats, np.float64)
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAMS, np.float32)
+    p[OFF_MU:OFF_MU + F] = feats.mean(0)
+    p[OFF_INV_SIGMA:OFF_INV_SIGMA + F] = 1.0 / np.maximum(feats.std(0), 1e-6)
+    p[OFF_W1:OFF_B1] = rng.normal(0, np.sqrt(2.0 / F), H * F)
+    p[OFF_W2:OFF_B2] = rng.normal(0, np.sqrt(2.0 / H), H * H)
+    p[OFF_W3:OFF_B3] = rng.normal(0, np.sqrt(1.0 / H), H)
+    return p
+
+
+def _hits(labels: np.ndarray, gt: np.ndarray) -> np.ndarray:
+    """Number of ground-truth labels in each row: labels [..., k] against
+    gt rows broadcast over the leading axes."""
+    return (labels[..., :, None] == gt[..., None, :]).any(-1).sum(-1)
+
+
+def recall(labels: np.ndarray, gt: np.ndarray) -> float:
+    k = gt.shape[1]
+    return float(_hits(labels[:, :k].astype(np.uint64), gt.astype(np.uint64)).mean() / k)
+
+
+def checkpoint_dataset(index, ck: dict, gt: np.ndarray):
+    """(features [n, 6], labels [n]) of every recorded checkpoint: label 1 when
+    the checkpoint's top-k holds at least as many true neighbours as the
+    search's final answer."""
+    nq, R, k = ck["ids"].shape
+    lab_of = index.labels_by_internal_id()
+    gt = gt.astype(np.uint64)
+    final = _hits(ck["labels"].astype(np.uint64), gt)            # [nq]
+    X, Y = [], []
+    for a in range(0, nq, 512):
+        b = min(nq, a + 512)
+        ids = ck["ids"][a:b]
+        valid = np.arange(R)[None, :] < ck["nckpt"][a:b, None]      # [q, R]
+        lab = np.where(ids == _NONE, np.uint64(2**64 - 1), lab_of[np.minimum(ids, len(lab_of) - 1)])
+        now = _hits(lab, gt[a:b, None, :])                          # [q, R]
+        y = (now >= final[a:b, None]).astype(np.float32)
+        X.append(ck["feat"][a:b][valid])
+        Y.append(y[valid])
+    return np.concatenate(X).astype(np.float32), np.concatenate(Y).astype(np.float32)
+
+
+def train(feats: np.ndarray, labels: np.ndarray, params: Optional[np.ndarray] = None, epochs: int = 20,
+          batch: int = 1024, lr: float = 2e-3, pos_weight: float = 1.0, weight_decay: float = 1e-4, seed: int = 0,
+          device: int = 0):
+    """Train on the GPU; returns (params float32 [N_PARAMS], per-epoch loss)."""
+    feats = np.ascontiguousarray(feats, np.float32)
+    labels = np.ascontiguousarray(labels, np.float32)
+    p = np.array(init_params(feats, seed) if params is None else params, np.float32, copy=True)
+    o = _capi.TermTrainOpts(epochs=int(epochs), batch=int(batch), lr=float(lr), pos_weight=float(pos_weight),
+                            weight_decay=float(weight_decay), reserved=0, seed=int(seed))
+    losses = np.zeros(max(1, int(epochs)), np.float32)
+    _capi.check(_capi.lib().hnswgpu_term_train(int(device), feats.ctypes.data_as(C.c_void_p),
+                                               labels.ctypes.data_as(C.c_void_p), feats.shape[0], C.byref(o),
+                                               p.ctypes.data_as(C.c_void_p), losses.ctypes.data_as(C.c_void_p)))
+    return p, losses[:epochs]
+
+
+def loss_grad(params: np.ndarray, feats: np.ndarray, labels: np.ndarray, pos_weight: float = 1.0,
+              device: int = 0):
+    """Mean loss and gradient by the GPU training kernels."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(feats, np.float32)
+    y = np.ascontiguousarray(labels, np.float32)
+    loss = np.zeros(1, np.float32)
+    g = np.zeros(N_PARAMS, np.float32)
+    _capi.check(_capi.lib().hnswgpu_term_loss_grad(int(device), p.ctypes.data_as(C.c_void_p),
+                                                   f.ctypes.data_as(C.c_void_p), y.ctypes.data_as(C.c_void_p),
+                                                   f.shape[0], float(pos_weight), loss.ctypes.data_as(C.c_void_p),
+                                                   g.ctypes.data_as(C.c_void_p)))
+    return float(loss[0]), g
+
+
+def logits(params: np.ndarray, feats: np.ndarray, device: int = 0) -> np.ndarray:
+    """Logits by the search's own in-warp inference (fp16 weights)."""
+    p = np.ascontiguousarray(params, np.float32)
+    f = np.ascontiguousarray(feats, np.float32)
+    out = np.zeros(f.shape[0], np.float32)
+    _capi.check(_capi.lib().hnswgpu_term_logits(int(device), p.ctypes.data_as(C.c_void_p),
+                                                f.ctypes.data_as(C.c_void_p), f.shape[0],
+                                                out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def evaluate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, threshold: float):
+    """(recall@k, mean level-0 expansions) of the learned search at this
+    threshold."""
+    m = TerminationModel(model.params, model.period, float(threshold), model.ef_cap, model.precision, model.rerank)
+    index.set_termination_model(m)
+    lab, _, cnt, tr = index.knn_query_traced(queries, k, ef=model.ef_cap, tie_order="id", precision=model.precision,
+                                             rerank=model.rerank, learned=True)
+    return recall(lab, gt), float(tr[:, 2].mean())
+
+
+def calibrate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, target_recall: float,
+              candidates: Optional[np.ndarray] = None):
+    """Earliest-stopping logit threshold whose recall@k on these queries
+    meets the target; returns (threshold, curve [(threshold, recall,
+    mean expansions)])."""
+    if candidates is None:
+        candidates = np.concatenate([np.linspace(8.0, -4.0, 25), [-6.0, -8.0]])
+    curve = []
+    best = float("inf")
+    for t in sorted(candidates, reverse=True):
+        r, e = evaluate(index, queries, gt, k, model, t)
+        curve.append((float(t), r, e))
+        if r >= target_recall:
+            best = float(t)
+    return best, curve
+
+
+def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 128, period: int = 4, target_recall: float = 0.95,
+        precision: Optional[str] = None, rerank: Optional[int] = None, holdout: float = 0.3,
+        max_ckpt: Optional[int] = None, epochs: int = 20, seed: int = 0, gt: Optional[np.ndarray] = None,
+        device: int = 0):
+    """Trace, label, train and calibrate on `queries` (drawn from the query
+    distribution; a `holdout` share is kept for the calibration).  Returns
+    (TerminationModel, report)."""
+    precision = precision or index.precision
+    rerank = index.rerank if rerank is None else rerank
+    queries = np.ascontiguousarray(queries, np.float32)
+    if gt is None:
+        gt = index.knn_query_exact(queries, k)[0]
+    n = queries.shape[0]
+    perm = np.random.default_rng(seed).permutation(n)
+    nh = max(1, int(round(n * holdout)))
+    hold, tr = perm[:nh], perm[nh:]
+    if max_ckpt is None:
+        max_ckpt = max(16, (8 * ef_cap) // period)
+    ck = index.search_checkpoints(queries[tr], k, ef=ef_cap, period=period, max_ckpt=max_ckpt, precision=precision,
+                                  rerank=rerank)
+    X, y = checkpoint_dataset(index, ck, gt[tr])
+    params, losses = train(X, y, epochs=epochs, seed=seed, device=device)
+    model = TerminationModel(params, period, float("inf"), ef_cap, precision, int(rerank))
+    thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall)
+    model.threshold = thr
+    base_r, base_e = evaluate(index, queries[hold], gt[hold], k, model, float("inf"))
+    model.info = dict(samples=int(X.shape[0]), positive=float(y.mean()), loss=[float(v) for v in losses],
+                      curve=curve, cap_recall=base_r, cap_expansions=base_e, target_recall=target_recall)
+    index.set_termination_model(model)
+    return model, model.info

@@ -58,6 +58,17 @@ extern "C" {
                                      that exact distance ties resolve as in
                                      hnswlib (results identical to searchKnn);
                                      without it ties break by internal id.     */
+#define HNSWGPU_LEARNED_STOP 0x8u /* HNSW: end each query's level-0 beam when
+                                     the termination network set by
+                                     hnswgpu_set_termination_model judges its
+                                     top-k final; ef is then the cap.  Needs
+                                     dim % 16 == 0, maxM0 <= 32, no filter or
+                                     deletes, and the id tie order.           */
+#define HNSWGPU_EXACT_SCAN 0x10u  /* HNSW: answer by an exhaustive scan of the
+                                     index's resident vectors (exact k-NN,
+                                     the ground truth of recall measurements;
+                                     the allow mask applies, deletes are not
+                                     supported).                               */
 
 /* kernel status bits (hnswgpu_search_opts.status / hnswgpu_get_status) */
 #define HNSWGPU_STATUS_TIMEOUT 0x1u   /* a bounded wait gave up; results invalid   */
@@ -83,7 +94,7 @@ typedef struct hnswgpu_info {
 } hnswgpu_info;
 
 typedef struct hnswgpu_search_opts {
-    uint32_t flags;            /* HNSWGPU_DEVICE_PTRS | HNSWGPU_TRACE           */
+    uint32_t flags;            /* HNSWGPU_DEVICE_PTRS | HNSWGPU_TRACE | ...     */
     uint32_t precision;        /* HNSW traversal copy: HNSWGPU_PREC_FP32 (the
                                   reference's search), _BF16 or _FP8; the
                                   low-precision forms re-rank the best
@@ -201,6 +212,67 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
 HNSWGPU_API int hnswgpu_search_noalloc(const hnswgpu_index* index, const float* d_queries, uint64_t nq, uint64_t k,
                                        uint64_t ef, uint32_t flags, const uint8_t* d_allow, uint64_t* d_labels,
                                        float* d_dists, int32_t* d_counts, void* stream);
+
+/* ------------------------------------------------ learned early termination
+ * No counterpart in the reference, whose beam always runs until its
+ * candidate queue is exhausted (hnswlib/hnswalg.h:368-376).
+ *
+ * Every `period` level-0 expansions the beam forms a feature vector of its
+ * state (log2(1 + expansions); d_1 / |d_k|; (d_next - d_k) / |d_k|;
+ * log2(1 + d_entry / |d_k|); log2(1 + |q|^2); expansions since the top-k
+ * last changed / period; d_1, d_k = best and k-th distances in the beam,
+ * d_next = the candidate expanded next, d_entry = the level-0 entry point).
+ * A 6 -> 64 -> 64 -> 1 ReLU network maps it to the logit of "the top-k is
+ * final".  Parameters: HNSWGPU_TERM_PARAMS float32 in the order
+ * mu[6], inv_sigma[6] (x = (f - mu) * inv_sigma), W1[64][6], b1[64],
+ * W2[64][64], b2[64], w3[64], b3. */
+#define HNSWGPU_TERM_FEATURES 6
+#define HNSWGPU_TERM_HIDDEN 64
+#define HNSWGPU_TERM_PARAMS 4685
+
+/* Install (params != NULL) or remove (NULL) the index's termination network;
+ * HNSWGPU_LEARNED_STOP searches evaluate it every `period` expansions and
+ * stop when the logit exceeds `logit_threshold`.  The search runs the
+ * network with fp16 weights and fp32 accumulation. */
+HNSWGPU_API int hnswgpu_set_termination_model(hnswgpu_index* index, const float* params, uint32_t period,
+                                              float logit_threshold);
+
+/* Training data: the same search as hnswgpu_search (host pointers, id tie
+ * order, opts->precision / rerank / ef honoured) that also records, every
+ * `period` expansions, the feature vector (out_feat: nq x max_ckpt x 6) and
+ * the internal ids of the current top-k (out_ids: nq x max_ckpt x k,
+ * 0xffffffff where the beam holds fewer); out_nckpt[i] = rows written for
+ * query i (at most max_ckpt). */
+HNSWGPU_API int hnswgpu_search_checkpoints(hnswgpu_index* index, const float* queries, uint64_t nq, uint64_t k,
+                                           const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt,
+                                           float* out_feat, uint32_t* out_ids, uint32_t* out_nckpt,
+                                           uint64_t* out_labels, float* out_dists, int32_t* out_counts);
+
+typedef struct hnswgpu_term_train_opts {
+    uint32_t epochs;
+    uint32_t batch;            /* samples per Adam step (0: 1024)             */
+    float lr;                  /* Adam step size                              */
+    float pos_weight;          /* weight of the label-1 term of the loss      */
+    float weight_decay;        /* decoupled, on the weight matrices           */
+    uint32_t reserved;
+    uint64_t seed;             /* mini-batch shuffling                        */
+} hnswgpu_term_train_opts;
+
+/* Train the network on the GPU (forward / backward / Adam kernels) from n
+ * samples (feats: n x 6, labels: n floats in {0, 1}); `params` holds the
+ * initial values (mu / inv_sigma set by the caller) and receives the
+ * trained ones; out_epoch_loss (optional): mean batch loss per epoch. */
+HNSWGPU_API int hnswgpu_term_train(int device, const float* feats, const float* labels, uint64_t n,
+                                   const hnswgpu_term_train_opts* opts, float* params, float* out_epoch_loss);
+
+/* Mean loss and its gradient (HNSWGPU_TERM_PARAMS floats; zero for
+ * mu / inv_sigma) over n samples, computed by the training kernels. */
+HNSWGPU_API int hnswgpu_term_loss_grad(int device, const float* params, const float* feats, const float* labels,
+                                       uint64_t n, float pos_weight, float* out_loss, float* out_grad);
+
+/* Logits of n feature vectors by the search's own in-warp inference. */
+HNSWGPU_API int hnswgpu_term_logits(int device, const float* params, const float* feats, uint64_t n,
+                                    float* out_logits);
 
 /* OR of the kernel status bits raised by searches on this index since the
  * last call (synchronises the index's stream); clears them. */

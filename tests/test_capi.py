@@ -34,13 +34,17 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_header(tmp_path):
     prog = tmp_path / "sz.c"
     prog.write_text('#include <stdio.h>\n#include "hnswgpu.h"\n#include <stddef.h>\n'
-                    'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(hnswgpu_info), sizeof(hnswgpu_search_opts),'
-                    ' offsetof(hnswgpu_info, device_bytes), offsetof(hnswgpu_search_opts, stream));return 0;}\n')
+                    'int main(void){printf("%zu %zu %zu %zu %zu %zu %d\\n", sizeof(hnswgpu_info), sizeof(hnswgpu_search_opts),'
+                    ' offsetof(hnswgpu_info, device_bytes), offsetof(hnswgpu_search_opts, stream),'
+                    ' sizeof(hnswgpu_term_train_opts), offsetof(hnswgpu_term_train_opts, seed),'
+                    ' HNSWGPU_TERM_PARAMS);return 0;}\n')
     exe = tmp_path / "sz"
     subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)])
-    a, b, c, d = map(int, subprocess.check_output([str(exe)]).split())
+    a, b, c, d, e, f, g = map(int, subprocess.check_output([str(exe)]).split())
     assert a == C.sizeof(_capi.Info) and b == C.sizeof(_capi.SearchOpts)
     assert c == _capi.Info.device_bytes.offset and d == _capi.SearchOpts.stream.offset
+    assert e == C.sizeof(_capi.TermTrainOpts) and f == _capi.TermTrainOpts.seed.offset
+    assert g == _capi.TERM_PARAMS
 
 
 def test_version_and_error_string():

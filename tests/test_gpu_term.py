@@ -1,0 +1,149 @@
+"""Learned early termination on the GPU: the training kernels' gradients and
+the in-search inference against the float64 oracle, the checkpoint traces
+against the search they record, and the stop rule itself (needs a B200)."""
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from hnsw_rabitq_b200 import learned
+from oracle import oracle as O
+from oracle import term_mlp as T
+from tests.helpers import build_hnsw
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_problem(n, seed=0):
+    rng = np.random.default_rng(seed)
+    f = (rng.normal(size=(n, 6)) * [1, 0.5, 0.3, 2, 1, 3] + [3, 0.5, 0.1, 1, 10, 2]).astype(np.float32)
+    y = (rng.random(n) < 0.35).astype(np.float32)
+    p = learned.init_params(f, seed)
+    p[T.OFF_B1:T.OFF_W2] = rng.normal(0, 0.1, T.H)
+    p[T.OFF_B2:T.OFF_W3] = rng.normal(0, 0.1, T.H)
+    p[T.OFF_B3] = -0.2
+    return p, f, y
+
+
+@pytest.mark.parametrize("n,pw", [(1, 1.0), (127, 1.0), (1000, 2.5), (4097, 1.0)])
+def test_gradient_matches_oracle(n, pw):
+    """Forward + backward kernels (float32, per-CTA partial sums reduced in
+    a fixed order) against the float64 oracle: |g - g_ref| <= 1e-4 * max|g_ref|
+    + 1e-7 per entry, loss to 1e-5 relative."""
+    p, f, y = _random_problem(n, seed=n)
+    loss, g = learned.loss_grad(p, f, y, pw)
+    rl, rg = T.loss_grad(p, f, y, pw)
+    assert abs(loss - rl) <= 1e-5 * abs(rl) + 1e-7
+    assert np.all(g[:T.OFF_W1] == 0)
+    tol = 1e-4 * np.abs(rg).max() + 1e-7
+    assert np.abs(g - rg).max() <= tol, np.abs(g - rg).max()
+    # deterministic: same inputs, same bits
+    assert np.array_equal(learned.loss_grad(p, f, y, pw)[1].view(np.uint32), g.view(np.uint32))
+
+
+def test_inference_matches_oracle_with_fp16_weights():
+    """The search's in-warp inference (fp16 weights, fp32 accumulation)
+    against the oracle with the same fp16-rounded weights: within 1e-4
+    relative to the logit scale."""
+    p, f, _ = _random_problem(3000, seed=5)
+    z = learned.logits(p, f)
+    ref = T.forward(p, f, fp16_weights=True)
+    assert np.abs(z - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
+    # and close to the float32 network
+    assert np.abs(z - T.forward(p, f)).max() <= 2e-2 * max(1.0, np.abs(ref).max())
+
+
+def test_training_learns_a_separable_rule():
+    rng = np.random.default_rng(3)
+    f = rng.normal(size=(20000, 6)).astype(np.float32)
+    y = ((f[:, 0] + 0.5 * f[:, 3] > 0.2) & (f[:, 5] > -1)).astype(np.float32)
+    p, losses = learned.train(f, y, epochs=15, batch=512, lr=3e-3, seed=1)
+    assert losses[-1] < 0.5 * losses[0]
+    acc = np.mean((learned.logits(p, f) > 0) == (y > 0.5))
+    assert acc > 0.97, acc
+    # the trained loss agrees with the oracle's evaluation of those weights
+    assert abs(T.loss_grad(p, f, y)[0] - learned.loss_grad(p, f, y)[0]) < 1e-4
+
+
+@pytest.fixture(scope="module")
+def gmm_index(tmp_path_factory):
+    from hnsw_rabitq_b200.datasets import gmm_1m_128
+    x, q = gmm_1m_128(n=30000, nq=1500)
+    path = tmp_path_factory.mktemp("term") / "gmm.bin"
+    build_hnsw(path, x, "l2", M=16, efc=100, num_threads=8)
+    g = H.Index("l2", 128)
+    g.load_index(str(path))
+    return g, x, q
+
+
+def test_checkpoint_trace_is_the_search(gmm_index):
+    """Recording checkpoints does not change the search; each row's features
+    restate the beam it saw: expansions = period * (row + 1), d_1 / |d_k| from
+    the exact distances of the recorded top-k ids."""
+    g, x, q = gmm_index
+    q = q[:300]
+    k, ef, period = 10, 96, 4
+    pl, pd, pc, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id")
+    ck = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=400)
+    assert np.array_equal(ck["labels"], pl) and np.array_equal(ck["dists"].view(np.uint32), pd.view(np.uint32))
+    # a checkpoint after every `period`-th expansion that has a successor
+    assert np.all(ck["nckpt"] <= pt[:, 2] // period)
+    assert np.all(ck["nckpt"] >= (pt[:, 2] - 1) // period)
+    lab_of = g.labels_by_internal_id()
+    for i in range(0, 300, 15):
+        for r in range(int(ck["nckpt"][i])):
+            f = ck["feat"][i, r]
+            assert abs(f[0] - np.log2(1 + period * (r + 1))) < 1e-5
+            ids = ck["ids"][i, r]
+            assert np.all(ids != 0xffffffff)
+            d = O.distances("l2", q[i], x[lab_of[ids].astype(np.int64)])
+            assert np.all(np.diff(d) >= 0)
+            assert abs(f[1] - min(4.0, d[0] / abs(d[-1]))) <= 1e-6 * max(1.0, abs(f[1]))
+            assert 0 <= f[5] <= 16
+
+
+def test_stop_rule_bounds(gmm_index):
+    """Threshold +inf never stops (identical to the plain search); threshold
+    -inf stops at the first checkpoint."""
+    g, x, q = gmm_index
+    q = q[:400]
+    p, f, _ = _random_problem(10)
+    k, ef, period = 10, 64, 4
+    pl, pd, _, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id")
+    g.set_termination_model(learned.TerminationModel(p, period, float("inf")))
+    ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
+    assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
+    g.set_termination_model(learned.TerminationModel(p, period, -float("inf")))
+    ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
+    assert np.all(lt[:, 2] <= period) and np.all(lc == k)
+    assert np.all(np.diff(ld, axis=1) >= 0)
+    g.set_termination_model(None)
+    with pytest.raises(RuntimeError, match="no termination model"):
+        g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
+
+
+def test_fit_meets_target_with_less_work(gmm_index):
+    """Trained and calibrated on 1000 queries, evaluated on 500 others: the
+    learned search reaches the target recall@10 (less a small
+    generalisation margin) with fewer level-0 expansions than the cap."""
+    g, x, q = gmm_index
+    tr, te = q[:1000], q[1000:]
+    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0)
+    assert rep["samples"] > 10000 and 0.05 < rep["positive"] < 0.95
+    assert rep["loss"][-1] < rep["loss"][0]
+    gt = g.knn_query_exact(te, 10)[0]
+    g.learned_stop = True
+    g.tie_order = "id"
+    g.set_ef(model.ef_cap)
+    lab, _ = g.knn_query(te, 10)
+    r = learned.recall(lab, gt)
+    _, _, _, tl = g.knn_query_traced(te, 10, ef=model.ef_cap, learned=True)
+    _, _, _, tp = g.knn_query_traced(te, 10, ef=model.ef_cap, learned=False)
+    assert r >= 0.94, (r, rep["curve"])
+    assert tl[:, 2].mean() < 0.9 * tp[:, 2].mean(), (tl[:, 2].mean(), tp[:, 2].mean())
+
+
+def test_exact_scan_is_ground_truth(gmm_index):
+    g, x, q = gmm_index
+    l, d = g.knn_query_exact(q[:200], 10)
+    rl, rd = O.bf_matrix("l2", x, q[:200], 10)
+    assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))

@@ -1,0 +1,77 @@
+"""CPU checks of the early-termination pieces that need no GPU: the float64
+oracle's gradient against central finite differences, the parameter layout
+shared with the C ABI, and the checkpoint labelling of the training set."""
+import numpy as np
+
+from hnsw_rabitq_b200 import _capi, learned
+from oracle import term_mlp as T
+
+
+def _problem(seed=0, n=40):
+    rng = np.random.default_rng(seed)
+    f = rng.normal(size=(n, T.F)) * 2 + 1
+    y = (rng.random(n) < 0.4).astype(np.float64)
+    p = learned.init_params(f, seed).astype(np.float64)
+    p[T.OFF_B1:T.OFF_W2] = rng.normal(0, 0.1, T.H)
+    p[T.OFF_B2:T.OFF_W3] = rng.normal(0, 0.1, T.H)
+    p[T.OFF_B3] = 0.3
+    return p, f, y
+
+
+def test_layout_matches_c_abi():
+    assert T.N_PARAMS == _capi.TERM_PARAMS == learned.N_PARAMS
+    assert (T.OFF_W1, T.OFF_B1, T.OFF_W2, T.OFF_B2, T.OFF_W3, T.OFF_B3) == \
+        (learned.OFF_W1, learned.OFF_B1, learned.OFF_W2, learned.OFF_B2, learned.OFF_W3, learned.OFF_B3)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    p, f, y = _problem()
+    for pw in (1.0, 3.0):
+        loss, g = T.loss_grad(p, f, y, pw)
+        assert np.all(g[:T.OFF_W1] == 0)
+        rng = np.random.default_rng(1)
+        idx = np.concatenate([rng.choice(np.arange(T.OFF_W1, T.N_PARAMS), 120, replace=False), [T.OFF_B3]])
+        h = 1e-6
+        for i in idx:
+            a, b = p.copy(), p.copy()
+            a[i] += h
+            b[i] -= h
+            num = (T.loss_grad(a, f, y, pw)[0] - T.loss_grad(b, f, y, pw)[0]) / (2 * h)
+            assert abs(num - g[i]) <= 1e-6 + 1e-5 * abs(num), (i, num, g[i])
+
+
+def test_forward_matches_loss_definition():
+    p, f, y = _problem(2)
+    z = T.forward(p, f)
+    sp = lambda v: np.logaddexp(0, v)
+    want = np.mean(2.0 * y * sp(-z) + (1 - y) * sp(z))
+    assert abs(T.loss_grad(p, f, y, 2.0)[0] - want) < 1e-12
+
+
+class _FakeIndex:
+    def __init__(self, labels):
+        self._l = np.asarray(labels, np.uint64)
+
+    def labels_by_internal_id(self):
+        return self._l
+
+
+def test_checkpoint_labels():
+    # internal id i has label 100 + i; k = 3
+    idx = _FakeIndex(100 + np.arange(10))
+    N = 0xffffffff
+    ck = dict(
+        ids=np.array([[[0, 1, N], [0, 1, 2], [0, 1, 3], [9, 9, 9]],
+                      [[5, 6, 7], [5, 6, 8], [0, 0, 0], [0, 0, 0]]], np.uint32),
+        nckpt=np.array([3, 2], np.uint32),
+        feat=np.arange(2 * 4 * 6, dtype=np.float32).reshape(2, 4, 6),
+        labels=np.array([[100, 101, 103], [105, 106, 108]], np.uint64))
+    gt = np.array([[100, 101, 102], [105, 106, 107]], np.uint64)
+    X, y = learned.checkpoint_dataset(idx, ck, gt)
+    # query 0: final hits 2; checkpoints hit 2, 3, 2 -> all 1
+    # query 1: final hits 2; checkpoints hit 3, 2 -> 1, 1
+    assert X.shape == (5, 6) and np.array_equal(y, [1, 1, 1, 1, 1])
+    ck["labels"][0] = [100, 101, 102]  # final hits 3: only checkpoint 1 reaches it
+    X, y = learned.checkpoint_dataset(idx, ck, gt)
+    assert np.array_equal(y, [0, 1, 0, 1, 1])
+    assert np.array_equal(X[3], ck["feat"][1, 0])
