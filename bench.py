@@ -7,21 +7,31 @@ mixture (centres U[0,255], sigma 20) rounded to integers in [0,255]; 10,000
 queries from the same mixture; graph built by the reference (hnswlib 0.9.0,
 M=16, ef_construction=200); k=10.
 
-Metric: queries/s at recall@10 >= 0.95.  Recall is measured against exact
-top-10 from the GPU brute force (bit-identical to the reference's
-BruteforceSearch).  The smallest ef of the sweep 10..400 that reaches the
-target is the operating point.
+Metric: queries/s at recall@10 >= 0.95 of the learned-termination + FP8
+search, with the plain FP32 beam (both tie orders) measured beside it in the
+same run.  Recall is measured against exact top-10 from the GPU brute force
+(bit-identical to the reference's BruteforceSearch).
 
-* ``value``  -- device-resident throughput: K launches over the 10,000
-  resident queries, timed with CUDA events on the launch stream.
-* ``e2e``    -- the same through the C ABI (hnswgpu_search) with pinned host
-  buffers: host->device copy of the queries, search, device->host copy of the
-  labels/distances/counts every step, wall-clock timed.
-* ``roofline`` -- HBM bound: algorithmic bytes per query from the oracle's
-  trace at the same ef (link lists read x their size + distance evaluations x
-  512 B), divided by the kernel time.
+* plain FP32: the smallest ef of the sweep 10..400 whose recall@10 meets the
+  target, device-resident timed loop.
+* learned + FP8 (``value``): the termination network is trained on the GPU
+  from checkpoint traces of 20,000 training queries (a query stream disjoint
+  from the 10,000 evaluation queries), its cap and logit threshold
+  calibrated on a held-out third of them; K launches over the 10,000 resident
+  queries, timed with CUDA events on the launch stream.  If the evaluation
+  recall falls short of the target, the calibration target is raised (no
+  retraining) until it does not.
+* ``e2e``    -- the learned + FP8 search through the C ABI (hnswgpu_search)
+  with pinned host buffers: host->device copy of the queries, search,
+  device->host copy of the labels/distances/counts every step, wall clock.
+* ``roofline`` -- HBM bound: algorithmic bytes per query of the headline
+  kernel from its own work counters (link lists x their size, fp8 rows of
+  144 B, float32 upper-layer and re-rank rows of 512 B), divided by the
+  kernel time; the plain beam's fraction (bytes from the oracle's trace at
+  the same ef) sits under ``plain_fp32``.
 * ``cpu_baseline`` -- the reference's own knn_query (oracle/_ref) on the
-  host cores of this machine, all threads, same index / queries / ef.
+  host cores of this machine, all threads, same index / queries, at the
+  plain operating point's ef.
 
 ``--impl reference`` times the reference's knn_query instead (CPU, all host
 threads; rank 0 only under torchrun).
@@ -64,7 +74,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", action="store_true", help="only run the timed loop (for ncu)")
     ap.add_argument("--tie-order", default="reference", choices=["reference", "id"],
-                    help="reference: heap replay, results identical to hnswlib; id: ties by internal id")
+                    help="tie order of --profile-steps: reference (heap replay, results identical to hnswlib) "
+                         "or id (ties by internal id)")
+    ap.add_argument("--train-queries", type=int, default=20_000, help="learned termination: training queries")
+    ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
+    ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
+    ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
     return ap.parse_args()
 
 
@@ -223,12 +238,129 @@ def recall(found, gt):
 
 
 # -------------------------------------------------------------- our GPU arm
-def run_ours(args, dist: Dist):
+class DeviceLoop:
+    """Device-resident batch search through the C ABI (HNSWGPU_DEVICE_PTRS):
+    queries and outputs stay in HBM, one kernel launch per step."""
+
+    def __init__(self, idx, q, dev, k=10):
+        import torch
+        from hnsw_rabitq_b200 import _capi
+        self.idx, self.k, self.nq, self.dev = idx, k, q.shape[0], dev
+        self.lib, self.capi = _capi.lib(), _capi
+        self.stream = torch.cuda.Stream(device=dev)
+        self.dq = torch.from_numpy(q).to(f"cuda:{dev}")
+        self.dl = torch.empty((self.nq, k), dtype=torch.int64, device=f"cuda:{dev}")
+        self.dd = torch.empty((self.nq, k), dtype=torch.float32, device=f"cuda:{dev}")
+        self.dc = torch.empty((self.nq,), dtype=torch.int32, device=f"cuda:{dev}")
+
+    def opts(self, ef, flags=0, precision=0, rerank=0):
+        o = self.capi.SearchOpts()
+        o.flags = self.capi.DEVICE_PTRS | flags
+        o.ef, o.precision, o.rerank = ef, precision, rerank
+        o.stream = self.stream.cuda_stream
+        return o
+
+    def step(self, o):
+        import ctypes as C
+        self.capi.check(self.lib.hnswgpu_search(self.idx._h, C.c_void_p(self.dq.data_ptr()), self.nq, self.k,
+                                                C.byref(o), C.c_void_p(self.dl.data_ptr()),
+                                                C.c_void_p(self.dd.data_ptr()), C.c_void_p(self.dc.data_ptr())))
+
+    def labels(self):
+        self.stream.synchronize()  # the search ran on this (non-blocking) stream
+        return self.dl.cpu().numpy().view(np.uint64)
+
+    def time(self, o, steps, warmup, dist, clocks=False):
+        """ms per step (max over ranks), CUDA events on the launch stream."""
+        import torch
+        with torch.cuda.stream(self.stream):
+            for _ in range(warmup):
+                self.step(o)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clk = ClockSampler(self.dev) if clocks else None
+        if clk:
+            clk.__enter__()
+        with torch.cuda.stream(self.stream):
+            ev0.record(self.stream)
+            for _ in range(steps):
+                self.step(o)
+            ev1.record(self.stream)
+        torch.cuda.synchronize()
+        if clk:
+            clk.__exit__()
+        dist.barrier()
+        return dist.max(ev0.elapsed_time(ev1)) / steps, (clk.summary() if clk else None)
+
+
+def e2e_qps(idx, q, o_flags, ef, precision, rerank, steps, warmup, dist, expect, k=10):
+    """Same search through the public C ABI with pinned HOST buffers: the
+    call copies the queries in, searches and copies labels / distances /
+    counts out every step (wall clock, max over ranks)."""
     import ctypes as C
 
     import torch
+    from hnsw_rabitq_b200 import _capi
+    lib = _capi.lib()
+    nq = q.shape[0]
+    hq = torch.from_numpy(q).pin_memory()
+    hl = torch.empty((nq, k), dtype=torch.int64).pin_memory()
+    hd = torch.empty((nq, k), dtype=torch.float32).pin_memory()
+    hc = torch.empty((nq,), dtype=torch.int32).pin_memory()
+    o = _capi.SearchOpts()
+    o.flags, o.ef, o.precision, o.rerank = o_flags, ef, precision, rerank
 
-    from hnsw_rabitq_b200 import Index, _capi
+    def call():
+        _capi.check(lib.hnswgpu_search(idx._h, C.c_void_p(hq.data_ptr()), nq, k, C.byref(o),
+                                       C.c_void_p(hl.data_ptr()), C.c_void_p(hd.data_ptr()),
+                                       C.c_void_p(hc.data_ptr())))
+
+    for _ in range(warmup):
+        call()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = dist.max(time.perf_counter() - t0)
+    assert np.array_equal(hl.numpy().view(np.uint64), expect)
+    return dist.world * nq * steps / dt, int(q.nbytes), int(nq * k * 8 + nq * k * 4 + nq * 4)
+
+
+def plain_sweep(idx, loop, q, gt, target, tie_order, fixed_ef=0):
+    """Smallest ef of the sweep whose recall@10 meets the target."""
+    from hnsw_rabitq_b200 import _capi
+    flags = _capi.EXACT_TIES if tie_order == "reference" else 0
+    sweep, ef_star = [], fixed_ef
+    for ef in ([fixed_ef] if fixed_ef else EFS):
+        loop.step(loop.opts(ef, flags))
+        r = recall(loop.labels(), gt) if gt is not None else None
+        sweep.append({"ef": ef, "recall": None if r is None else round(r, 5)})
+        if r is not None and r >= target and not ef_star:
+            ef_star = ef
+            break
+    return (ef_star or EFS[-1]), flags, sweep
+
+
+def train_termination(idx, args):
+    """Learned termination for the FP8 beam: trained on queries drawn from the
+    same mixture (a stream disjoint from the evaluation queries), cap and
+    threshold calibrated on a held-out share of them."""
+    from hnsw_rabitq_b200 import learned
+    from hnsw_rabitq_b200.datasets import gmm_1m_128_queries
+    tq = gmm_1m_128_queries(args.train_queries, stream_seed=1000)
+    t0 = time.perf_counter()
+    model, rep = learned.fit(idx, tq, k=10, ef_cap=args.term_cap, period=args.term_period,
+                             target_recall=args.target_recall + 0.005, precision="fp8", rerank=args.rerank,
+                             epochs=20, seed=0)
+    return model, rep, tq, time.perf_counter() - t0
+
+
+def run_ours(args, dist: Dist):
+    import torch
+
+    from hnsw_rabitq_b200 import Index, _capi, learned
 
     dev = dist.local
     torch.cuda.set_device(dev)
@@ -237,131 +369,105 @@ def run_ours(args, dist: Dist):
     gt = None if args.profile_steps else ground_truth(x, q)
     idx = Index("l2", 128)
     idx.device = dev
-    idx.tie_order = args.tie_order
     idx.load_index(path)
     info = idx._info()
-    if args.profile_steps and not args.ef:
-        raise SystemExit("--profile-steps needs --ef")
-
-    # ---- operating point: smallest ef with recall@10 >= target
-    sweep = []
-    ef_star = args.ef
-    if not ef_star:
-        for ef in EFS:
-            idx.set_ef(ef)
-            t = time.perf_counter()
-            lab, _ = idx.knn_query(q, k=10)
-            dt = time.perf_counter() - t
-            r = recall(lab, gt)
-            sweep.append({"ef": ef, "recall": round(r, 5), "qps_e2e_untimed": round(q.shape[0] / dt, 1)})
-            if r >= args.target_recall and not ef_star:
-                ef_star = ef
-                break
-        if not ef_star:
-            ef_star = EFS[-1]
-    idx.set_ef(ef_star)
-    lab, _ = idx.knn_query(q, k=10)
-    rec = recall(lab, gt) if gt is not None else None
-
-    # ---- device-resident timed loop
-    lib = _capi.lib()
+    _capi.check(_capi.lib().hnswgpu_build_traversal_copy(idx._h, _capi.PREC_FP8))
+    loop = DeviceLoop(idx, q, dev)
     nq, k = q.shape[0], 10
-    stream = torch.cuda.Stream(device=dev)
-    dq = torch.from_numpy(q).to(f"cuda:{dev}")
-    dl = torch.empty((nq, k), dtype=torch.int64, device=f"cuda:{dev}")
-    dd = torch.empty((nq, k), dtype=torch.float32, device=f"cuda:{dev}")
-    dc = torch.empty((nq,), dtype=torch.int32, device=f"cuda:{dev}")
-    tie_flag = _capi.EXACT_TIES if args.tie_order == "reference" else 0
-    opts = _capi.SearchOpts()
-    opts.flags = _capi.DEVICE_PTRS | tie_flag
-    opts.ef = ef_star
-    opts.stream = stream.cuda_stream
-
-    def step():
-        _capi.check(lib.hnswgpu_search(idx._h, C.c_void_p(dq.data_ptr()), nq, k, C.byref(opts),
-                                       C.c_void_p(dl.data_ptr()), C.c_void_p(dd.data_ptr()),
-                                       C.c_void_p(dc.data_ptr())))
-
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step()
-    torch.cuda.synchronize()
-    # the device results equal the host-path results
-    assert np.array_equal(dl.cpu().numpy().view(np.uint64), lab)
-    dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(dev) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record(stream)
-            for _ in range(args.steps):
-                step()
-            ev1.record(stream)
-        torch.cuda.synchronize()
-    dist.barrier()
-    ms_local = ev0.elapsed_time(ev1)
-    ms_total = dist.max(ms_local)
-    ms_step = ms_total / args.steps
-    value = dist.world * nq * args.steps / (ms_total / 1e3)
     if args.profile_steps:
+        if not args.ef:
+            raise SystemExit("--profile-steps needs --ef")
+        tie = _capi.EXACT_TIES if args.tie_order == "reference" else 0
+        loop.time(loop.opts(args.ef, tie), args.steps, args.warmup, dist)
         return None
 
-    # ---- e2e through the C ABI with pinned host buffers
-    hq = torch.from_numpy(q).pin_memory()
-    hl = torch.empty((nq, k), dtype=torch.int64).pin_memory()
-    hd = torch.empty((nq, k), dtype=torch.float32).pin_memory()
-    hc = torch.empty((nq,), dtype=torch.int32).pin_memory()
-    eopts = _capi.SearchOpts()
-    eopts.flags = tie_flag
-    eopts.ef = ef_star
+    # ---- plain FP32 beam (the comparison), both tie orders
+    plain = {}
+    for order in ("id", "reference"):
+        ef_p, fl_p, sw = plain_sweep(idx, loop, q, gt, args.target_recall, order, args.ef)
+        o = loop.opts(ef_p, fl_p)
+        loop.step(o)
+        lab_p = loop.labels()
+        ms_p, _ = loop.time(o, args.steps, args.warmup, dist)
+        plain[order] = {"ef": ef_p, "recall@10": round(recall(lab_p, gt), 5), "ms_per_step": round(ms_p, 4),
+                        "qps": round(dist.world * nq / (ms_p / 1e3), 1), "sweep": sw}
 
-    def e2e_step():
-        _capi.check(lib.hnswgpu_search(idx._h, C.c_void_p(hq.data_ptr()), nq, k, C.byref(eopts),
-                                       C.c_void_p(hl.data_ptr()), C.c_void_p(hd.data_ptr()),
-                                       C.c_void_p(hc.data_ptr())))
-
-    for _ in range(args.warmup):
-        e2e_step()
-    dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    e2e_s = dist.max(time.perf_counter() - t0)
-    e2e_qps = dist.world * nq * args.steps / e2e_s
-    assert np.array_equal(hl.numpy().view(np.uint64), lab)
+    # ---- learned termination + FP8 traversal + FP32 re-rank (the headline)
+    model, rep, tq, fit_s = train_termination(idx, args)
+    flags = _capi.LEARNED_STOP
+    tgt = args.target_recall + 0.005
+    for _ in range(6):
+        o = loop.opts(model.ef_cap, flags, _capi.PREC_FP8, args.rerank)
+        loop.step(o)
+        lab = loop.labels()
+        rec = recall(lab, gt)
+        if rec >= args.target_recall:
+            break
+        # the held-out calibration fell short on the evaluation queries:
+        # tighten its target (no retraining) and recalibrate
+        tgt += 0.005
+        hold = tq[: max(1, len(tq) // 3)]
+        hgt = idx.knn_query_exact(hold, 10)[0]
+        cap, thr, _ = learned.calibrate(idx, hold, hgt, 10, model, tgt, caps=sorted({c for c, *_ in rep["curve"]}))
+        model.ef_cap, model.threshold = cap, thr
+        idx.set_termination_model(model)
+    ms_step, clk = loop.time(o, args.steps, args.warmup, dist, clocks=True)
+    value = dist.world * nq * args.steps / (ms_step * args.steps / 1e3)
+    _, _, _, trace = idx.knn_query_traced(q, 10, ef=model.ef_cap, tie_order="id", precision="fp8",
+                                          rerank=args.rerank, learned=True)
+    e2e, h2d, d2h = e2e_qps(idx, q, flags, model.ef_cap, _capi.PREC_FP8, args.rerank, args.steps, args.warmup,
+                            dist, lab)
 
     out = None
     if dist.rank == 0:
         peak, peak_kind = peaks()
-        cpu, bytes_per_q = cpu_baseline(args, path, q, ef_star, info) if not args.no_cpu_baseline else (None, None)
-        roof = None
-        if bytes_per_q:
-            per_launch = bytes_per_q * nq
-            achieved = per_launch / (ms_step / 1e3) / 1e9
-            roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                    "frac": round(achieved / peak, 4), "traffic": committed_traffic(args.tie_order, ef_star),
-                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                    else "fallback 6.65 TB/s",
-                    "algorithmic_bytes_per_query": round(bytes_per_q, 1)}
+        # algorithmic bytes of the headline kernel from its own work counters:
+        # upper-layer link lists (4 + 4 maxM) and float32 rows; level-0 link
+        # lists (4 + 4 maxM0) and fp8 rows (128 B + 16 B scale block); the
+        # float32 re-rank of the pool (at most ef_cap rows of 512 B)
+        fp8_row = 128 + 16
+        rr = args.rerank or model.ef_cap
+        bq = (trace[:, 0] * (4 + 4 * info.maxM) + trace[:, 1] * 512 + trace[:, 2] * (4 + 4 * info.maxM0)
+              + trace[:, 3] * fp8_row).mean() + min(rr, model.ef_cap) * 512
+        achieved = bq * nq / (ms_step / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": committed_traffic("learned_fp8", model.ef_cap),
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "algorithmic_bytes_per_query": round(float(bq), 1),
+                "kernel": "hnsw_search_kernel<L2, fp8 traversal, learned stop>"}
+        cpu, bytes_q = (cpu_baseline(args, path, q, plain["id"]["ef"], info) if not args.no_cpu_baseline
+                        else (None, None))
+        if bytes_q:
+            ms_id = plain["id"]["ms_per_step"]
+            plain["id"]["roofline_hbm_frac"] = round(bytes_q * nq / (ms_id / 1e3) / 1e9 / peak, 4)
+            plain["id"]["algorithmic_bytes_per_query"] = round(bytes_q, 1)
         out = {
-            "metric": "QPS at recall@10>=0.95 (plain FP32 GPU HNSW, 1M x 128 L2)",
+            "metric": "QPS at recall@10>=0.95, learned termination + FP8 traversal (FP32 re-rank) GPU HNSW, "
+                      "1M x 128 L2",
             "value": round(value, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "vs_baseline": None, "dtype": "fp8 traversal, f32 accumulation and re-rank", "data": "synthetic",
             "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
                                    "HNSW M=16 efc=200, 10,000 queries, k=10",
-                       "method": "plain fp32 beam, reference semantics, tie order: " + args.tie_order,
-                       "ef": ef_star,
-                       "recall@10": round(rec, 5), "global_batch": nq, "parallelism": f"replicas x{dist.world}",
-                       "l2_flush": "not needed: index data 640 MB > 126 MB L2",
-                       "index_device_bytes": info.device_bytes},
-            "sweep": sweep,
+                       "method": "learned early termination (6-64-64-1 fp16 MLP every "
+                                 f"{model.period} expansions) over an fp8 e4m3 per-row-scaled beam, fp32 re-rank",
+                       "ef_cap": model.ef_cap, "logit_threshold": model.threshold,
+                       "recall@10": round(rec, 5), "mean_l0_expansions": round(float(trace[:, 2].mean()), 2),
+                       "global_batch": nq, "parallelism": f"replicas x{dist.world}",
+                       "l2_flush": "not needed: index data 640 MB + fp8 copy 144 MB > 126 MB L2",
+                       "index_device_bytes": int(idx._info().device_bytes),
+                       "training": {"queries": int(tq.shape[0]), "samples": rep["samples"],
+                                    "positive_share": round(rep["positive"], 4),
+                                    "loss_first_last": [round(rep["loss"][0], 4), round(rep["loss"][-1], 4)],
+                                    "trained_cap": rep["trained_cap"], "fit_seconds": round(fit_s, 1)}},
+            "plain_fp32": plain,
+            "speedup_vs_plain_fp32": {o2: round(value / plain[o2]["qps"], 3) for o2 in plain},
             "roofline": roof,
             "cpu_baseline": cpu,
-            "e2e": {"value": round(e2e_qps, 1), "unit": "queries/s", "h2d_bytes_per_step": int(q.nbytes),
-                    "d2h_bytes_per_step": int(nq * k * 8 + nq * k * 4 + nq * 4)},
+            "e2e": {"value": round(e2e, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
-            "clocks": clk.summary(),
+            "clocks": clk,
         }
     return out
 
@@ -437,13 +543,16 @@ def run_reference(args, dist: Dist):
         lab, _ = p.knn_query(q, k=10, num_threads=threads)
     dt = time.perf_counter() - t0
     qps = q.shape[0] * args.steps / dt
-    return {"impl": "reference", "metric": "QPS at recall@10>=0.95 (plain FP32 GPU HNSW, 1M x 128 L2)",
+    return {"impl": "reference",
+            "metric": "QPS at recall@10>=0.95, learned termination + FP8 traversal (FP32 re-rank) GPU HNSW, "
+                      "1M x 128 L2",
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
                                    "HNSW M=16 efc=200, 10,000 queries, k=10",
-                       "method": "hnswlib 0.9.0 knn_query (CPU)", "ef": ef_star,
+                       "method": "hnswlib 0.9.0 knn_query (CPU, fixed ef: the reference has no learned or "
+                                 "FP8 search)", "ef": ef_star,
                        "recall@10_sample500": round(recall(lab[:500], gt), 5)},
             "cpu_baseline": {"value": round(qps, 1), "unit": "queries/s", "cores": threads, "kind": "reference",
                              "sample": f"{q.shape[0]} queries per step"},

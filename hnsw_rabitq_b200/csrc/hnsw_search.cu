@@ -56,7 +56,8 @@ struct WarpSmem {
     uint64_t* extra;
     uint32_t* vis;
     uint64_t* topheap;   // tie-exact mode: replay of top_candidates
-    uint64_t* candheap;  // tie-exact mode: replay of candidate_set
+    SplitHeap candheap;  // tie-exact mode: replay of candidate_set
+    int cand_total;      // tie-exact mode: its capacity (shared + spill)
     uint64_t* accbuf;    // tie-exact mode: accepted keys of one chunk, link order
     uint64_t* evbuf;     // tie-exact mode: keys evicted from top_candidates
 };
@@ -662,7 +663,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
                 int cn = csz, tn = tsz;
                 for (int t = 0; t < na; t++) {
                     const uint64_t e = s.accbuf[t];
-                    if (cn < (int)p.cand_cap) ref_heap_push(s.candheap, cn, e, CandLess());
+                    if (cn < s.cand_total) ref_heap_push(s.candheap, cn, e, CandLess());
                     else ovf = 1;
                     ref_heap_push(s.topheap, tn, e, TopLess());
                     if (tn > ef) s.evbuf[nev++] = ref_heap_pop(s.topheap, tn, TopLess());
@@ -700,7 +701,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             term_features((float)ct.l0_exp, d1, dk, dn, d0, qn, (float)(ct.l0_exp - last_change),
                           1.0f / (float)p.term_period, fe);
             if (TERM == 1) {
-                if (nckpt < p.term_max_ckpt) {
+                if (nckpt + 1 < p.term_max_ckpt) {  // the last row is kept for the final state
                     const size_t row = (size_t)qi * p.term_max_ckpt + nckpt;
                     if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
                     for (int i = lane; i < kq; i += 32)
@@ -743,8 +744,8 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             csz--;
             __syncwarp();
             if (spec && top_id != next) {
-                // cannot happen when the prediction holds; recover by refetching
-                status |= HNSWGPU_STATUS_TIMEOUT_BIT;
+                // only after a full candidate heap dropped a push (flagged as
+                // an overflow): fetch the actual top instead
                 if (fn.n0 > 0) {
                     mbar_wait(s.bar, phase);
                     phase ^= 1u;
@@ -759,7 +760,22 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         ct.l0_exp += 1;
         PT_MARK(2);
     }
-    if (TERM == 1 && lane == 0) p.ckpt_count[qi] = min(nckpt, p.term_max_ckpt);
+    if (TERM == 1 && p.term_max_ckpt > 0) {
+        // final row: the beam's top-k when it ends (before any re-rank) and
+        // the features of that state; labels of the earlier rows refer to it
+        const uint32_t r = min(nckpt, p.term_max_ckpt - 1);
+        const size_t row = (size_t)qi * p.term_max_ckpt + r;
+        const int kk = min(kq, psize);
+        const float dk = funkey(khi(s.pool[kk - 1]));
+        float fe[kTermFeatures];
+        term_features((float)ct.l0_exp, funkey(khi(s.pool[0])), dk, dk, d0, qn, (float)(ct.l0_exp - last_change),
+                      1.0f / (float)p.term_period, fe);
+        if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
+        for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+        if (lane == 0) p.ckpt_count[qi] = r + 1;
+    } else if (TERM == 1 && lane == 0) {
+        p.ckpt_count[qi] = 0;
+    }
     return true;
 }
 
@@ -1063,7 +1079,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
                         uint64_t e = s.accbuf[t];
                         const bool al = ((uint32_t)e & EXP_BIT) != 0;
                         e &= KEY_MASK;
-                        if (cn < (int)p.cand_cap) ref_heap_push(s.candheap, cn, e, CandLess());
+                        if (cn < s.cand_total) ref_heap_push(s.candheap, cn, e, CandLess());
                         else ovf = 1;
                         if (al) {
                             ref_heap_push(s.topheap, tn, e, TopLess());
@@ -1175,7 +1191,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_k
     s.extra = reinterpret_cast<uint64_t*>(base + p.off_extra);
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
     s.topheap = reinterpret_cast<uint64_t*>(base + p.off_top);
-    s.candheap = reinterpret_cast<uint64_t*>(base + p.off_cand);
+    {
+        const uint32_t gw = blockIdx.x * kWarpsPerBlock + warp;
+        const bool spill = p.cand_spill != nullptr && gw < p.cand_spill_warps;
+        s.candheap = SplitHeap{reinterpret_cast<uint64_t*>(base + p.off_cand),
+                               spill ? p.cand_spill + (size_t)gw * p.cand_spill_cap : nullptr, (int)p.cand_cap};
+        s.cand_total = (int)p.cand_cap + (spill ? (int)p.cand_spill_cap : 0);
+    }
     s.accbuf = reinterpret_cast<uint64_t*>(base + p.off_acc);
     s.evbuf = reinterpret_cast<uint64_t*>(base + p.off_ev);
     if (lane == 0) mbar_init(s.bar, 1);

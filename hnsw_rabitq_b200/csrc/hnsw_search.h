@@ -29,10 +29,13 @@ constexpr int kTermOffB2 = kTermOffW2 + kTermHidden * kTermHidden;
 constexpr int kTermOffW3 = kTermOffB2 + kTermHidden;
 constexpr int kTermOffB3 = kTermOffW3 + kTermHidden;
 constexpr int kTermParams = kTermOffB3 + 1;
-// Inference form (device): float mu[6], inv_sigma[6], b1[64], b2[64], b3,
-// pad[3] (kTermPackedFloats floats), then half W1[64][6], W2[64][64], w3[64].
+// Inference form (device), laid out for coalesced warp reads: float mu[6],
+// inv_sigma[6], b1[64], b2[64], b3, pad[3] (kTermPackedFloats floats); then
+// half W1[64][8] (rows padded to 16 bytes), W2 as half2 [32][64] holding
+// (W2[u][2p], W2[u][2p+1]) at [p][u], and w3[64].
 constexpr int kTermPackedFloats = 2 * kTermFeatures + 2 * kTermHidden + 4;
-constexpr int kTermPackedHalves = kTermHidden * kTermFeatures + kTermHidden * kTermHidden + kTermHidden;
+constexpr int kTermW1Stride = 8;
+constexpr int kTermPackedHalves = kTermHidden * kTermW1Stride + kTermHidden * kTermHidden + kTermHidden;
 constexpr size_t kTermPackedBytes = (size_t)kTermPackedFloats * 4 + (size_t)kTermPackedHalves * 2;
 // Convert the float32 parameter vector (kTermParams) into the inference form.
 void pack_term_model(const float* params, unsigned char* out);
@@ -71,7 +74,10 @@ struct SearchParams {
     uint32_t links_unique;        // no level-0 list repeats an id (checked at load)
     uint32_t exact;               // replay the reference's heaps (tie order exact)
     uint32_t pool_cap;            // ef (canonical) or ef + 32 (tie-exact)
-    uint32_t cand_cap;            // tie-exact: candidate heap capacity
+    uint32_t cand_cap;            // tie-exact: candidate heap entries in shared memory
+    uint32_t cand_spill_cap;      // tie-exact: further entries per warp in cand_spill
+    uint32_t cand_spill_warps;    // warps that cand_spill has room for
+    uint64_t* cand_spill;         // tie-exact: global tail of each warp's candidate heap
     // outputs
     uint64_t* out_labels;
     float* out_dists;

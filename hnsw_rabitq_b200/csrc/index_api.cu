@@ -112,6 +112,7 @@ struct hnswgpu_index {
     DevBuf<float> bf_norms;    // brute force: per-row helper values
     DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
     DevBuf<unsigned char> term_model;  // learned termination: packed network
+    DevBuf<uint64_t> cand_spill;       // tie-exact mode: candidate-heap tails
     uint32_t term_period = 0;
     float term_logit = 0.f;
     std::mutex mu;
@@ -430,7 +431,7 @@ void ensure_traversal_copy(hnswgpu_index* h, uint32_t prec) {
 // work_counter / done_counter / status are left for the caller to set).
 hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef,
                                   const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace,
-                                  bool exact, uint32_t prec = 0, uint32_t rerank = 0) {
+                                  bool exact, uint32_t prec = 0, uint32_t rerank = 0, bool spill = false) {
     hnswgpu::SearchParams p{};
     p.vecs = h->vecs.p;
     p.links0 = h->links0.p;
@@ -470,8 +471,17 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     p.extra_cap = p.bare ? 0u : std::max<uint32_t>(128u, 4u * p.ef);
     p.exact = exact ? 1u : 0u;
     p.pool_cap = exact ? p.ef + 32u : p.ef;
-    // the reference's candidate heap is never pruned; it peaks near 8 x ef
-    p.cand_cap = exact ? std::max<uint32_t>(256u, 10u * p.ef) : 0u;
+    // The reference's candidate heap is never pruned.  Its peak per query
+    // (oracle traces, 1M x 128, M=16): median ~2.5-3 x ef, 99th percentile
+    // ~7-8 x ef, maximum ~10 x ef at small ef.  With a spill area the
+    // shared-memory head holds 4 x ef and the global tail 24 x ef more;
+    // without one (the allocation-free entry point) shared memory holds it all.
+    if (exact && spill) {
+        p.cand_cap = std::max<uint32_t>(128u, 4u * p.ef);
+        p.cand_spill_cap = std::max<uint32_t>(1024u, 24u * p.ef);
+    } else {
+        p.cand_cap = exact ? std::max<uint32_t>(512u, 12u * p.ef) : 0u;
+    }
     p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
     if (prec) {
         if (!p.fast16 || !p.bare || p.maxM0 > 32 || exact)
@@ -546,9 +556,20 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
               uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact, uint32_t prec,
               uint32_t rerank, const TermCfg* term) {
     if (prec) ensure_traversal_copy(h, prec);
-    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank);
+    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank, true);
     apply_term(h, p, term);
     p.status = h->status.p;
+    if (exact) {
+        // one tail per resident warp: at most 32 CTAs per SM
+        const uint64_t warps = (uint64_t)h->num_sms * 32u * hnswgpu::kWarpsPerBlock;
+        const uint64_t need = warps * p.cand_spill_cap;
+        if (h->cand_spill.n < need) {
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            h->cand_spill.alloc(need);
+        }
+        p.cand_spill = h->cand_spill.p;
+        p.cand_spill_warps = (uint32_t)warps;
+    }
 #ifdef HNSWGPU_PHASE_TIMING
     static unsigned long long* phase_buf = nullptr;
     if (!phase_buf) {

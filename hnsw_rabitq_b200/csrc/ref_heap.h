@@ -40,8 +40,11 @@ struct CandLess {
     }
 };
 
-template <class Less>
-__host__ __device__ __forceinline__ void ref_heap_push(uint64_t* h, int& n, uint64_t v, Less less) {
+// `A` is a pointer or any type whose operator[] returns a uint64_t& (the
+// search keeps the top levels of its candidate heap in shared memory and
+// the deeper ones in a global spill area).
+template <class A, class Less>
+__host__ __device__ __forceinline__ void ref_heap_push(A h, int& n, uint64_t v, Less less) {
     int hole = n++;
     while (hole > 0) {
         int parent = (hole - 1) / 2;
@@ -53,8 +56,8 @@ __host__ __device__ __forceinline__ void ref_heap_push(uint64_t* h, int& n, uint
 }
 
 // Removes and returns the top entry (n >= 1).
-template <class Less>
-__host__ __device__ __forceinline__ uint64_t ref_heap_pop(uint64_t* h, int& n, Less less) {
+template <class A, class Less>
+__host__ __device__ __forceinline__ uint64_t ref_heap_pop(A h, int& n, Less less) {
     const uint64_t top = h[0];
     const int len = n - 1;
     if (len > 0) {
@@ -82,5 +85,14 @@ __host__ __device__ __forceinline__ uint64_t ref_heap_pop(uint64_t* h, int& n, L
     n = len;
     return top;
 }
+
+// Heap storage split between a shared-memory head (entries [0, cap_s)) and a
+// global-memory tail (entries [cap_s, cap_s + cap_g)).
+struct SplitHeap {
+    uint64_t* s;
+    uint64_t* g;
+    int cap_s;
+    __host__ __device__ __forceinline__ uint64_t& operator[](int i) const { return i < cap_s ? s[i] : g[i - cap_s]; }
+};
 
 }  // namespace hnswgpu

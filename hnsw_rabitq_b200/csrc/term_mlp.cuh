@@ -36,7 +36,8 @@ __device__ __forceinline__ void term_features(float e, float d1, float dk, float
 
 // The network's logit for one feature vector (identical in every lane),
 // computed by the whole warp: lane j owns hidden units 2j and 2j + 1 of both
-// hidden layers.  `m` is the packed inference form (pack_term_model).
+// hidden layers.  `m` is the packed inference form (pack_term_model), read
+// with coalesced loads: each step of layer 2 reads 256 contiguous bytes.
 __device__ __forceinline__ float term_logit(const float* __restrict__ m, const float f[kTermFeatures], int lane) {
     constexpr unsigned kFull = 0xffffffffu;
     const float* mu = m;
@@ -45,36 +46,42 @@ __device__ __forceinline__ float term_logit(const float* __restrict__ m, const f
     const float* b2 = b1 + kTermHidden;
     const float b3 = __ldg(b2 + kTermHidden);
     const __half* W1 = reinterpret_cast<const __half*>(m + kTermPackedFloats);
-    const __half* W2 = W1 + kTermHidden * kTermFeatures;
-    const __half* w3 = W2 + kTermHidden * kTermHidden;
+    const uint2* W2 = reinterpret_cast<const uint2*>(W1 + kTermHidden * kTermW1Stride);
+    const __half2* w3 = reinterpret_cast<const __half2*>(W1 + kTermHidden * kTermW1Stride + kTermHidden * kTermHidden);
     float x[kTermFeatures];
 #pragma unroll
     for (int i = 0; i < kTermFeatures; i++) x[i] = (f[i] - __ldg(mu + i)) * __ldg(inv_sigma + i);
-    float h1[2];
+    // layer 1: rows 2j and 2j + 1 of W1 are 32 contiguous bytes
+    const float2 bb1 = __ldg(reinterpret_cast<const float2*>(b1) + lane);
+    float h1[2] = {bb1.x, bb1.y};
 #pragma unroll
     for (int s = 0; s < 2; s++) {
-        const int u = 2 * lane + s;
-        float acc = __ldg(b1 + u);
+        const uint4 raw = __ldg(reinterpret_cast<const uint4*>(W1) + 2 * lane + s);
+        const __half2* w = reinterpret_cast<const __half2*>(&raw);
+        float acc = h1[s];
 #pragma unroll
-        for (int i = 0; i < kTermFeatures; i++) acc = fmaf(__half2float(W1[u * kTermFeatures + i]), x[i], acc);
+        for (int i = 0; i < kTermFeatures / 2; i++) {
+            const float2 wf = __half22float2(w[i]);
+            acc = fmaf(wf.y, x[2 * i + 1], fmaf(wf.x, x[2 * i], acc));
+        }
         h1[s] = fmaxf(acc, 0.f);
     }
     // layer 2: unit pair (2p, 2p + 1) of layer 1 lives in lane p
-    float acc0 = __ldg(b2 + 2 * lane), acc1 = __ldg(b2 + 2 * lane + 1);
-    const __half2* r0 = reinterpret_cast<const __half2*>(W2 + (2 * lane) * kTermHidden);
-    const __half2* r1 = reinterpret_cast<const __half2*>(W2 + (2 * lane + 1) * kTermHidden);
+    const float2 bb2 = __ldg(reinterpret_cast<const float2*>(b2) + lane);
+    float acc0 = bb2.x, acc1 = bb2.y;
 #pragma unroll 8
     for (int pr = 0; pr < kTermHidden / 2; pr++) {
         const float ha = __shfl_sync(kFull, h1[0], pr), hb = __shfl_sync(kFull, h1[1], pr);
-        const float2 w0 = __half22float2(r0[pr]), w1 = __half22float2(r1[pr]);
+        const uint2 raw = __ldg(W2 + pr * (kTermHidden / 2) + lane);
+        const float2 w0 = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+        const float2 w1 = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
         acc0 = fmaf(w0.y, hb, fmaf(w0.x, ha, acc0));
         acc1 = fmaf(w1.y, hb, fmaf(w1.x, ha, acc1));
     }
-    const float part = fmaf(__half2float(w3[2 * lane + 1]), fmaxf(acc1, 0.f),
-                            __half2float(w3[2 * lane]) * fmaxf(acc0, 0.f));
-    float sum = part;
+    const float2 o = __half22float2(w3[lane]);
+    float sum = fmaf(o.y, fmaxf(acc1, 0.f), o.x * fmaxf(acc0, 0.f));
 #pragma unroll
-    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+    for (int s = 16; s; s >>= 1) sum += __shfl_xor_sync(kFull, sum, s);
     return sum + b3;
 }
 

@@ -45,9 +45,15 @@ void pack_term_model(const float* params, unsigned char* out) {
     f[2 * kTermFeatures + 2 * kTermHidden] = params[kTermOffB3];
     for (int i = 2 * kTermFeatures + 2 * kTermHidden + 1; i < kTermPackedFloats; i++) f[i] = 0.f;
     __half* h = reinterpret_cast<__half*>(out + (size_t)kTermPackedFloats * 4);
-    for (int i = 0; i < kTermHidden * kTermFeatures; i++) h[i] = __float2half_rn(params[kTermOffW1 + i]);
-    h += kTermHidden * kTermFeatures;
-    for (int i = 0; i < kTermHidden * kTermHidden; i++) h[i] = __float2half_rn(params[kTermOffW2 + i]);
+    for (int u = 0; u < kTermHidden; u++)
+        for (int i = 0; i < kTermW1Stride; i++)
+            h[u * kTermW1Stride + i] = __float2half_rn(i < kTermFeatures ? params[kTermOffW1 + u * kTermFeatures + i] : 0.f);
+    h += kTermHidden * kTermW1Stride;
+    for (int pr = 0; pr < kTermHidden / 2; pr++)
+        for (int u = 0; u < kTermHidden; u++) {
+            h[(pr * kTermHidden + u) * 2] = __float2half_rn(params[kTermOffW2 + u * kTermHidden + 2 * pr]);
+            h[(pr * kTermHidden + u) * 2 + 1] = __float2half_rn(params[kTermOffW2 + u * kTermHidden + 2 * pr + 1]);
+        }
     h += kTermHidden * kTermHidden;
     for (int i = 0; i < kTermHidden; i++) h[i] = __float2half_rn(params[kTermOffW3 + i]);
 }

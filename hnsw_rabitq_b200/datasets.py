@@ -62,6 +62,16 @@ def gmm_1m_128(n: int = 1_000_000, nq: int = 10_000, dim: int = 128, n_comp: int
     return x, q
 
 
+def gmm_1m_128_queries(nq: int, stream_seed: int, dim: int = 128, n_comp: int = 1024, sigma: float = 20.0,
+                       seed: int = 0) -> np.ndarray:
+    """More queries from the mixture of ``gmm_1m_128(seed=seed)`` (same
+    centres), drawn from ``default_rng(stream_seed)``: the training queries
+    of the learned termination, disjoint from the evaluation queries when
+    ``stream_seed`` differs from ``seed + 1``."""
+    centres = _gmm_centres_u255(n_comp, dim, seed + 7)
+    return _draw_gmm_u255(np.random.default_rng(stream_seed), centres, nq, sigma)
+
+
 def _unit_rows(a: np.ndarray) -> np.ndarray:
     a /= np.linalg.norm(a, axis=1, keepdims=True).astype(np.float32)
     return a

@@ -93,19 +93,23 @@ def recall(labels: np.ndarray, gt: np.ndarray) -> float:
 def checkpoint_dataset(index, ck: dict, gt: np.ndarray):
     """(features [n, 6], labels [n]) of every recorded checkpoint: label 1 when
     the checkpoint's top-k holds at least as many true neighbours as the
-    search's final answer."""
+    beam's final top-k (the last row of each query, itself not a sample).
+    Both are taken before any re-rank, so low-precision searches compare
+    like with like."""
     nq, R, k = ck["ids"].shape
     lab_of = index.labels_by_internal_id()
     gt = gt.astype(np.uint64)
-    final = _hits(ck["labels"].astype(np.uint64), gt)            # [nq]
+    n = ck["nckpt"].astype(np.int64)
     X, Y = [], []
     for a in range(0, nq, 512):
         b = min(nq, a + 512)
         ids = ck["ids"][a:b]
-        valid = np.arange(R)[None, :] < ck["nckpt"][a:b, None]      # [q, R]
         lab = np.where(ids == _NONE, np.uint64(2**64 - 1), lab_of[np.minimum(ids, len(lab_of) - 1)])
-        now = _hits(lab, gt[a:b, None, :])                          # [q, R]
-        y = (now >= final[a:b, None]).astype(np.float32)
+        hits = _hits(lab, gt[a:b, None, :])                         # [q, R]
+        last = np.maximum(n[a:b] - 1, 0)
+        final = hits[np.arange(b - a), last]                        # [q]
+        valid = np.arange(R)[None, :] < last[:, None]               # rows before the final one
+        y = (hits >= final[:, None]).astype(np.float32)
         X.append(ck["feat"][a:b][valid])
         Y.append(y[valid])
     return np.concatenate(X).astype(np.float32), np.concatenate(Y).astype(np.float32)
@@ -153,39 +157,50 @@ def logits(params: np.ndarray, feats: np.ndarray, device: int = 0) -> np.ndarray
     return out
 
 
-def evaluate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, threshold: float):
+def evaluate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, threshold: float,
+             ef_cap: Optional[int] = None):
     """(recall@k, mean level-0 expansions) of the learned search at this
-    threshold."""
-    m = TerminationModel(model.params, model.period, float(threshold), model.ef_cap, model.precision, model.rerank)
+    threshold and cap."""
+    cap = int(ef_cap or model.ef_cap)
+    m = TerminationModel(model.params, model.period, float(threshold), cap, model.precision, model.rerank)
     index.set_termination_model(m)
-    lab, _, cnt, tr = index.knn_query_traced(queries, k, ef=model.ef_cap, tie_order="id", precision=model.precision,
+    lab, _, cnt, tr = index.knn_query_traced(queries, k, ef=cap, tie_order="id", precision=model.precision,
                                              rerank=model.rerank, learned=True)
     return recall(lab, gt), float(tr[:, 2].mean())
 
 
 def calibrate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, target_recall: float,
-              candidates: Optional[np.ndarray] = None):
-    """Earliest-stopping logit threshold whose recall@k on these queries
-    meets the target; returns (threshold, curve [(threshold, recall,
-    mean expansions)])."""
+              caps=None, candidates: Optional[np.ndarray] = None):
+    """Cap and logit threshold of the cheapest learned search (fewest mean
+    level-0 expansions) whose recall@k on these queries meets the target.
+    A threshold of +inf never stops early, so each cap's plain fixed-ef
+    search is among the candidates.  Returns (cap, threshold, curve
+    [(cap, threshold, recall, mean expansions)]); (max cap, +inf) when no
+    candidate meets the target."""
+    caps = sorted(caps or [model.ef_cap])
     if candidates is None:
-        candidates = np.concatenate([np.linspace(8.0, -4.0, 25), [-6.0, -8.0]])
+        candidates = np.linspace(6.0, -4.0, 21)
+    ths = [float("inf")] + sorted((float(t) for t in candidates), reverse=True)
     curve = []
-    best = float("inf")
-    for t in sorted(candidates, reverse=True):
-        r, e = evaluate(index, queries, gt, k, model, t)
-        curve.append((float(t), r, e))
-        if r >= target_recall:
-            best = float(t)
-    return best, curve
+    best = (float("inf"), caps[-1], float("inf"))
+    for cap in caps:
+        for t in ths:
+            r, e = evaluate(index, queries, gt, k, model, t, cap)
+            curve.append((int(cap), t, r, e))
+            if r >= target_recall and e < best[0]:
+                best = (e, int(cap), t)
+            if r < target_recall - 0.03:
+                break  # lower thresholds stop earlier still
+    return best[1], best[2], curve
 
 
-def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 128, period: int = 4, target_recall: float = 0.95,
+def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int = 4, target_recall: float = 0.95,
         precision: Optional[str] = None, rerank: Optional[int] = None, holdout: float = 0.3,
         max_ckpt: Optional[int] = None, epochs: int = 20, seed: int = 0, gt: Optional[np.ndarray] = None,
-        device: int = 0):
-    """Trace, label, train and calibrate on `queries` (drawn from the query
-    distribution; a `holdout` share is kept for the calibration).  Returns
+        caps=None, device: int = 0):
+    """Trace (at ef = ef_cap), label, train and calibrate on `queries` (drawn
+    from the query distribution; a `holdout` share is kept for the
+    calibration of the cap, at most ef_cap, and threshold).  Returns
     (TerminationModel, report)."""
     precision = precision or index.precision
     rerank = index.rerank if rerank is None else rerank
@@ -203,10 +218,12 @@ def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 128, period: int 
     X, y = checkpoint_dataset(index, ck, gt[tr])
     params, losses = train(X, y, epochs=epochs, seed=seed, device=device)
     model = TerminationModel(params, period, float("inf"), ef_cap, precision, int(rerank))
-    thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall)
-    model.threshold = thr
-    base_r, base_e = evaluate(index, queries[hold], gt[hold], k, model, float("inf"))
+    if caps is None:
+        caps = [c for c in (k, 16, 24, 32, 40, 44, 48, 52, 56, 64, 80, 96, 128, 192, 256, 384, 512)
+                if k <= c <= ef_cap]
+    cap, thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall, caps=caps)
+    model.ef_cap, model.threshold = cap, thr
     model.info = dict(samples=int(X.shape[0]), positive=float(y.mean()), loss=[float(v) for v in losses],
-                      curve=curve, cap_recall=base_r, cap_expansions=base_e, target_recall=target_recall)
+                      curve=curve, trained_cap=ef_cap, target_recall=target_recall)
     index.set_termination_model(model)
     return model, model.info

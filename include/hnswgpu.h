@@ -242,7 +242,10 @@ HNSWGPU_API int hnswgpu_set_termination_model(hnswgpu_index* index, const float*
  * `period` expansions, the feature vector (out_feat: nq x max_ckpt x 6) and
  * the internal ids of the current top-k (out_ids: nq x max_ckpt x k,
  * 0xffffffff where the beam holds fewer); out_nckpt[i] = rows written for
- * query i (at most max_ckpt). */
+ * query i (1..max_ckpt when max_ckpt > 0).  The last row of each query
+ * (out_nckpt[i] - 1) holds the state at the end of the beam: its top-k
+ * before any re-rank, the reference for labelling the earlier rows;
+ * checkpoints beyond max_ckpt - 1 are dropped. */
 HNSWGPU_API int hnswgpu_search_checkpoints(hnswgpu_index* index, const float* queries, uint64_t nq, uint64_t k,
                                            const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt,
                                            float* out_feat, uint32_t* out_ids, uint32_t* out_nckpt,

@@ -225,14 +225,18 @@ def test_full_size_parity_1m():
         build_hnsw(path + ".tmp", x, "l2", M=16, efc=200, num_threads=os.cpu_count())
         os.replace(path + ".tmp", path)
     del x
-    qs = q[:3000]
     g = gpu_index(path, "l2", 128)
     o = O.Hnsw(path, "l2", 128)
-    for ef in (48, 64, 128):
+    # small ef: the reference's candidate heap reaches ~10 x ef on some of the
+    # 10,000 queries (all of them are checked there)
+    for ef in (16, 24, 48, 64, 128):
+        qs = q if ef <= 24 else q[:3000]
         g.set_ef(ef)
         rl, rd, _, rt = o.search(qs, 10, ef, mode=O.REFERENCE, trace=True)
+        assert rt[:, 5].max() > 4 * ef  # the heap outgrows its shared-memory head
         g.tie_order = "reference"
         xl, xd = g.knn_query(qs, k=10)
+        assert g.get_status() == 0, "candidate heap overflow"
         assert np.array_equal(xl, rl) and np.array_equal(xd.view(np.uint32), rd.view(np.uint32))
         g.tie_order = "id"
         gl, gd = g.knn_query(qs, k=10)

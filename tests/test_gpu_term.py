@@ -85,12 +85,20 @@ def test_checkpoint_trace_is_the_search(gmm_index):
     pl, pd, pc, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id")
     ck = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=400)
     assert np.array_equal(ck["labels"], pl) and np.array_equal(ck["dists"].view(np.uint32), pd.view(np.uint32))
-    # a checkpoint after every `period`-th expansion that has a successor
-    assert np.all(ck["nckpt"] <= pt[:, 2] // period)
-    assert np.all(ck["nckpt"] >= (pt[:, 2] - 1) // period)
+    # a checkpoint after every `period`-th expansion that has a successor,
+    # then the final state
+    n = ck["nckpt"].astype(np.int64) - 1
+    assert np.all(n <= pt[:, 2] // period) and np.all(n >= (pt[:, 2] - 1) // period)
     lab_of = g.labels_by_internal_id()
+    final = ck["ids"][np.arange(300), n]
+    assert np.array_equal(lab_of[final], pl)
+    assert np.allclose(ck["feat"][np.arange(300), n, 0], np.log2(1 + pt[:, 2]), atol=1e-5)
+    # rows beyond the cap are dropped, the final row is kept
+    small = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=3)
+    assert np.all(small["nckpt"] == np.minimum(ck["nckpt"], 3))
+    assert np.array_equal(small["ids"][np.arange(300), small["nckpt"].astype(np.int64) - 1], final)
     for i in range(0, 300, 15):
-        for r in range(int(ck["nckpt"][i])):
+        for r in range(int(n[i])):
             f = ck["feat"][i, r]
             assert abs(f[0] - np.log2(1 + period * (r + 1))) < 1e-5
             ids = ck["ids"][i, r]
@@ -127,9 +135,10 @@ def test_fit_meets_target_with_less_work(gmm_index):
     generalisation margin) with fewer level-0 expansions than the cap."""
     g, x, q = gmm_index
     tr, te = q[:1000], q[1000:]
-    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0)
+    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0, caps=[96])
     assert rep["samples"] > 10000 and 0.05 < rep["positive"] < 0.95
     assert rep["loss"][-1] < rep["loss"][0]
+    assert model.ef_cap == 96 and np.isfinite(model.threshold)
     gt = g.knn_query_exact(te, 10)[0]
     g.learned_stop = True
     g.tie_order = "id"
@@ -140,6 +149,16 @@ def test_fit_meets_target_with_less_work(gmm_index):
     _, _, _, tp = g.knn_query_traced(te, 10, ef=model.ef_cap, learned=False)
     assert r >= 0.94, (r, rep["curve"])
     assert tl[:, 2].mean() < 0.9 * tp[:, 2].mean(), (tl[:, 2].mean(), tp[:, 2].mean())
+
+
+def test_fit_fp8_labels_use_the_beam_state(gmm_index):
+    """A low-precision beam is labelled against its own final top-k (before
+    the re-rank): the positive share stays far from zero."""
+    g, x, q = gmm_index
+    model, rep = learned.fit(g, q[:600], k=10, ef_cap=64, period=4, target_recall=0.9, precision="fp8",
+                             epochs=5, seed=1, caps=[48, 64])
+    assert 0.2 < rep["positive"] < 0.95, rep["positive"]
+    assert model.precision == "fp8" and model.ef_cap in (48, 64)
 
 
 def test_exact_scan_is_ground_truth(gmm_index):
