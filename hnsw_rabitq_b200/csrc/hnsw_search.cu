@@ -559,13 +559,65 @@ __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem&
     return true;
 }
 
+// ---- learned early termination (see term_mlp.cuh)
+struct TermState {
+    uint32_t last_change = 0;  // expansion count when the top-k last changed
+    uint32_t nckpt = 0;        // checkpoints taken
+};
+
+// Checkpoint after `e` level-0 expansions, with a next candidate of distance
+// key `next_dk` waiting: trace mode records the features and the top-k ids;
+// learned mode returns true when the network says stop.
+template <int TERM>
+__device__ __forceinline__ bool term_checkpoint(const SearchParams& p, const WarpSmem& s, int lane, uint32_t qi,
+                                                uint32_t e, int psize, uint32_t next_dk, float d_entry, float qn,
+                                                TermState& ts) {
+    if (psize == 0) return false;  // nothing admissible found yet
+    const int kq = (int)p.k;
+    const int kk = min(kq, psize);
+    float fe[kTermFeatures];
+    term_features((float)e, funkey(khi(s.pool[0])), funkey(khi(s.pool[kk - 1])), funkey(next_dk), d_entry, qn,
+                  (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    if (TERM == 1) {
+        if (ts.nckpt + 1 < p.term_max_ckpt) {  // the last row is kept for the final state
+            const size_t row = (size_t)qi * p.term_max_ckpt + ts.nckpt;
+            if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
+            for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+        }
+        ts.nckpt++;
+        return false;
+    }
+    return term_logit(p.term_model, fe, lane) > p.term_logit;
+}
+
+// Trace mode, end of the beam: the final row holds its top-k (before any
+// re-rank) and the features of that state; labels of earlier rows refer to it.
+__device__ __forceinline__ void term_final_row(const SearchParams& p, const WarpSmem& s, int lane, uint32_t qi,
+                                               uint32_t e, int psize, float d_entry, float qn, const TermState& ts) {
+    if (p.term_max_ckpt == 0) {
+        if (lane == 0) p.ckpt_count[qi] = 0;
+        return;
+    }
+    const int kq = (int)p.k;
+    const uint32_t r = min(ts.nckpt, p.term_max_ckpt - 1);
+    const size_t row = (size_t)qi * p.term_max_ckpt + r;
+    const int kk = min(kq, psize);
+    const float d1 = kk > 0 ? funkey(khi(s.pool[0])) : 0.f;
+    const float dk = kk > 0 ? funkey(khi(s.pool[kk - 1])) : 0.f;
+    float fe[kTermFeatures];
+    term_features((float)e, d1, dk, dk, d_entry, qn, (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
+    for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+    if (lane == 0) p.ckpt_count[qi] = r + 1;
+}
+
 template <int SPACE, bool EXACT, int PREC, int TERM>
 __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
                                PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
                                uint32_t& status, uint32_t qi, float qn) {
     const int ef = (int)p.ef;
     const int kq = (int)p.k;
-    uint32_t last_change = 0, nckpt = 0;  // learned termination state
+    TermState ts;
     const int pcap = (int)p.pool_cap;
     int hint_p = 0, csz = 0;
     // the entry point is pushed and popped at once (hnswalg.h:325-359)
@@ -606,7 +658,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         }
         const bool accept = live && cntP + cntN < ef;
         const unsigned pmask = __ballot_sync(FULL, accept);
-        if (TERM && __any_sync(FULL, accept && cntP + cntN < kq)) last_change = ct.l0_exp;
+        if (TERM && __any_sync(FULL, accept && cntP + cntN < kq)) ts.last_change = ct.l0_exp;
         PT_MARK(6);
         // ---- the next candidate
         uint64_t kmin = accept ? key : ~0ull;  // smallest accepted key
@@ -691,32 +743,15 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
         }
         PT_MARK(8);
-        if (TERM && have_next && ct.l0_exp % p.term_period == 0) {
-            // checkpoint: features of the state after this expansion
-            const int kk = min(kq, psize);
-            const float d1 = funkey(khi(s.pool[0]));
-            const float dk = funkey(khi(s.pool[kk - 1]));
-            const float dn = funkey(next_dk);
-            float fe[kTermFeatures];
-            term_features((float)ct.l0_exp, d1, dk, dn, d0, qn, (float)(ct.l0_exp - last_change),
-                          1.0f / (float)p.term_period, fe);
-            if (TERM == 1) {
-                if (nckpt + 1 < p.term_max_ckpt) {  // the last row is kept for the final state
-                    const size_t row = (size_t)qi * p.term_max_ckpt + nckpt;
-                    if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-                    for (int i = lane; i < kq; i += 32)
-                        p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
-                }
-                nckpt++;
-            } else if (term_logit(p.term_model, fe, lane) > p.term_logit) {
-                // confident that the top-k is final: drain the prefetched
-                // expansion and stop
-                if (fn.n0 > 0) {
-                    mbar_wait(s.bar, phase);
-                    phase ^= 1u;
-                }
-                break;
+        if (TERM && have_next && ct.l0_exp % p.term_period == 0 &&
+            term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d0, qn, ts)) {
+            // confident that the top-k is final: drain the prefetched
+            // expansion and stop
+            if (fn.n0 > 0) {
+                mbar_wait(s.bar, phase);
+                phase ^= 1u;
             }
+            break;
         }
         if (EXACT) {
             // the reference's loop head: top of candidate_set vs lowerBound
@@ -760,22 +795,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         ct.l0_exp += 1;
         PT_MARK(2);
     }
-    if (TERM == 1 && p.term_max_ckpt > 0) {
-        // final row: the beam's top-k when it ends (before any re-rank) and
-        // the features of that state; labels of the earlier rows refer to it
-        const uint32_t r = min(nckpt, p.term_max_ckpt - 1);
-        const size_t row = (size_t)qi * p.term_max_ckpt + r;
-        const int kk = min(kq, psize);
-        const float dk = funkey(khi(s.pool[kk - 1]));
-        float fe[kTermFeatures];
-        term_features((float)ct.l0_exp, funkey(khi(s.pool[0])), dk, dk, d0, qn, (float)(ct.l0_exp - last_change),
-                      1.0f / (float)p.term_period, fe);
-        if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-        for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
-        if (lane == 0) p.ckpt_count[qi] = r + 1;
-    } else if (TERM == 1 && lane == 0) {
-        p.ckpt_count[qi] = 0;
-    }
+    if (TERM == 1) term_final_row(p, s, lane, qi, ct.l0_exp, psize, d0, qn, ts);
     return true;
 }
 
@@ -900,6 +920,13 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
     const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
     const bool pipe = FAST16 && bare && p.maxM0 <= 32;
+    float qn = 0.f;
+    if (TERM) {  // |q|^2, a feature of the termination network
+        for (uint32_t i = lane; i < p.dim; i += 32) qn = fmaf(s.q[i], s.q[i], qn);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) qn += __shfl_xor_sync(FULL, qn, o);
+    }
+    TermState ts;
     if (pipe) {
         float d0;
         if (PREC == 0) {
@@ -921,12 +948,6 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         const float4* q4 = reinterpret_cast<const float4*>(s.q);
 #pragma unroll
         for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
-        float qn = 0.f;
-        if (TERM) {  // |q|^2, a feature of the termination network
-            for (uint32_t i = lane; i < p.dim; i += 32) qn = fmaf(s.q[i], s.q[i], qn);
-#pragma unroll
-            for (int o = 16; o; o >>= 1) qn += __shfl_xor_sync(FULL, qn, o);
-        }
         __syncwarp();
         if (!base_pipelined<SPACE, EXACT, PREC, TERM>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status,
                                                       qi, qn))
@@ -988,6 +1009,9 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         bool from_extra = kx < kp;
         if (from_extra && psize == (int)ef && khi(kx) > khi(s.pool[psize - 1])) break;
         uint64_t ck = from_extra ? kx : kp;
+        if (TERM && ct.l0_exp > 0 && ct.l0_exp % p.term_period == 0 &&
+            term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, khi(ck), curd, qn, ts))
+            break;
         __syncwarp();
         if (lane == 0) {
             if (from_extra) s.extra[ix] = ck | EXP_BIT;
@@ -1060,6 +1084,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             }
             bool accept = live && (uint32_t)(cntP + cntN) < ef;
             unsigned pmask = __ballot_sync(FULL, accept && allowed);
+            if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < (int)p.k)) ts.last_change = ct.l0_exp;
             unsigned xmask = bare ? 0u : __ballot_sync(FULL, accept && !allowed);
             PT_MARK(6);
             int nev = 0;
@@ -1115,6 +1140,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         }
     }
     PT_MARK(2);
+    if (TERM == 1) term_final_row(p, s, lane, qi, ct.l0_exp, psize, curd, qn, ts);
     }  // general loop
 
     const uint32_t k = p.k;
@@ -1317,12 +1343,14 @@ cudaError_t launch_lowp(const SearchParams& p, int num_sms, cudaStream_t stream,
     return p.prec == 1 ? launch_t<SPACE, true, false, 1>(p, num_sms, stream, blocks_out)
                        : launch_t<SPACE, true, false, 2>(p, num_sms, stream, blocks_out);
 }
-// learned termination (id tie order, pipelined beam; checked by the host)
+// learned termination (id tie order; checked by the host)
 template <int SPACE, int TERM>
 cudaError_t launch_term_p(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
-    return p.prec == 0   ? launch_t<SPACE, true, false, 0, TERM>(p, num_sms, stream, blocks_out)
-           : p.prec == 1 ? launch_t<SPACE, true, false, 1, TERM>(p, num_sms, stream, blocks_out)
-                         : launch_t<SPACE, true, false, 2, TERM>(p, num_sms, stream, blocks_out);
+    if (p.prec == 0)
+        return p.fast16 ? launch_t<SPACE, true, false, 0, TERM>(p, num_sms, stream, blocks_out)
+                        : launch_t<SPACE, false, false, 0, TERM>(p, num_sms, stream, blocks_out);
+    return p.prec == 1 ? launch_t<SPACE, true, false, 1, TERM>(p, num_sms, stream, blocks_out)
+                       : launch_t<SPACE, true, false, 2, TERM>(p, num_sms, stream, blocks_out);
 }
 
 template <int SPACE>

@@ -531,10 +531,7 @@ struct TermCfg {
 
 void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg* t) {
     if (!t || !t->mode) return;
-    if (!p.fast16 || !p.bare || p.maxM0 > 32 || p.exact)
-        throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
-                       "learned termination needs dim % 16 == 0, maxM0 <= 32, no filter / deletes and the id tie "
-                       "order");
+    if (p.exact) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "learned termination needs the id tie order");
     p.term_mode = t->mode;
     if (t->mode == 1) {
         if (t->period == 0) throw ApiError(HNSWGPU_ERR_ARG, "checkpoint period must be > 0");

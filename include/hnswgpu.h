@@ -62,8 +62,7 @@ extern "C" {
                                      the termination network set by
                                      hnswgpu_set_termination_model judges its
                                      top-k final; ef is then the cap.  Needs
-                                     dim % 16 == 0, maxM0 <= 32, no filter or
-                                     deletes, and the id tie order.           */
+                                     the id tie order (no HNSWGPU_EXACT_TIES). */
 #define HNSWGPU_EXACT_SCAN 0x10u  /* HNSW: answer by an exhaustive scan of the
                                      index's resident vectors (exact k-NN,
                                      the ground truth of recall measurements;

@@ -166,3 +166,36 @@ def test_exact_scan_is_ground_truth(gmm_index):
     l, d = g.knn_query_exact(q[:200], 10)
     rl, rd = O.bf_matrix("l2", x, q[:200], 10)
     assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))
+
+
+def test_learned_stop_general_path(tmp_path):
+    """Filters, deletes and dims that are not multiples of 16 take the general
+    beam; its checkpoints and stop rule behave as the pipelined beam's."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((8000, 20)).astype(np.float32)
+    q = rng.standard_normal((300, 20)).astype(np.float32)
+    build_hnsw(tmp_path / "g.bin", x, "l2", M=12, efc=100)
+    g = H.Index("l2", 20)
+    g.load_index(str(tmp_path / "g.bin"))
+    for lab in range(0, 8000, 37):
+        g.mark_deleted(lab)
+    flt = lambda l: l % 3 != 0
+    k, ef, period = 10, 80, 4
+    pl, pd, pc, pt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id")
+    ck = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=200)
+    # checkpoints are unfiltered searches: compare with the unfiltered plain run
+    ul, _, _, ut = g.knn_query_traced(q, k, ef=ef, tie_order="id")
+    assert np.array_equal(ck["labels"], ul)
+    lab_of = g.labels_by_internal_id()
+    n = ck["nckpt"].astype(np.int64) - 1
+    assert np.array_equal(lab_of[ck["ids"][np.arange(300), n]], ul)
+    assert np.all(n <= ut[:, 2] // period)
+    p, f, _ = _random_problem(3)
+    g.set_termination_model(learned.TerminationModel(p, period, float("inf")))
+    ll, ld, lc, lt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id", learned=True)
+    assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
+    assert all(flt(int(v)) and int(v) % 37 for row in ll for v in row)
+    g.set_termination_model(learned.TerminationModel(p, period, -float("inf")))
+    ll, ld, lc, lt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id", learned=True)
+    assert np.all(lt[:, 2] <= period)
+    assert all(flt(int(v)) and int(v) % 37 for i in range(300) for v in ll[i, :lc[i]])
