@@ -48,6 +48,19 @@ class TermTrainOpts(C.Structure):
                 ("weight_decay", C.c_float), ("reserved", U32), ("seed", U64)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("max_inflight", U32), ("max_batch", U32), ("smem_budget", U64)]
+
+
+class Request(C.Structure):
+    _fields_ = [("k", U32), ("ef", U32), ("filter", I32), ("flags", U32), ("precision", U32), ("rerank", U32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", U64), ("completed", U64), ("batches", U64), ("mean_batch", C.c_double),
+                ("p50_us", C.c_double), ("p99_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double)]
+
+
 SIGNATURES = {
     "hnswgpu_last_error": (C.c_char_p, []),
     "hnswgpu_version": (C.c_char_p, []),
@@ -69,6 +82,13 @@ SIGNATURES = {
     "hnswgpu_term_train": (C.c_int, [C.c_int, P, P, U64, C.POINTER(TermTrainOpts), P, P]),
     "hnswgpu_term_loss_grad": (C.c_int, [C.c_int, P, P, P, U64, C.c_float, P, P]),
     "hnswgpu_term_logits": (C.c_int, [C.c_int, P, P, U64, P]),
+    "hnswgpu_server_create": (C.c_int, [P, C.POINTER(ServerOpts), C.POINTER(P)]),
+    "hnswgpu_server_add_filter": (C.c_int, [P, P, C.POINTER(I32)]),
+    "hnswgpu_server_submit": (C.c_int, [P, P, C.POINTER(Request), C.POINTER(U64)]),
+    "hnswgpu_server_wait": (C.c_int, [P, U64, P, P, P, P]),
+    "hnswgpu_server_replay": (C.c_int, [P, P, U64, P, P, U32, P, P, P, P]),
+    "hnswgpu_server_get_stats": (C.c_int, [P, C.POINTER(ServerStats), C.c_int]),
+    "hnswgpu_server_destroy": (C.c_int, [P]),
 }
 
 _lib = None

@@ -38,91 +38,21 @@
 static_assert(HNSWGPU_TERM_PARAMS == hnswgpu::kTermParams, "termination parameter count");
 static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feature count");
 
-namespace {
+#include "index_internal.h"
 
+namespace hnswgpu_host {
 thread_local std::string g_last_error;
+}  // namespace hnswgpu_host
+using namespace hnswgpu_host;
 
-struct ApiError : std::runtime_error {
-    int code;
-    ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-void cuda_check(cudaError_t e, const char* what) {
-    if (e != cudaSuccess) {
-        throw ApiError(e == cudaErrorMemoryAllocation ? HNSWGPU_ERR_NOMEM : HNSWGPU_ERR_CUDA,
-                       std::string(what) + ": " + cudaGetErrorString(e));
-    }
-}
-
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    void alloc(size_t count) {
-        release();
-        if (count == 0) return;
-        cuda_check(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
-        n = count;
-    }
-    void ensure(size_t count) {
-        if (count > n) alloc(count);
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    size_t bytes() const { return n * sizeof(T); }
-    ~DevBuf() { release(); }
-};
-
+namespace {
 template <class T>
 void rd(std::ifstream& in, T& v) {
     in.read((char*)&v, sizeof(T));
 }
-
 }  // namespace
 
-struct hnswgpu_index {
-    int is_bf = 0;
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    int space = 0;
-    uint64_t dim = 0;
-    uint32_t row_floats = 0;
-    uint64_t count = 0, max_elements = 0;
-    uint64_t M = 0, maxM = 0, maxM0 = 0, efc = 0, ef = 10;
-    int32_t maxlevel = 0;
-    uint32_t ep = 0;
-    std::vector<uint64_t> labels;
-    std::unordered_map<uint64_t, uint32_t> lookup;
-    std::vector<uint32_t> deleted;  // host copy of the bitmap
-    bool links_unique = true;       // no level-0 list repeats an id
-    uint64_t num_deleted = 0;
-    DevBuf<float> vecs;
-    DevBuf<uint32_t> links0, upper_off, upper_links, deleted_bits;
-    DevBuf<uint64_t> dlabels;
-    // per-call workspace
-    DevBuf<uint32_t> counters;  // ring of work counters
-    uint32_t next_counter = 0;
-    DevBuf<uint32_t> status;
-    DevBuf<unsigned char> io;  // host-pointer calls: queries + outputs
-    DevBuf<uint8_t> allow;
-    DevBuf<float> bf_norms;    // brute force: per-row helper values
-    DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
-    DevBuf<unsigned char> term_model;  // learned termination: packed network
-    DevBuf<uint64_t> cand_spill;       // tie-exact mode: candidate-heap tails
-    uint32_t term_period = 0;
-    float term_logit = 0.f;
-    std::mutex mu;
-    uint64_t device_bytes() const {
-        return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
-               dlabels.bytes() + bf_norms.bytes() + tcopy[1].bytes() + tcopy[2].bytes();
-    }
-};
-
-namespace {
+namespace hnswgpu_host {
 
 void set_device(hnswgpu_index* h) { cuda_check(cudaSetDevice(h->device), "cudaSetDevice"); }
 
@@ -402,19 +332,6 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
-template <class F>
-int guarded(F fn) {
-    try {
-        g_last_error.clear();
-        return fn();
-    } catch (const ApiError& e) {
-        return fail(e.code, e.what());
-    } catch (const std::bad_alloc&) {
-        return fail(HNSWGPU_ERR_NOMEM, "Not enough memory");
-    } catch (const std::exception& e) {
-        return fail(HNSWGPU_ERR_ARG, e.what());
-    }
-}
 
 void ensure_traversal_copy(hnswgpu_index* h, uint32_t prec) {
     if (prec != 1 && prec != 2) throw ApiError(HNSWGPU_ERR_ARG, "precision must be HNSWGPU_PREC_BF16 or _FP8");
@@ -431,7 +348,7 @@ void ensure_traversal_copy(hnswgpu_index* h, uint32_t prec) {
 // work_counter / done_counter / status are left for the caller to set).
 hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef,
                                   const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace,
-                                  bool exact, uint32_t prec = 0, uint32_t rerank = 0, bool spill = false) {
+                                  bool exact, uint32_t prec, uint32_t rerank, bool spill) {
     hnswgpu::SearchParams p{};
     p.vecs = h->vecs.p;
     p.links0 = h->links0.p;
@@ -520,14 +437,6 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     return p;
 }
 
-// Learned-termination settings of one launch (mode 1: record checkpoints,
-// 2: stop early with the index's network).
-struct TermCfg {
-    uint32_t mode = 0, period = 0, max_ckpt = 0;
-    float* feat = nullptr;
-    uint32_t* ids = nullptr;
-    uint32_t* count = nullptr;
-};
 
 void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg* t) {
     if (!t || !t->mode) return;
@@ -585,7 +494,7 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
 
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
-                uint32_t prec = 0, uint32_t rerank = 0, const TermCfg* term = nullptr, bool scan = false) {
+                uint32_t prec, uint32_t rerank, const TermCfg* term, bool scan) {
     if (scan && !h->is_bf && h->num_deleted)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "HNSWGPU_EXACT_SCAN: the index has deleted elements");
     if (h->is_bf || scan) {
@@ -611,7 +520,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
     }
 }
 
-}  // namespace
+}  // namespace hnswgpu_host
 
 #ifdef HNSWGPU_BOUNDS_CHECK
 namespace hnswgpu {

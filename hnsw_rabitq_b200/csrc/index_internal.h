@@ -1,0 +1,138 @@
+// Internal host-side declarations shared by the C-ABI translation units
+// (index_api.cu: loading and search entry points; server.cu: the serving
+// loop).  Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "hnswgpu.h"
+#include "hnsw_search.h"
+
+namespace hnswgpu_host {
+
+extern thread_local std::string g_last_error;
+
+struct ApiError : std::runtime_error {
+    int code;
+    ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw ApiError(e == cudaErrorMemoryAllocation ? HNSWGPU_ERR_NOMEM : HNSWGPU_ERR_CUDA,
+                       std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        cuda_check(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void ensure(size_t count) {
+        if (count > n) alloc(count);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+    ~DevBuf() { release(); }
+};
+
+}  // namespace hnswgpu_host
+
+struct hnswgpu_index {
+    template <class T>
+    using DevBuf = hnswgpu_host::DevBuf<T>;
+    int is_bf = 0;
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int space = 0;
+    uint64_t dim = 0;
+    uint32_t row_floats = 0;
+    uint64_t count = 0, max_elements = 0;
+    uint64_t M = 0, maxM = 0, maxM0 = 0, efc = 0, ef = 10;
+    int32_t maxlevel = 0;
+    uint32_t ep = 0;
+    std::vector<uint64_t> labels;
+    std::unordered_map<uint64_t, uint32_t> lookup;
+    std::vector<uint32_t> deleted;  // host copy of the bitmap
+    bool links_unique = true;       // no level-0 list repeats an id
+    uint64_t num_deleted = 0;
+    DevBuf<float> vecs;
+    DevBuf<uint32_t> links0, upper_off, upper_links, deleted_bits;
+    DevBuf<uint64_t> dlabels;
+    // per-call workspace
+    DevBuf<uint32_t> counters;  // ring of work counters
+    uint32_t next_counter = 0;
+    DevBuf<uint32_t> status;
+    DevBuf<unsigned char> io;  // host-pointer calls: queries + outputs
+    DevBuf<uint8_t> allow;
+    DevBuf<float> bf_norms;    // brute force: per-row helper values
+    DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
+    DevBuf<unsigned char> term_model;  // learned termination: packed network
+    DevBuf<uint64_t> cand_spill;       // tie-exact mode: candidate-heap tails
+    uint32_t term_period = 0;
+    float term_logit = 0.f;
+    std::mutex mu;
+    uint64_t device_bytes() const {
+        return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
+               dlabels.bytes() + bf_norms.bytes() + tcopy[1].bytes() + tcopy[2].bytes();
+    }
+};
+
+
+namespace hnswgpu_host {
+
+// Learned-termination settings of one launch (mode 1: record checkpoints,
+// 2: stop early with the index's network).
+struct TermCfg {
+    uint32_t mode = 0, period = 0, max_ckpt = 0;
+    float* feat = nullptr;
+    uint32_t* ids = nullptr;
+    uint32_t* count = nullptr;
+};
+
+int fail(int code, const std::string& msg);
+
+template <class F>
+int guarded(F fn) {
+    try {
+        g_last_error.clear();
+        return fn();
+    } catch (const ApiError& e) {
+        return fail(e.code, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(HNSWGPU_ERR_NOMEM, "Not enough memory");
+    } catch (const std::exception& e) {
+        return fail(HNSWGPU_ERR_ARG, e.what());
+    }
+}
+
+void set_device(hnswgpu_index* h);
+void ensure_traversal_copy(hnswgpu_index* h, uint32_t prec);
+// Launch parameters of one HNSW search on device buffers (no allocation).
+hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef,
+                                  const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace,
+                                  bool exact, uint32_t prec = 0, uint32_t rerank = 0, bool spill = false);
+// One search launch (HNSW beam, or brute force / exact scan) on device
+// buffers on stream `st`; the caller holds h->mu.
+void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
+                uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
+                uint32_t prec = 0, uint32_t rerank = 0, const TermCfg* term = nullptr, bool scan = false);
+
+}  // namespace hnswgpu_host

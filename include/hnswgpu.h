@@ -276,6 +276,66 @@ HNSWGPU_API int hnswgpu_term_loss_grad(int device, const float* params, const fl
 HNSWGPU_API int hnswgpu_term_logits(int device, const float* params, const float* feats, uint64_t n,
                                     float* out_logits);
 
+/* ------------------------------------------------------------ serving loop
+ * Continuous batching of single-query requests over one HNSW index (no
+ * counterpart in the reference, where each caller thread runs its own
+ * searchKnn).  A scheduler thread batches waiting requests that share a
+ * search configuration (k, ef, filter, flags, precision, re-rank), launches
+ * each batch on one of `max_inflight` CUDA streams so that batches overlap on
+ * the device, and admits a batch only while the shared-memory footprint of
+ * the queries in flight (one warp and its configuration's per-warp layout
+ * each) stays within `smem_budget`; a finished batch frees its share at
+ * once.  A request's results are those of hnswgpu_search for the same query
+ * and settings, whatever else is in flight. */
+typedef struct hnswgpu_server hnswgpu_server;
+
+typedef struct hnswgpu_server_opts {
+    uint32_t max_inflight;     /* concurrent batches (streams); 0: 8          */
+    uint32_t max_batch;        /* queries per batch; 0: 4096                  */
+    uint64_t smem_budget;      /* admission budget in bytes of per-query
+                                  shared-memory footprint in flight; 0: twice
+                                  the device's shared memory (SMs x per SM)  */
+} hnswgpu_server_opts;
+
+typedef struct hnswgpu_request {
+    uint32_t k;
+    uint32_t ef;               /* 0: the index's ef                          */
+    int32_t filter;            /* hnswgpu_server_add_filter id, or -1        */
+    uint32_t flags;            /* HNSWGPU_EXACT_TIES or HNSWGPU_LEARNED_STOP  */
+    uint32_t precision;        /* HNSWGPU_PREC_*                              */
+    uint32_t rerank;           /* as hnswgpu_search_opts.rerank               */
+} hnswgpu_request;
+
+typedef struct hnswgpu_server_stats {
+    uint64_t submitted, completed, batches;
+    double mean_batch;         /* queries per batch                           */
+    double p50_us, p99_us, mean_us, max_us; /* submission -> results on the
+                                  host, over requests completed since the
+                                  last reset                                  */
+} hnswgpu_server_stats;
+
+HNSWGPU_API int hnswgpu_server_create(hnswgpu_index* index, const hnswgpu_server_opts* opts, hnswgpu_server** out);
+/* Register a filter: a byte per internal id (hnswgpu_get_labels order),
+ * nonzero = the label may be returned; out_id names it in requests. */
+HNSWGPU_API int hnswgpu_server_add_filter(hnswgpu_server* server, const uint8_t* allow, int32_t* out_id);
+/* Queue one query (dim floats, copied); returns at once with a ticket. */
+HNSWGPU_API int hnswgpu_server_submit(hnswgpu_server* server, const float* query, const hnswgpu_request* req,
+                                      uint64_t* out_ticket);
+/* Block until the ticket's results are ready (req.k labels / distances,
+ * closest first, count, latency in microseconds); releases the ticket. */
+HNSWGPU_API int hnswgpu_server_wait(hnswgpu_server* server, uint64_t ticket, uint64_t* labels, float* dists,
+                                    int32_t* count, double* latency_us);
+/* Open-loop load: submit request i (queries + i * dim, reqs[i]) at
+ * arrival_us[i] microseconds after the call starts, from the calling thread,
+ * then collect every result (rows of k_stride labels / distances, padded
+ * with UINT64_MAX / +inf) and its latency. */
+HNSWGPU_API int hnswgpu_server_replay(hnswgpu_server* server, const float* queries, uint64_t n,
+                                      const hnswgpu_request* reqs, const double* arrival_us, uint32_t k_stride,
+                                      uint64_t* labels, float* dists, int32_t* counts, double* latency_us);
+HNSWGPU_API int hnswgpu_server_get_stats(hnswgpu_server* server, hnswgpu_server_stats* out, int reset);
+/* Finish every queued request, then release the server (not the index). */
+HNSWGPU_API int hnswgpu_server_destroy(hnswgpu_server* server);
+
 /* OR of the kernel status bits raised by searches on this index since the
  * last call (synchronises the index's stream); clears them. */
 HNSWGPU_API int hnswgpu_get_status(hnswgpu_index* index, uint32_t* out_bits);

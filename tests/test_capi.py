@@ -47,6 +47,19 @@ def test_struct_layouts_match_header(tmp_path):
     assert g == _capi.TERM_PARAMS
 
 
+def test_server_struct_layouts(tmp_path):
+    prog = tmp_path / "sv.c"
+    prog.write_text('#include <stdio.h>\n#include "hnswgpu.h"\n#include <stddef.h>\n'
+                    'int main(void){printf("%zu %zu %zu %zu %zu\\n", sizeof(hnswgpu_server_opts),'
+                    ' sizeof(hnswgpu_request), sizeof(hnswgpu_server_stats), offsetof(hnswgpu_request, rerank),'
+                    ' offsetof(hnswgpu_server_stats, max_us));return 0;}\n')
+    exe = tmp_path / "sv"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)])
+    a, b, c, d, e = map(int, subprocess.check_output([str(exe)]).split())
+    assert (a, b, c) == (C.sizeof(_capi.ServerOpts), C.sizeof(_capi.Request), C.sizeof(_capi.ServerStats))
+    assert d == _capi.Request.rerank.offset and e == _capi.ServerStats.max_us.offset
+
+
 def test_version_and_error_string():
     lib = _capi.lib()
     assert b"sm_100a" in lib.hnswgpu_version()

@@ -1,0 +1,106 @@
+"""Serving loop (continuous batching) on the GPU: every request's result is
+the same whether it runs alone or inside a mixed, overlapping load of other
+k / ef / filter / tie-order / precision / learned-stop requests; admission by
+footprint bounds what is in flight (needs a B200)."""
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from hnsw_rabitq_b200 import learned
+from hnsw_rabitq_b200.serving import Server, poisson_arrivals
+from tests.helpers import build_hnsw
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def served(tmp_path_factory):
+    rng = np.random.default_rng(5)
+    x = (rng.standard_normal((20000, 64)) * 3).astype(np.float32)
+    q = (rng.standard_normal((1200, 64)) * 3).astype(np.float32)
+    path = tmp_path_factory.mktemp("srv") / "s.bin"
+    build_hnsw(path, x, "l2", M=16, efc=100, num_threads=8)
+    g = H.Index("l2", 64)
+    g.load_index(str(path))
+    for lab in range(0, 20000, 20):  # 5 % deleted
+        g.mark_deleted(lab)
+    # a termination network (random weights, finite threshold): what matters
+    # here is that the learned stop is deterministic per query
+    f = rng.normal(size=(100, 6)).astype(np.float32)
+    g.set_termination_model(learned.TerminationModel(learned.init_params(f, 1), 4, 0.5))
+    return g, x, q
+
+
+def _mix(n, rng, parity_id):
+    reqs = []
+    for i in range(n):
+        reqs.append(Server.request(k=int(rng.choice([1, 10, 100])), ef=int(rng.choice([32, 64, 128, 256])),
+                                   filter=parity_id if rng.random() < 0.3 else -1,
+                                   tie_order="reference" if rng.random() < 0.2 else "id",
+                                   learned=False, precision="fp32"))
+        if reqs[-1].flags == 0 and rng.random() < 0.3:
+            reqs[-1].flags = H._capi.LEARNED_STOP
+    return reqs
+
+
+def test_same_alone_and_in_mix(served):
+    g, x, q = served
+    rng = np.random.default_rng(9)
+    with Server(g, max_inflight=6, max_batch=256) as srv:
+        parity = srv.add_filter(lambda l: l % 2 == 0)
+        reqs = _mix(len(q), rng, parity)
+        # in the mix: Poisson arrivals at 100k requests/s
+        ml, md, mc, lat = srv.replay(q, reqs, poisson_arrivals(len(q), 100_000, seed=2))
+        st = srv.stats()
+        assert st["completed"] == len(q) and st["batches"] > 1
+        assert np.all(lat > 0) and st["p99_us"] >= st["p50_us"] > 0
+        # alone: one request at a time through the same server
+        for i in range(0, len(q), 7):
+            r = reqs[i]
+            t = srv.submit(q[i], k=r.k, ef=r.ef, filter=r.filter,
+                           tie_order="reference" if r.flags & H._capi.EXACT_TIES else "id",
+                           learned=bool(r.flags & H._capi.LEARNED_STOP))
+            al, ad, _ = srv.wait(t)
+            assert mc[i] == len(al)
+            assert np.array_equal(al, ml[i, :mc[i]]), i
+            assert np.array_equal(ad.view(np.uint32), md[i, :mc[i]].view(np.uint32)), i
+
+
+def test_matches_batch_search(served):
+    """A served request equals the batched C-ABI search with the same settings."""
+    g, x, q = served
+    with Server(g) as srv:
+        parity = srv.add_filter(lambda l: l % 2 == 0)
+        n = 300
+        reqs = [Server.request(k=10, ef=64, filter=parity if i % 2 else -1) for i in range(n)]
+        ml, md, mc, _ = srv.replay(q[:n], reqs, np.zeros(n))
+    fl, fd, fc, _ = g.knn_query_traced(q[:n], 10, filter=lambda l: l % 2 == 0, ef=64, tie_order="id")
+    ul, ud, uc, _ = g.knn_query_traced(q[:n], 10, ef=64, tie_order="id")
+    for i in range(n):
+        want = (fl, fc) if i % 2 else (ul, uc)
+        assert mc[i] == want[1][i] and np.array_equal(ml[i, :mc[i]], want[0][i, :mc[i]])
+
+
+def test_admission_budget_serialises(served):
+    """A budget of one query's footprint forces batches of one."""
+    g, x, q = served
+    with Server(g, smem_budget=1) as srv:
+        with pytest.raises(RuntimeError, match="exceeds the admission budget"):
+            srv.replay(q[:3], [Server.request(k=10, ef=64)] * 3, np.zeros(3))
+    with Server(g, max_batch=1) as srv:
+        ml, _, mc, _ = srv.replay(q[:20], [Server.request(k=10, ef=64)] * 20, np.zeros(20))
+        st = srv.stats()
+        assert st["batches"] == 20 and st["mean_batch"] == 1
+    ul, _, _, _ = g.knn_query_traced(q[:20], 10, ef=64, tie_order="id")
+    assert np.array_equal(ml, ul)
+
+
+def test_rejects_bad_requests(served):
+    g, x, q = served
+    with Server(g) as srv:
+        with pytest.raises(RuntimeError, match="unknown filter"):
+            srv.submit(q[0], k=10, filter=3)
+        with pytest.raises(RuntimeError, match="id tie order"):
+            srv.submit(q[0], k=10, tie_order="reference", learned=True)
+        with pytest.raises(RuntimeError, match="k must be positive"):
+            srv.submit(q[0], k=0)
