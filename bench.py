@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--target-recall", type=float, default=0.95)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", action="store_true", help="only run the timed loop (for ncu)")
+    ap.add_argument("--profile-learned", type=float, default=None, metavar="LOGIT",
+                    help="train the termination network, then only run the learned + FP8 loop with this logit "
+                         "threshold at ef = --term-cap (for ncu; no calibration sweep)")
     ap.add_argument("--tie-order", default="reference", choices=["reference", "id"],
                     help="tie order of --profile-steps: reference (heap replay, results identical to hnswlib) "
                          "or id (ties by internal id)")
@@ -80,6 +83,8 @@ def parse():
     ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
     ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
     ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
+    ap.add_argument("--serve-rates", type=int, nargs="*", default=[200_000, 1_000_000],
+                    help="Poisson arrival rates (requests/s) of the serving-latency measurement")
     return ap.parse_args()
 
 
@@ -374,6 +379,19 @@ def run_ours(args, dist: Dist):
     _capi.check(_capi.lib().hnswgpu_build_traversal_copy(idx._h, _capi.PREC_FP8))
     loop = DeviceLoop(idx, q, dev)
     nq, k = q.shape[0], 10
+    if args.profile_learned is not None:
+        from hnsw_rabitq_b200.datasets import gmm_1m_128_queries
+        tq = gmm_1m_128_queries(args.train_queries, stream_seed=1000)
+        tgt = idx.knn_query_exact(tq, 10)[0]
+        ck = idx.search_checkpoints(tq, 10, ef=args.term_cap, period=args.term_period,
+                                    max_ckpt=max(16, 8 * args.term_cap // args.term_period), precision="fp8",
+                                    rerank=args.rerank)
+        params, _ = learned.train(*learned.checkpoint_dataset(idx, ck, tgt), epochs=20, seed=0)
+        idx.set_termination_model(learned.TerminationModel(params, args.term_period, args.profile_learned,
+                                                           args.term_cap, "fp8", args.rerank))
+        loop.time(loop.opts(args.term_cap, _capi.LEARNED_STOP, _capi.PREC_FP8, args.rerank), args.steps,
+                  args.warmup, dist)
+        return None
     if args.profile_steps:
         if not args.ef:
             raise SystemExit("--profile-steps needs --ef")
@@ -417,6 +435,7 @@ def run_ours(args, dist: Dist):
                                           rerank=args.rerank, learned=True)
     e2e, h2d, d2h = e2e_qps(idx, q, flags, model.ef_cap, _capi.PREC_FP8, args.rerank, args.steps, args.warmup,
                             dist, lab)
+    latency = serving_latency(idx, q, model, args, lab)
 
     out = None
     if dist.rank == 0:
@@ -468,7 +487,34 @@ def run_ours(args, dist: Dist):
             "e2e": {"value": round(e2e, 1), "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "clocks": clk,
+            "latency": latency,
         }
+    return out
+
+
+def serving_latency(idx, q, model, args, expect):
+    """Per-request latency through the serving loop (continuous batching):
+    the evaluation queries arrive one by one as a Poisson process and are
+    submitted natively at their arrival times, each with the headline
+    configuration (k=10, learned stop, FP8 beam, cap ef); latency = submission
+    to results on the host."""
+    from hnsw_rabitq_b200.serving import Server, poisson_arrivals
+    out = []
+    req = Server.request(k=10, ef=model.ef_cap, learned=True, precision="fp8", rerank=args.rerank)
+    with Server(idx) as srv:
+        srv.replay(q[:2000], [req] * 2000, poisson_arrivals(2000, 200_000, seed=11))  # warm-up
+        for rate in args.serve_rates:
+            srv.stats(reset=True)
+            arr = poisson_arrivals(q.shape[0], rate, seed=rate)
+            t0 = time.perf_counter()
+            lab, _, cnt, lat = srv.replay(q, [req] * q.shape[0], arr)
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            assert np.array_equal(lab, expect)  # same results as the batch launch
+            out.append({"arrival_rate_qps": rate, "p50_us": round(float(np.percentile(lat, 50)), 1),
+                        "p99_us": round(float(np.percentile(lat, 99)), 1),
+                        "mean_us": round(float(lat.mean()), 1), "served_qps": round(q.shape[0] / wall, 1),
+                        "mean_batch": round(st["mean_batch"], 2), "requests": int(q.shape[0])})
     return out
 
 
