@@ -32,6 +32,7 @@
 
 #include "hnswgpu.h"
 #include "bf_search.h"
+#include "bf_tc.h"
 #include "device_common.cuh"
 #include "hnsw_search.h"
 
@@ -492,12 +493,181 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
                "hnsw_search launch");
 }
 
+// Exact brute force of a batch on device buffers (bf_search.cu).
+static void run_bf_exact(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, const uint8_t* dallow,
+                         uint64_t* dl, float* dd, int32_t* dc, cudaStream_t st) {
+    hnswgpu::BfParams b{};
+    b.vecs = h->vecs.p;
+    b.labels = h->dlabels.p;
+    b.allow = dallow;
+    b.count = (uint32_t)h->count;
+    b.dim = (uint32_t)h->dim;
+    b.row_floats = h->row_floats;
+    b.queries = dq;
+    b.nq = (uint32_t)nq;
+    b.k = (uint32_t)k;
+    b.normalize = h->space == HNSWGPU_SPACE_COSINE ? 1u : 0u;
+    b.out_labels = dl;
+    b.out_dists = dd;
+    b.out_counts = dc;
+    b.status = h->status.p;
+    cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st), "bf_search launch");
+}
+
+static uint32_t pow2_at_least(uint64_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Tensor-core brute force (bf_tc.cu) of a BruteforceSearch index over its
+// bf16 / fp8 copy: sampled threshold, tcgen05 scores with fused candidate
+// filtering, selection of the R best and exact float32 re-rank; queries the
+// filter could not bound are answered by the exact kernel.  Synchronises.
+void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint32_t rerank, const uint8_t* dallow,
+               uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, uint32_t prec) {
+    const uint64_t n = h->count;
+    const uint32_t dim = (uint32_t)h->dim;
+    const uint64_t R = std::max<uint64_t>(k, rerank ? rerank : 4 * k);
+    if (R > 1024) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "tensor-core brute force: over-fetch (rerank, or 4 k) must be <= 1024");
+    if (nq > 0x7fffffffull) throw ApiError(HNSWGPU_ERR_ARG, "batch too large");
+    const bool first = !h->tc_rowinfo[prec].p;
+    ensure_traversal_copy(h, prec);
+    const uint32_t trow = hnswgpu::traversal_row_bytes(prec, dim);
+    if (first) {
+        h->tc_rowinfo[prec].alloc(n);
+        cuda_check(hnswgpu::launch_tc_rowinfo(h->vecs.p, (uint32_t)n, dim, h->row_floats, h->tcopy[prec].p, trow, prec,
+                                              h->tc_rowinfo[prec].p, h->stream),
+                   "rowinfo launch");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    }
+    // sampling: about 5 R rows of the whole set below the 16th-best sampled distance
+    const bool sampled = n > 16384;
+    uint64_t step = 1, n_sample = n, cap = n;
+    if (sampled) {
+        const uint64_t S = std::min<uint64_t>(8192, std::max<uint64_t>(64, 16 * n / (5 * R)));
+        step = std::max<uint64_t>(1, n / S);
+        n_sample = (n + step - 1) / step;
+        const uint64_t expected = 16 * n / n_sample;
+        cap = std::min<uint64_t>(16384, pow2_at_least(std::max<uint64_t>(3 * expected, 2 * R)));
+    }
+    const uint32_t sort_cap = pow2_at_least(std::max<uint64_t>(cap, 1));
+    const size_t sel_smem = hnswgpu::tc_select_smem(sort_cap, dim, (uint32_t)R);
+    int max_optin = 0;
+    cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+    if (sel_smem + 1024 > (size_t)max_optin)
+        throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "tensor-core brute force: candidate list too large for shared memory");
+    h->tc_qf.ensure(nq * dim);
+    h->tc_qt.ensure(nq * trow + 16);
+    h->tc_qscale.ensure(nq);
+    h->tc_tau.ensure(nq);
+    h->tc_cnt.ensure(nq);
+    h->tc_flags.ensure(nq);
+    h->tc_buf.ensure(nq * cap);
+    cuda_check(hnswgpu::launch_tc_query_prep(dq, (uint32_t)nq, dim, h->space == HNSWGPU_SPACE_COSINE, prec, trow,
+                                             h->tc_qf.p, h->tc_qt.p, h->tc_qscale.p, st),
+               "query prep launch");
+    CUtensorMap qmap, xmap, smap;
+    cuda_check(hnswgpu::tc_encode_map(h->tc_qt.p, prec, nq, dim, trow, 128, &qmap), "tensor map (queries)");
+    cuda_check(hnswgpu::tc_encode_map(h->tcopy[prec].p, prec, n, dim, trow, 256, &xmap), "tensor map (rows)");
+    const int space = h->space == HNSWGPU_SPACE_L2 ? 0 : 1;
+    hnswgpu::TcArgs a{};
+    a.nq = (uint32_t)nq;
+    a.k_blocks = (dim * (prec == 1 ? 2u : 1u) + 127) / 128;
+    a.rowinfo = h->tc_rowinfo[prec].p;
+    a.qscale = h->tc_qscale.p;
+    a.allow = dallow;
+    a.tau = h->tc_tau.p;
+    a.cnt = h->tc_cnt.p;
+    a.buf = h->tc_buf.p;
+    a.cap = (uint32_t)cap;
+    a.status = h->status.p;
+    if (sampled) {
+        cuda_check(hnswgpu::tc_encode_map(h->tcopy[prec].p, prec, n_sample, dim, (uint64_t)trow * step, 256, &smap),
+                   "tensor map (sample)");
+        hnswgpu::TcArgs t = a;
+        t.n_rows = (uint32_t)n_sample;
+        t.row_step = step;
+        t.chunk_tiles = 1;
+        cuda_check(hnswgpu::launch_tc_scores(qmap, smap, t, prec, space, 1, h->num_sms, st), "threshold launch");
+    } else {
+        cuda_check(hnswgpu::launch_tc_fill(h->tc_tau.p, nq, __builtin_inff(), st), "fill launch");
+    }
+    cuda_check(cudaMemsetAsync(h->tc_cnt.p, 0, nq * 4, st), "cudaMemsetAsync");
+    a.n_rows = (uint32_t)n;
+    a.row_step = 1;
+    {
+        const uint64_t q_tiles = (nq + 127) / 128, n_tiles = (n + 255) / 256;
+        a.chunk_tiles = (uint32_t)std::max<uint64_t>(1, (q_tiles * n_tiles + 8ull * h->num_sms - 1) / (8ull * h->num_sms));
+        a.chunk_tiles = std::min<uint32_t>(a.chunk_tiles, (uint32_t)n_tiles);
+    }
+    cuda_check(hnswgpu::launch_tc_scores(qmap, xmap, a, prec, space, 0, h->num_sms, st), "scores launch");
+    if (dtrace) cuda_check(cudaMemsetAsync(dtrace, 0, nq * 16, st), "cudaMemsetAsync");
+    hnswgpu::TcSelectArgs sa{};
+    sa.nq = (uint32_t)nq;
+    sa.k = (uint32_t)k;
+    sa.R = (uint32_t)R;
+    sa.cap = (uint32_t)cap;
+    sa.sort_cap = sort_cap;
+    sa.dim = dim;
+    sa.row_floats = h->row_floats;
+    sa.sampled = sampled ? 1u : 0u;
+    sa.cnt = h->tc_cnt.p;
+    sa.buf = h->tc_buf.p;
+    sa.qf = h->tc_qf.p;
+    sa.vecs = h->vecs.p;
+    sa.labels = h->dlabels.p;
+    sa.out_labels = dl;
+    sa.out_dists = dd;
+    sa.out_counts = dc;
+    sa.flags = h->tc_flags.p;
+    sa.trace = dtrace;
+    cuda_check(hnswgpu::launch_tc_select(sa, space, st), "select launch");
+    // queries the filter could not bound: exact kernel
+    std::vector<uint8_t> flags(nq);
+    cuda_check(cudaMemcpyAsync(flags.data(), h->tc_flags.p, nq, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    uint32_t status = 0;
+    cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+    cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    if (status & HNSWGPU_STATUS_TIMEOUT) throw ApiError(HNSWGPU_ERR_KERNEL, "tensor-core kernel timed out waiting");
+    std::vector<uint32_t> redo;
+    for (uint64_t i = 0; i < nq; i++)
+        if (flags[i]) redo.push_back((uint32_t)i);
+    if (!redo.empty()) {
+        const uint64_t m = redo.size();
+        h->tc_idx.ensure(m);
+        DevBuf<float> rq, rd;
+        DevBuf<uint64_t> rl;
+        DevBuf<int32_t> rc;
+        rq.alloc(m * dim);
+        rd.alloc(m * k);
+        rl.alloc(m * k);
+        rc.alloc(m);
+        cuda_check(cudaMemcpyAsync(h->tc_idx.p, redo.data(), m * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        cuda_check(hnswgpu::launch_tc_gather(dq, h->tc_idx.p, (uint32_t)m, dim, rq.p, st), "gather launch");
+        run_bf_exact(h, rq.p, m, k, dallow, rl.p, rd.p, rc.p, st);
+        cuda_check(hnswgpu::launch_tc_scatter(h->tc_idx.p, (uint32_t)m, (uint32_t)k, rl.p, rd.p, rc.p, dl, dd, dc, st),
+                   "scatter launch");
+        if (dtrace) {
+            // mark fallback queries in trace[2]
+            std::vector<uint32_t> tr(nq * 4);
+            cuda_check(cudaMemcpyAsync(tr.data(), dtrace, nq * 16, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            for (uint32_t i : redo) tr[(size_t)i * 4 + 2] = 1;
+            cuda_check(cudaMemcpyAsync(dtrace, tr.data(), nq * 16, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        }
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    }
+}
+
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
                 uint32_t prec, uint32_t rerank, const TermCfg* term, bool scan) {
     if (scan && !h->is_bf && h->num_deleted)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "HNSWGPU_EXACT_SCAN: the index has deleted elements");
-    if (h->is_bf || scan) {
+    if (h->is_bf && prec) {
+        run_bf_tc(h, dq, nq, k, rerank, dallow, dl, dd, dc, dtrace, st, prec);
+    } else if (h->is_bf || scan) {
         hnswgpu::BfParams b{};
         b.vecs = h->vecs.p;
         b.labels = h->dlabels.p;

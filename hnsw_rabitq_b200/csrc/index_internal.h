@@ -86,6 +86,13 @@ struct hnswgpu_index {
     DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
     DevBuf<unsigned char> term_model;  // learned termination: packed network
     DevBuf<uint64_t> cand_spill;       // tie-exact mode: candidate-heap tails
+    DevBuf<float2> tc_rowinfo[3];      // tensor-core brute force: (|x|^2, scale) per row and precision
+    // tensor-core brute force: per-call workspace
+    DevBuf<float> tc_qf, tc_qscale, tc_tau;
+    DevBuf<unsigned char> tc_qt;
+    DevBuf<uint32_t> tc_cnt, tc_idx;
+    DevBuf<uint64_t> tc_buf;
+    DevBuf<uint8_t> tc_flags;
     uint32_t term_period = 0;
     float term_logit = 0.f;
     std::mutex mu;

@@ -326,6 +326,11 @@ class BFIndex(_GpuIndex):
         self._maxel = 0
         self._dirty = False
         self.cur_l = 0
+        # "fp32": the reference's exact scan; "bf16" / "fp8": tensor-core scores
+        # over a low-precision copy, the best `rerank` candidates (default
+        # 4 k, at most 1024) re-ranked with exact float32 distances
+        self.precision = "fp32"
+        self.rerank = 0
 
     def __repr__(self):
         return f"<hnsw_rabitq_b200.BFIndex(space='{self.space}', dim={self.dim})>"
@@ -448,7 +453,17 @@ class BFIndex(_GpuIndex):
         if data.shape[1] != self.dim:
             raise RuntimeError("Wrong dimensionality of the vectors")
         self._sync()
-        labels, dists, counts, _ = self._search(data, k, filter)
+        labels, dists, counts, _ = self._search(data, k, filter, precision=self.precision, rerank=self.rerank)
         if counts.size and counts.min() < k:
             raise RuntimeError("Cannot return the results in a contiguous 2D array. There are not enough elements.")
         return labels, dists
+
+    def knn_query_traced(self, data, k: int = 1, filter=None, precision: Optional[str] = None,
+                         rerank: Optional[int] = None):
+        """knn_query plus, for the tensor-core forms, per-query counters
+        [candidates below the threshold, 0, 1 if answered by the exact
+        kernel, 0]; no exception for short results."""
+        data = _input_rows(data)
+        self._sync()
+        return self._search(data, k, filter, trace=True, precision=precision or self.precision,
+                            rerank=self.rerank if rerank is None else rerank)
