@@ -83,6 +83,9 @@ def parse():
     ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
     ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
     ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
+    ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768"],
+                    help="gmm1m128: the HNSW headline (default); bf768: tensor-core brute force, 1M x 768 IP, "
+                         "k=100, over-fetch 400, recall against float64 exact top-k")
     ap.add_argument("--serve-rates", type=int, nargs="*", default=[200_000, 1_000_000],
                     help="Poisson arrival rates (requests/s) of the serving-latency measurement")
     return ap.parse_args()
@@ -518,6 +521,101 @@ def serving_latency(idx, q, model, args, expect):
     return out
 
 
+def measured_tflops():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_bf768(args, dist: Dist):
+    """Tensor-core brute force on 1,000,000 unit vectors (dim 768, 256-component
+    mixture, inner product), 10,000 queries, k = 100, over-fetch 4 k = 400,
+    float32 re-rank; recall against the float64 exact top-100."""
+    import ctypes as C
+
+    import torch
+
+    from hnsw_rabitq_b200 import BFIndex, _capi
+    from hnsw_rabitq_b200.datasets import gmm_unit_ip
+    from hnsw_rabitq_b200.groundtruth import fp64_distances, fp64_topk
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    n = args.n if args.n != 1_000_000 else 1_000_000
+    x, q = gmm_unit_ip(n=n, nq=args.nq, dim=768)
+    g = BFIndex("ip", 768)
+    g.device = dev
+    g.init_index(n)
+    g.add_items(x)
+    g._sync()  # upload the rows now, outside any timed region
+    del x
+    k, R = 100, 400
+    if not args.profile_steps:
+        t0 = time.perf_counter()
+        gt, d64, cert = fp64_topk(g, q, k)
+        gt_s = time.perf_counter() - t0
+    lib = _capi.lib()
+    nq = q.shape[0]
+    dq = torch.from_numpy(q).to(f"cuda:{dev}")
+    dl = torch.empty((nq, k), dtype=torch.int64, device=f"cuda:{dev}")
+    dd = torch.empty((nq, k), dtype=torch.float32, device=f"cuda:{dev}")
+    dc = torch.empty((nq,), dtype=torch.int32, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(prec, steps, warmup):
+        o = _capi.SearchOpts()
+        o.flags, o.precision, o.rerank, o.stream = _capi.DEVICE_PTRS, prec, R, stream.cuda_stream
+        call = lambda: _capi.check(lib.hnswgpu_search(g._h, C.c_void_p(dq.data_ptr()), nq, k, C.byref(o),
+                                                      C.c_void_p(dl.data_ptr()), C.c_void_p(dd.data_ptr()),
+                                                      C.c_void_p(dc.data_ptr())))
+        for _ in range(warmup):
+            call()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            call()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        stream.synchronize()
+        return ev0.elapsed_time(ev1) / steps, dl.cpu().numpy().view(np.uint64), dd.cpu().numpy()
+
+    if args.profile_steps:  # only the bf16 tensor-core search (for ncu)
+        timed(_capi.PREC_BF16, args.steps, args.warmup)
+        return None
+    peak, kind = measured_tflops()
+    arms = {}
+    for name, prec in (("bf16", _capi.PREC_BF16), ("fp8", _capi.PREC_FP8)):
+        ms, lab, dist_ = timed(prec, args.steps, args.warmup)
+        r = float(np.mean([len(np.intersect1d(lab[i], gt[i])) for i in range(nq)]) / k)
+        d64r = fp64_distances(g, q, lab)
+        err = np.abs(dist_.astype(np.float64) - d64r) / np.maximum(np.abs(d64r), 1e-30)
+        flops = 2.0 * nq * n * 768
+        arms[name] = {"qps": round(nq / (ms / 1e3), 1), "ms_per_step": round(ms, 3), "recall@100_vs_fp64": round(r, 5),
+                      "max_rel_err_vs_fp64": float(err.max()), "mean_rel_err_vs_fp64": float(err.mean()),
+                      "tensor_tflops": round(flops / (ms / 1e3) / 1e12, 1),
+                      "frac_of_bf16_peak": round(flops / (ms / 1e3) / 1e12 / peak, 4)}
+    ms32, lab32, _ = timed(_capi.PREC_FP32, 1, 1)
+    r32 = float(np.mean([len(np.intersect1d(lab32[i], gt[i])) for i in range(nq)]) / k)
+    best = arms["fp8"] if arms["fp8"]["qps"] > arms["bf16"]["qps"] else arms["bf16"]
+    return {"metric": "QPS at recall@100 vs float64 exact top-100, tensor-core brute force (bf16 / fp8 scores, "
+                      "fp32 re-rank), 1M x 768 IP",
+            "value": best["qps"], "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 / fp8 e4m3 tensor-core scores, f32 re-rank", "data": "synthetic",
+            "config": {"workload": "gmm_unit_ip: 1,000,000 x 768 unit vectors (256-component mixture, noise norm 0.3), "
+                                   "10,000 queries, inner product, k=100, over-fetch 400",
+                       "fp64_gt_seconds": round(gt_s, 1), "fp64_gt_certified": float(cert.mean())},
+            "arms": arms,
+            "exact_fp32": {"qps": round(nq / (ms32 / 1e3), 1), "ms_per_step": round(ms32, 2),
+                           "recall@100_vs_fp64": round(r32, 5)},
+            "roofline": {"bound": "tensor", "achieved": best["tensor_tflops"], "peak": peak, "unit": "TFLOP/s",
+                         "frac": best["frac_of_bf16_peak"], "traffic": None,
+                         "peak_source": f"{kind} bf16 (MEASURED_PEAKS.json bf16_tflops); fp8 nominal peak is 2x"},
+            "gpu_launches": None}
+
+
 def committed_traffic(tie_order, ef):
     """DRAM bytes per launch of hnsw_search_kernel from the committed ncu
     summary (profiles/), for the same tie order and ef, or None."""
@@ -623,7 +721,7 @@ def main():
         return 0
     dist = Dist(args.gpus)
     try:
-        out = run_ours(args, dist)
+        out = run_bf768(args, dist) if args.workload == "bf768" else run_ours(args, dist)
     finally:
         dist.close()
     if out is not None and dist.rank == 0:

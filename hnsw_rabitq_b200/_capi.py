@@ -82,6 +82,7 @@ SIGNATURES = {
     "hnswgpu_term_train": (C.c_int, [C.c_int, P, P, U64, C.POINTER(TermTrainOpts), P, P]),
     "hnswgpu_term_loss_grad": (C.c_int, [C.c_int, P, P, P, U64, C.c_float, P, P]),
     "hnswgpu_term_logits": (C.c_int, [C.c_int, P, P, U64, P]),
+    "hnswgpu_fp64_distances": (C.c_int, [P, P, U64, P, U64, P]),
     "hnswgpu_server_create": (C.c_int, [P, C.POINTER(ServerOpts), C.POINTER(P)]),
     "hnswgpu_server_add_filter": (C.c_int, [P, P, C.POINTER(I32)]),
     "hnswgpu_server_submit": (C.c_int, [P, P, C.POINTER(Request), C.POINTER(U64)]),

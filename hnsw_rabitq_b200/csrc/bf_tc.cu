@@ -52,12 +52,45 @@ constexpr int kBBytes = kTileN * kKBytes;      // 32 KB
 constexpr int kStageBytes = kABytes + kBBytes;
 constexpr int kThreads = 192;
 constexpr int kTopT = 16;                      // sample rank of the threshold
+constexpr int kStageC = 8;                     // candidates staged per thread and tile
+
+#ifdef HNSWGPU_TC_TIMING
+// Opt-in role timing of the scores pass (not in the shipped library): per
+// CTA, cycles of [producer wait-empty, producer total, MMA wait-full, MMA
+// wait-tmem, MMA total, epilogue wait-tfull, epilogue busy, epilogue total].
+__device__ unsigned long long g_tc_timing[256][10];
+#define TCT_ADD(i, v) atomicAdd(&g_tc_timing[blockIdx.x & 255][i], (unsigned long long)(v))
+#else
+#define TCT_ADD(i, v)
+#endif
 
 struct TcSmem {
+    float2 hinfo[2][kTileN];  // per-row helpers of the tiles in the two accumulators
+    uint64_t cst[128][2][kStageC];  // candidates of the current / previous tile per epilogue thread
     uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], done;
     uint32_t tmem, error;
 };
 constexpr size_t kSmemBytes = 1024 + (size_t)kStages * kStageBytes + sizeof(TcSmem);
+
+// Bounded pipeline wait without a suspend-time hint: the tile pipeline waits
+// ~26 times per tile, and a suspended thread's late wake-up cost more than
+// the spin (measured).  The bound (2^26 polls, seconds) only ends a wait
+// that can no longer complete.
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t addr = smem_u32(bar);
+    for (uint32_t it = 0; it < (1u << 26); it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 __device__ __forceinline__ void tc_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -114,6 +147,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
     for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 consecutive fp32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
+    uint32_t r[64];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -126,6 +170,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~(uintptr_t)1023);
     TcSmem& s = *reinterpret_cast<TcSmem*>(base + (size_t)kStages * kStageBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // bf16 inner product needs no per-row helper (every scale is 1)
+    constexpr bool NEEDH = !(PREC == 1 && SPACE == 1);
 
     const uint32_t q_tiles = (a.nq + kTileM - 1) / kTileM;
     const uint32_t n_tiles = (a.n_rows + kTileN - 1) / kTileN;
@@ -160,29 +206,45 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         // ---- TMA producer
         if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
+            int stage = 0, hacc = 0;
+            uint32_t phase = 0, haphase = 0;
+            const long long p0 = clock64();
             for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x) {
                 const uint32_t qt = it % q_tiles, ck = it / q_tiles;
                 const uint32_t t_end = min(n_tiles, (ck + 1) * chunk);
                 for (uint32_t t = ck * chunk; t < t_end && !*err; t++) {
+                    // the helper slot of this tile is the one of its accumulator:
+                    // free once the epilogue released that accumulator
+                    if (NEEDH && !tc_wait(&s.tempty[hacc], haphase ^ 1u)) {
+                        *err = 1;
+                        break;
+                    }
                     for (int kb = 0; kb < kb_count; kb++) {
-                        if (!mbar_wait(&s.empty[stage], phase ^ 1u)) {
+                        const long long w0 = clock64();
+                        if (!tc_wait(&s.empty[stage], phase ^ 1u)) {
                             *err = 1;
                             break;
                         }
+                        TCT_ADD(0, clock64() - w0);
                         unsigned char* sa = base + (size_t)stage * kStageBytes;
-                        mbar_arrive_expect_tx(&s.full[stage], kStageBytes);
+                        const bool with_h = NEEDH && kb == 0;
+                        mbar_arrive_expect_tx(&s.full[stage], kStageBytes + (with_h ? kTileN * 8 : 0));
                         const int x = kb * (PREC == 1 ? kKBytes / 2 : kKBytes);
                         tma_load_2d(sa, &qmap, x, (int)(qt * kTileM), &s.full[stage]);
                         tma_load_2d(sa + kABytes, &xmap, x, (int)(t * kTileN), &s.full[stage]);
+                        if (with_h) bulk_g2s(&s.hinfo[hacc][0], a.rowinfo + (size_t)t * kTileN, kTileN * 8, &s.full[stage]);
                         if (++stage == kStages) {
                             stage = 0;
                             phase ^= 1u;
                         }
                     }
+                    if (++hacc == 2) {
+                        hacc = 0;
+                        haphase ^= 1u;
+                    }
                 }
             }
+            TCT_ADD(1, clock64() - p0);
         }
     } else if (warp == 1) {
         // ---- MMA issuer
@@ -193,21 +255,26 @@ __global__ void __launch_bounds__(kThreads, 1)
                                    ((uint32_t)(kTileN >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
             int stage = 0, acc = 0;
             uint32_t phase = 0, aphase = 0;
+            const long long m0 = clock64();
             for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x) {
                 const uint32_t ck = it / q_tiles;
                 const uint32_t t_end = min(n_tiles, (ck + 1) * chunk);
                 for (uint32_t t = ck * chunk; t < t_end && !*err; t++) {
-                    if (!mbar_wait(&s.tempty[acc], aphase ^ 1u)) {
+                    const long long w1 = clock64();
+                    if (!tc_wait(&s.tempty[acc], aphase ^ 1u)) {
                         *err = 1;
                         break;
                     }
+                    TCT_ADD(3, clock64() - w1);
                     tc_fence_after();
                     const uint32_t d = tmem + (uint32_t)acc * kTileN;
                     for (int kb = 0; kb < kb_count; kb++) {
-                        if (!mbar_wait(&s.full[stage], phase)) {
+                        const long long w2 = clock64();
+                        if (!tc_wait(&s.full[stage], phase)) {
                             *err = 1;
                             break;
                         }
+                        TCT_ADD(2, clock64() - w2);
                         tc_fence_after();
                         const uint32_t sa = smem_u32(base + (size_t)stage * kStageBytes);
                         const uint64_t da = umma_desc(sa), db = umma_desc(sa + kABytes);
@@ -227,9 +294,10 @@ __global__ void __launch_bounds__(kThreads, 1)
                     }
                 }
             }
+            TCT_ADD(4, clock64() - m0);
             // every MMA issued has completed before TMEM is released
             umma_commit(&s.done);
-            mbar_wait(&s.done, 0);
+            tc_wait(&s.done, 0);
         }
         __syncwarp();
     } else {
@@ -238,58 +306,106 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int r = quarter * 32 + lane;  // query row within the tile
         int acc = 0;
         uint32_t aphase = 0;
+        const long long e0 = clock64();
         for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x) {
             const uint32_t qt = it % q_tiles, ck = it / q_tiles;
             const uint32_t q = qt * kTileM + r;
             const bool qok = q < a.nq;
-            const float tau = (MODE == 0 && qok) ? a.tau[q] : __int_as_float(0x7f800000);
+            // queries past nq get tau = -inf: no candidate passes
+            const float tau = !qok ? -__int_as_float(0x7f800000)
+                                   : (MODE == 0 ? a.tau[q] : __int_as_float(0x7f800000));
             const float sq = qok ? a.qscale[q] : 0.f;
+            // IP: d = -(s sq sc); L2: d = |x|^2 - 2 s sq sc
+            const float coef = (SPACE == 0 ? -2.0f : -1.0f) * sq;
+            // candidates of a tile are staged, then claimed with one atomic
+            // whose result is used a tile later (its latency hidden)
+            uint64_t* cst = &s.cst[r][0][0];
+            int cb_cur = 0, n_cur = 0, n_prev = 0;
+            uint32_t prev_slot = 0;
             float top[kTopT];
 #pragma unroll
             for (int i = 0; i < kTopT; i++) top[i] = __int_as_float(0x7f800000);
             const uint32_t t_end = min(n_tiles, (ck + 1) * chunk);
             for (uint32_t t = ck * chunk; t < t_end; t++) {
-                if (!mbar_wait(&s.tfull[acc], aphase)) {
+                const long long w3 = clock64();
+                if (!tc_wait(&s.tfull[acc], aphase)) {
                     *err = 1;
                     break;
                 }
+                const long long b0 = clock64();
+                if (lane == 0) TCT_ADD(5, b0 - w3);
                 tc_fence_after();
                 const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * kTileN;
+                const float2* hinfo = s.hinfo[acc];
 #pragma unroll 1
-                for (int c0 = 0; c0 < kTileN; c0 += 32) {
-                    float v[32];
-                    tmem_ld32(taddr + (uint32_t)c0, v);
+                for (int cb = 0; cb < 4; cb++) {
+                    float v[64];
+#ifdef HNSWGPU_TC_TIMING
+                    const long long l0 = clock64();
+#endif
+                    tmem_ld64(taddr + (uint32_t)(cb * 64), v);
+#ifdef HNSWGPU_TC_TIMING
+                    if (lane == 0) TCT_ADD(8, clock64() - l0);
+#endif
 #pragma unroll
-                    for (int j = 0; j < 32; j++) {
-                        // per-row helpers (|x|^2, scale): the same address in
-                        // every lane, an L1 broadcast
-                        const uint32_t lr = t * kTileN + (uint32_t)(c0 + j);
-                        // NaN compares false with everything: rows past the
-                        // end, queries past nq and filtered rows are never kept
-                        float dd = __int_as_float(0x7fc00000);
-                        if (qok && lr < a.n_rows) {
-                            const uint64_t g = (uint64_t)lr * a.row_step;
-                            const float2 inf = __ldg(a.rowinfo + g);
-                            const float dot = v[j] * sq * inf.y;
-                            dd = SPACE == 0 ? fmaf(-2.0f, dot, inf.x) : -dot;
-                            if (a.allow && !a.allow[g]) dd = __int_as_float(0x7fc00000);  // NaN: never kept
+                    for (int j = 0; j < 64; j++) {
+                        const int col = cb * 64 + j;
+                        float dd;
+                        if (!NEEDH) {
+                            dd = v[j] * coef;
+                        } else {
+                            const float2 h = hinfo[col];  // one broadcast shared-memory load
+                            const float sv = PREC == 1 ? v[j] : v[j] * h.y;
+                            dd = SPACE == 0 ? fmaf(sv, coef, h.x) : sv * coef;
                         }
+                        // row range and filter are checked only for the rare
+                        // rows that pass the threshold
                         if (MODE == 0) {
-                            if (dd <= tau) {  // false for NaN
-                                const uint32_t slot = atomicAdd(a.cnt + q, 1u);
-                                if (slot < a.cap)
-                                    a.buf[(size_t)q * a.cap + slot] = mkkey(dd, (uint32_t)((uint64_t)lr * a.row_step));
+                            if (dd <= tau) {
+                                const uint32_t lr = t * kTileN + (uint32_t)col;
+                                const uint64_t g = (uint64_t)lr * a.row_step;
+                                if (lr < a.n_rows && (!a.allow || a.allow[g])) {
+                                    const uint64_t key = mkkey(dd, (uint32_t)g);
+                                    if (n_cur < kStageC) {
+                                        cst[cb_cur * kStageC + n_cur++] = key;
+                                    } else {  // more than kStageC in one tile: direct append
+                                        const uint32_t slot = atomicAdd(a.cnt + q, 1u);
+                                        if (slot < a.cap) a.buf[(size_t)q * a.cap + slot] = key;
+                                    }
+                                }
                             }
                         } else if (dd < top[kTopT - 1]) {
+                            const uint32_t lr = t * kTileN + (uint32_t)col;
+                            const uint64_t g = (uint64_t)lr * a.row_step;
+                            if (lr < a.n_rows && (!a.allow || a.allow[g])) {
 #pragma unroll
-                            for (int i = 0; i < kTopT; i++) {
-                                const float lo = fminf(dd, top[i]), hi = fmaxf(dd, top[i]);
-                                top[i] = lo;
-                                dd = hi;
+                                for (int i = 0; i < kTopT; i++) {
+                                    const float lo = fminf(dd, top[i]), hi = fmaxf(dd, top[i]);
+                                    top[i] = lo;
+                                    dd = hi;
+                                }
                             }
                         }
                     }
                 }
+#ifdef HNSWGPU_TC_TIMING
+                const long long f0 = clock64();
+#endif
+                if (MODE == 0) {
+                    // write the previous tile's candidates (their slots were
+                    // claimed a tile ago), then claim this tile's
+                    for (int i = 0; i < n_prev; i++)
+                        if (prev_slot + i < a.cap)
+                            a.buf[(size_t)q * a.cap + prev_slot + i] = cst[(cb_cur ^ 1) * kStageC + i];
+                    n_prev = n_cur;
+                    if (n_cur) prev_slot = atomicAdd(a.cnt + q, (uint32_t)n_cur);
+                    n_cur = 0;
+                    cb_cur ^= 1;
+                }
+#ifdef HNSWGPU_TC_TIMING
+                if (lane == 0) TCT_ADD(9, clock64() - f0);
+#endif
+                if (lane == 0) TCT_ADD(6, clock64() - b0);
                 tc_fence_before();
                 tc_arrive(&s.tempty[acc]);
                 if (++acc == 2) {
@@ -298,7 +414,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
             }
             if (MODE == 1 && qok) a.tau[q] = top[kTopT - 1];
+            if (MODE == 0)  // the item's last claimed batch
+                for (int i = 0; i < n_prev; i++)
+                    if (prev_slot + i < a.cap)
+                        a.buf[(size_t)q * a.cap + prev_slot + i] = cst[(cb_cur ^ 1) * kStageC + i];
         }
+        if (lane == 0) TCT_ADD(7, clock64() - e0);
     }
     __syncthreads();
     if (threadIdx.x == 0 && *err) atomicOr(a.status, HNSWGPU_STATUS_TIMEOUT_BIT);
@@ -364,6 +485,14 @@ __global__ void tc_query_prep_kernel(const float* __restrict__ q, uint32_t nq, u
     if (lane == 0) qscale[row] = scale;
 }
 
+// Helpers of the sampled rows, contiguous (the threshold pass reads them
+// tile by tile with bulk copies).
+__global__ void tc_gather_info_kernel(const float2* __restrict__ info, uint64_t n_sample, uint64_t step,
+                                      float2* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_sample) out[i] = info[i * step];
+}
+
 __global__ void tc_fill_kernel(float* p, uint64_t n, float v) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -415,14 +544,25 @@ __global__ void __launch_bounds__(256) tc_select_rerank_kernel(TcSelectArgs a) {
     uint32_t P2 = 1;
     while (P2 < R) P2 <<= 1;
     // exact float32 distances of the R best, reference summation order
-    for (uint32_t i = t; i < P2; i += blockDim.x) {
-        uint64_t e = ~0ull;
-        if (i < R) {
-            const uint32_t row = (uint32_t)keys[i];  // the candidate's row
-            const float d = distance<SPACE>(qv, a.vecs + (size_t)row * a.row_floats, (int)a.dim);
-            e = ((uint64_t)fkey(d) << 32) | i;
+    if (R > 0 && (a.dim & 15) == 0) {
+        // 4 lanes per row (coalesced 64-byte reads), 8 rows per warp step
+        const int warp = t >> 5, lane = t & 31, nw = blockDim.x >> 5;
+        for (uint32_t b = (uint32_t)warp * 8; b < P2; b += (uint32_t)nw * 8) {
+            const uint32_t i = b + (lane >> 2);
+            const uint32_t row = i < R ? (uint32_t)keys[i] : (uint32_t)keys[0];
+            const float d = group4_dist16<SPACE>(qv, a.vecs + (size_t)row * a.row_floats, (int)(a.dim >> 4), lane & 3);
+            if ((lane & 3) == 0 && i < P2) ek[i] = i < R ? (((uint64_t)fkey(d) << 32) | i) : ~0ull;
         }
-        ek[i] = e;
+    } else {
+        for (uint32_t i = t; i < P2; i += blockDim.x) {
+            uint64_t e = ~0ull;
+            if (i < R) {
+                const uint32_t row = (uint32_t)keys[i];  // the candidate's row
+                const float d = distance<SPACE>(qv, a.vecs + (size_t)row * a.row_floats, (int)a.dim);
+                e = ((uint64_t)fkey(d) << 32) | i;
+            }
+            ek[i] = e;
+        }
     }
     __syncthreads();
     for (uint32_t kk = 2; kk <= P2; kk <<= 1)
@@ -496,6 +636,41 @@ __global__ void tc_scatter_results_kernel(const uint32_t* __restrict__ idx, uint
     if (j == 0) oc[idx[r]] = c[r];
 }
 
+// Ground-truth oracle: float64 distances of (query, row) pairs, one warp per
+// pair (the only float64 arithmetic of the library).  space 0: squared L2;
+// 1: 1 - inner product, the query normalised in float64 when `normalize`.
+__global__ void fp64_distance_kernel(const float* __restrict__ q, uint64_t npairs, uint32_t m, uint32_t dim,
+                                     const float* __restrict__ vecs, uint32_t row_floats,
+                                     const uint32_t* __restrict__ rows, int space, int normalize,
+                                     double* __restrict__ out) {
+    const uint64_t pair = (uint64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+    const int lane = threadIdx.x & 31;
+    if (pair >= npairs) return;
+    const uint32_t row = rows[pair];
+    if (row == 0xffffffffu) {
+        if (lane == 0) out[pair] = __longlong_as_double(0x7ff8000000000000ll);
+        return;
+    }
+    const float* qv = q + (pair / m) * dim;
+    const float* xv = vecs + (uint64_t)row * row_floats;
+    double qs = 1.0;
+    if (normalize) {
+        double n2 = 0.0;
+        for (uint32_t i = lane; i < dim; i += 32) n2 = fma((double)qv[i], (double)qv[i], n2);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        qs = n2 > 0.0 ? 1.0 / sqrt(n2) : 1.0;
+    }
+    double acc = 0.0;
+    for (uint32_t i = lane; i < dim; i += 32) {
+        const double a = (double)qv[i] * qs, b = (double)xv[i];
+        acc = space == 0 ? fma(a - b, a - b, acc) : fma(a, b, acc);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[pair] = space == 0 ? acc : 1.0 - acc;
+}
+
 template <int PREC, int SPACE, int MODE>
 cudaError_t launch_tc(const CUtensorMap& qm, const CUtensorMap& xm, const TcArgs& a, int grid, cudaStream_t st) {
     auto fn = bf_tc_kernel<PREC, SPACE, MODE>;
@@ -508,6 +683,25 @@ cudaError_t launch_tc(const CUtensorMap& qm, const CUtensorMap& xm, const TcArgs
 }  // namespace
 
 size_t tc_smem_bytes() { return kSmemBytes; }
+
+#ifdef HNSWGPU_TC_TIMING
+cudaError_t tc_timing_read(unsigned long long* out) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_tc_timing, sizeof(unsigned long long) * 256 * 10);
+    if (e != cudaSuccess) return e;
+    static unsigned long long z[256][10];
+    return cudaMemcpyToSymbol(g_tc_timing, z, sizeof(z));
+}
+#endif
+
+cudaError_t launch_fp64_distances(const float* q, uint64_t nq, uint32_t m, uint32_t dim, const float* vecs,
+                                  uint32_t row_floats, const uint32_t* rows, int space, int normalize, double* out,
+                                  cudaStream_t st) {
+    const uint64_t npairs = nq * m;
+    if (!npairs) return cudaSuccess;
+    fp64_distance_kernel<<<(unsigned)((npairs + 7) / 8), 256, 0, st>>>(q, npairs, m, dim, vecs, row_floats, rows,
+                                                                       space, normalize, out);
+    return cudaGetLastError();
+}
 
 cudaError_t tc_encode_map(void* base, uint32_t prec, uint64_t rows, uint32_t dim, uint64_t row_pitch_bytes,
                           uint32_t box_rows, CUtensorMap* out) {
@@ -557,6 +751,13 @@ cudaError_t launch_tc_query_prep(const float* q, uint32_t nq, uint32_t dim, uint
                                  uint32_t trow_bytes, float* qf, unsigned char* qt, float* qscale, cudaStream_t st) {
     if (!nq) return cudaSuccess;
     tc_query_prep_kernel<<<(nq + 7) / 8, 256, 0, st>>>(q, nq, dim, normalize, prec, trow_bytes, qf, qt, qscale);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tc_gather_info(const float2* info, uint64_t n_sample, uint64_t step, float2* out,
+                                  cudaStream_t st) {
+    if (!n_sample) return cudaSuccess;
+    tc_gather_info_kernel<<<(unsigned)((n_sample + 255) / 256), 256, 0, st>>>(info, n_sample, step, out);
     return cudaGetLastError();
 }
 

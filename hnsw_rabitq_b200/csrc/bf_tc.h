@@ -15,7 +15,7 @@ struct TcArgs {
     uint64_t row_step;         // global row id = map row x row_step
     uint32_t k_blocks;         // 128-byte K blocks per row
     uint32_t chunk_tiles;      // MODE 0: 256-row tiles per work item
-    const float2* rowinfo;     // per global row: (|x|^2, scale)
+    const float2* rowinfo;     // per map row: (|x|^2, scale), padded to whole 256-row tiles
     const float* qscale;       // per query: scale of its low-precision row
     const uint8_t* allow;      // optional per-row mask
     float* tau;                // per query: threshold (MODE 0 reads, MODE 1 writes)
@@ -40,6 +40,9 @@ struct TcSelectArgs {
 };
 
 size_t tc_smem_bytes();
+cudaError_t launch_fp64_distances(const float* q, uint64_t nq, uint32_t m, uint32_t dim, const float* vecs,
+                                  uint32_t row_floats, const uint32_t* rows, int space, int normalize, double* out,
+                                  cudaStream_t st);
 size_t tc_select_smem(uint32_t sort_cap, uint32_t dim, uint32_t R);
 cudaError_t tc_encode_map(void* base, uint32_t prec, uint64_t rows, uint32_t dim, uint64_t row_pitch_bytes,
                           uint32_t box_rows, CUtensorMap* out);
@@ -51,6 +54,8 @@ cudaError_t launch_tc_rowinfo(const float* vecs, uint32_t count, uint32_t dim, u
 cudaError_t launch_tc_query_prep(const float* q, uint32_t nq, uint32_t dim, uint32_t normalize, uint32_t prec,
                                  uint32_t trow_bytes, float* qf, unsigned char* qt, float* qscale, cudaStream_t st);
 cudaError_t launch_tc_fill(float* p, uint64_t n, float v, cudaStream_t st);
+cudaError_t launch_tc_gather_info(const float2* info, uint64_t n_sample, uint64_t step, float2* out,
+                                  cudaStream_t st);
 cudaError_t launch_tc_select(const TcSelectArgs& a, int space, cudaStream_t st);
 cudaError_t launch_tc_gather(const float* src, const uint32_t* idx, uint32_t n, uint32_t dim, float* dst,
                              cudaStream_t st);

@@ -41,6 +41,12 @@ static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feat
 
 #include "index_internal.h"
 
+#ifdef HNSWGPU_TC_TIMING
+namespace hnswgpu {
+cudaError_t tc_timing_read(unsigned long long* out);
+}
+#endif
+
 namespace hnswgpu_host {
 thread_local std::string g_last_error;
 }  // namespace hnswgpu_host
@@ -535,7 +541,7 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
     ensure_traversal_copy(h, prec);
     const uint32_t trow = hnswgpu::traversal_row_bytes(prec, dim);
     if (first) {
-        h->tc_rowinfo[prec].alloc(n);
+        h->tc_rowinfo[prec].alloc((n + 255) / 256 * 256);  // whole tiles: read by 2 KB bulk copies
         cuda_check(hnswgpu::launch_tc_rowinfo(h->vecs.p, (uint32_t)n, dim, h->row_floats, h->tcopy[prec].p, trow, prec,
                                               h->tc_rowinfo[prec].p, h->stream),
                    "rowinfo launch");
@@ -585,9 +591,13 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
     if (sampled) {
         cuda_check(hnswgpu::tc_encode_map(h->tcopy[prec].p, prec, n_sample, dim, (uint64_t)trow * step, 256, &smap),
                    "tensor map (sample)");
+        h->tc_sinfo.ensure((n_sample + 255) / 256 * 256);
+        cuda_check(hnswgpu::launch_tc_gather_info(h->tc_rowinfo[prec].p, n_sample, step, h->tc_sinfo.p, st),
+                   "gather launch");
         hnswgpu::TcArgs t = a;
         t.n_rows = (uint32_t)n_sample;
         t.row_step = step;
+        t.rowinfo = h->tc_sinfo.p;
         t.chunk_tiles = 1;
         cuda_check(hnswgpu::launch_tc_scores(qmap, smap, t, prec, space, 1, h->num_sms, st), "threshold launch");
     } else {
@@ -597,9 +607,13 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
     a.n_rows = (uint32_t)n;
     a.row_step = 1;
     {
-        const uint64_t q_tiles = (nq + 127) / 128, n_tiles = (n + 255) / 256;
-        a.chunk_tiles = (uint32_t)std::max<uint64_t>(1, (q_tiles * n_tiles + 8ull * h->num_sms - 1) / (8ull * h->num_sms));
-        a.chunk_tiles = std::min<uint32_t>(a.chunk_tiles, (uint32_t)n_tiles);
+        // Work items are (query tile, 16 row tiles), ordered row-chunk major:
+        // the CTAs running at one time share one or two chunks (a few MB of
+        // rows), so each row tile comes from HBM once and from L2 for every
+        // other query tile.  Chunks of ~100 MB (a few items per CTA) missed
+        // L2 and re-read the rows ~11 times.
+        const uint64_t n_tiles = (n + 255) / 256;
+        a.chunk_tiles = (uint32_t)std::min<uint64_t>(16, n_tiles);
     }
     cuda_check(hnswgpu::launch_tc_scores(qmap, xmap, a, prec, space, 0, h->num_sms, st), "scores launch");
     if (dtrace) cuda_check(cudaMemsetAsync(dtrace, 0, nq * 16, st), "cudaMemsetAsync");
@@ -936,6 +950,37 @@ int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint6
     });
 }
 
+int hnswgpu_fp64_distances(hnswgpu_index* h, const float* queries, uint64_t nq, const uint64_t* labels, uint64_t m,
+                           double* out) {
+    return guarded([&] {
+        if (!h || (nq && m && (!queries || !labels || !out))) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (m > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "too many rows per query");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (!nq || !m) return HNSWGPU_OK;
+        std::vector<uint32_t> rows(nq * m);
+        for (uint64_t i = 0; i < nq * m; i++) {
+            auto it = h->lookup.find(labels[i]);
+            rows[i] = it == h->lookup.end() ? 0xffffffffu : it->second;
+        }
+        DevBuf<float> dq;
+        DevBuf<uint32_t> dr;
+        DevBuf<double> dout;
+        dq.alloc(nq * h->dim);
+        dr.alloc(nq * m);
+        dout.alloc(nq * m);
+        cuda_check(cudaMemcpyAsync(dq.p, queries, nq * h->dim * 4, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(dr.p, rows.data(), nq * m * 4, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+        cuda_check(hnswgpu::launch_fp64_distances(dq.p, nq, (uint32_t)m, (uint32_t)h->dim, h->vecs.p, h->row_floats, dr.p,
+                                                  h->space == HNSWGPU_SPACE_L2 ? 0 : 1,
+                                                  h->space == HNSWGPU_SPACE_COSINE ? 1 : 0, dout.p, h->stream),
+                   "fp64 distance launch");
+        cuda_check(cudaMemcpyAsync(out, dout.p, nq * m * 8, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        return HNSWGPU_OK;
+    });
+}
+
 int hnswgpu_set_termination_model(hnswgpu_index* h, const float* params, uint32_t period, float logit_threshold) {
     return guarded([&] {
         if (!h || h->is_bf) return fail(HNSWGPU_ERR_ARG, "a termination model needs an HNSW index");
@@ -1080,6 +1125,11 @@ HNSWGPU_API int hnswgpu_debug_record(unsigned long long* out) {
 }
 #endif
 
+#ifdef HNSWGPU_TC_TIMING
+HNSWGPU_API int hnswgpu_tc_timing(unsigned long long* out) {
+    return hnswgpu::tc_timing_read(out) == cudaSuccess ? 0 : -4;
+}
+#endif
 #ifdef HNSWGPU_PHASE_TIMING
 // Profiling builds only: per-phase cycle totals of all searches since the
 // last call (10 counters), cleared on read.

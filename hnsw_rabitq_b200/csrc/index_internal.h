@@ -89,6 +89,7 @@ struct hnswgpu_index {
     DevBuf<float2> tc_rowinfo[3];      // tensor-core brute force: (|x|^2, scale) per row and precision
     // tensor-core brute force: per-call workspace
     DevBuf<float> tc_qf, tc_qscale, tc_tau;
+    DevBuf<float2> tc_sinfo;           // helpers of the sampled rows
     DevBuf<unsigned char> tc_qt;
     DevBuf<uint32_t> tc_cnt, tc_idx;
     DevBuf<uint64_t> tc_buf;

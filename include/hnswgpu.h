@@ -94,10 +94,13 @@ typedef struct hnswgpu_info {
 
 typedef struct hnswgpu_search_opts {
     uint32_t flags;            /* HNSWGPU_DEVICE_PTRS | HNSWGPU_TRACE | ...     */
-    uint32_t precision;        /* HNSW traversal copy: HNSWGPU_PREC_FP32 (the
-                                  reference's search), _BF16 or _FP8; the
-                                  low-precision forms re-rank the best
-                                  `rerank` candidates with exact FP32
+    uint32_t precision;        /* HNSWGPU_PREC_FP32 (the reference's search),
+                                  _BF16 or _FP8.  HNSW: the beam traverses
+                                  that copy of the vectors; brute force: the
+                                  scan runs on the tensor cores over that
+                                  copy (sampled threshold, fused candidate
+                                  filter; synchronises).  Both re-rank the
+                                  best `rerank` candidates with exact FP32
                                   distances before returning k.                */
     uint64_t ef;               /* 0: use the index's ef_ (setEf)               */
     const uint8_t* allow;      /* optional per-internal-id byte mask: nonzero =
@@ -109,7 +112,9 @@ typedef struct hnswgpu_search_opts {
                                   level-0 expansions, level-0 distances.
                                   Same memory kind as the queries.            */
     void* stream;              /* cudaStream_t; NULL = the index's own stream  */
-    uint32_t rerank;           /* low precision: candidates re-ranked (0: ef)  */
+    uint32_t rerank;           /* low precision: candidates re-ranked; HNSW:
+                                  0 = ef; brute force: the over-fetch of the
+                                  tensor-core scan, 0 = 4 k, at most 1024     */
     uint32_t reserved1;
 } hnswgpu_search_opts;
 
@@ -211,6 +216,15 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
 HNSWGPU_API int hnswgpu_search_noalloc(const hnswgpu_index* index, const float* d_queries, uint64_t nq, uint64_t k,
                                        uint64_t ef, uint32_t flags, const uint8_t* d_allow, uint64_t* d_labels,
                                        float* d_dists, int32_t* d_counts, void* stream);
+
+/* Ground-truth oracle: float64 distances between each query and m rows
+ * given by label (labels: nq x m; out: nq x m doubles, NaN for an unknown
+ * label), in the index's space (squared L2; 1 - inner product; cosine with
+ * the query normalised in float64).  The only float64 arithmetic of the
+ * library; used to measure recall and the error of returned float32
+ * distances.  No counterpart in the reference. */
+HNSWGPU_API int hnswgpu_fp64_distances(hnswgpu_index* index, const float* queries, uint64_t nq,
+                                       const uint64_t* labels, uint64_t m, double* out);
 
 /* ------------------------------------------------ learned early termination
  * No counterpart in the reference, whose beam always runs until its

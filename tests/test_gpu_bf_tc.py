@@ -92,3 +92,29 @@ def test_rejects_large_overfetch():
     g = _bf(x, "l2")
     with pytest.raises(RuntimeError, match="over-fetch"):
         g.knn_query_traced(x[:2], 10, precision="bf16", rerank=2000)
+
+
+def test_fp64_oracle():
+    """The float64 oracle against numpy float64; its top-k certified."""
+    from hnsw_rabitq_b200.groundtruth import fp64_distances, fp64_topk
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((20000, 48)).astype(np.float32)
+    q = rng.standard_normal((50, 48)).astype(np.float32)
+    for space in ("l2", "ip", "cosine"):
+        g = _bf(x, space)
+        lab = rng.integers(0, 20000, (50, 7)).astype(np.uint64)
+        d = fp64_distances(g, q, lab)
+        xs = x.astype(np.float64)
+        if space == "cosine":
+            xs = O.normalize(x).astype(np.float64)  # stored rows are the binding's normalised float32
+            qs = q.astype(np.float64) / np.linalg.norm(q.astype(np.float64), axis=1, keepdims=True)
+        else:
+            qs = q.astype(np.float64)
+        rows = xs[lab.astype(np.int64)]
+        ref = ((qs[:, None, :] - rows) ** 2).sum(-1) if space == "l2" else 1.0 - (qs[:, None, :] * rows).sum(-1)
+        assert np.allclose(d, ref, rtol=1e-12, atol=1e-12)
+        tl, td, cert = fp64_topk(g, q, 10)
+        assert cert.all()
+        full = ((qs[:, None, :] - xs[None]) ** 2).sum(-1) if space == "l2" else 1.0 - qs @ xs.T
+        want = np.argsort(full, axis=1, kind="stable")[:, :10]
+        assert np.array_equal(tl.astype(np.int64), want)
