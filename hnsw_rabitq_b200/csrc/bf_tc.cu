@@ -158,6 +158,14 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, float* v) {
     for (int i = 0; i < 64; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// One accumulator column of this thread's TMEM lane (whole warp).
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return __uint_as_float(r);
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -347,43 +355,61 @@ __global__ void __launch_bounds__(kThreads, 1)
 #ifdef HNSWGPU_TC_TIMING
                     if (lane == 0) TCT_ADD(8, clock64() - l0);
 #endif
+                    // (1) unrolled and small: distances and a mask of the
+                    // columns under the threshold (rare)
+                    const float thr = MODE == 0 ? tau : top[kTopT - 1];
+                    uint32_t m_lo = 0, m_hi = 0;
 #pragma unroll
                     for (int j = 0; j < 64; j++) {
-                        const int col = cb * 64 + j;
                         float dd;
                         if (!NEEDH) {
                             dd = v[j] * coef;
                         } else {
-                            const float2 h = hinfo[col];  // one broadcast shared-memory load
+                            const float2 h = hinfo[cb * 64 + j];  // one broadcast shared-memory load
                             const float sv = PREC == 1 ? v[j] : v[j] * h.y;
                             dd = SPACE == 0 ? fmaf(sv, coef, h.x) : sv * coef;
                         }
-                        // row range and filter are checked only for the rare
-                        // rows that pass the threshold
+                        const bool p = MODE == 0 ? dd <= thr : dd < thr;
+                        if (j < 32) m_lo |= (uint32_t)p << j;
+                        else m_hi |= (uint32_t)p << (j - 32);
+                    }
+                    // (2) rolled, warp-uniform: each column some lane passes;
+                    // its score is read again from TMEM (one column)
+                    uint64_t any = ((uint64_t)__reduce_or_sync(0xffffffffu, m_hi) << 32) |
+                                   __reduce_or_sync(0xffffffffu, m_lo);
+                    const uint64_t mine = ((uint64_t)m_hi << 32) | m_lo;
+                    while (any) {
+                        const int j = __ffsll((long long)any) - 1;
+                        any &= any - 1;
+                        const int col = cb * 64 + j;
+                        __syncwarp();  // converge after the previous iteration's divergent tail
+                        const float sc = tmem_ld1(taddr + (uint32_t)col);
+                        if (!((mine >> j) & 1)) continue;
+                        float dd;
+                        if (!NEEDH) {
+                            dd = sc * coef;
+                        } else {
+                            const float2 h = hinfo[col];
+                            const float sv = PREC == 1 ? sc : sc * h.y;
+                            dd = SPACE == 0 ? fmaf(sv, coef, h.x) : sv * coef;
+                        }
+                        const uint32_t lr = t * kTileN + (uint32_t)col;
+                        const uint64_t g = (uint64_t)lr * a.row_step;
+                        if (lr >= a.n_rows || (a.allow && !a.allow[g])) continue;
                         if (MODE == 0) {
-                            if (dd <= tau) {
-                                const uint32_t lr = t * kTileN + (uint32_t)col;
-                                const uint64_t g = (uint64_t)lr * a.row_step;
-                                if (lr < a.n_rows && (!a.allow || a.allow[g])) {
-                                    const uint64_t key = mkkey(dd, (uint32_t)g);
-                                    if (n_cur < kStageC) {
-                                        cst[cb_cur * kStageC + n_cur++] = key;
-                                    } else {  // more than kStageC in one tile: direct append
-                                        const uint32_t slot = atomicAdd(a.cnt + q, 1u);
-                                        if (slot < a.cap) a.buf[(size_t)q * a.cap + slot] = key;
-                                    }
-                                }
+                            const uint64_t key = mkkey(dd, (uint32_t)g);
+                            if (n_cur < kStageC) {
+                                cst[cb_cur * kStageC + n_cur++] = key;
+                            } else {  // more than kStageC in one tile: direct append
+                                const uint32_t slot = atomicAdd(a.cnt + q, 1u);
+                                if (slot < a.cap) a.buf[(size_t)q * a.cap + slot] = key;
                             }
                         } else if (dd < top[kTopT - 1]) {
-                            const uint32_t lr = t * kTileN + (uint32_t)col;
-                            const uint64_t g = (uint64_t)lr * a.row_step;
-                            if (lr < a.n_rows && (!a.allow || a.allow[g])) {
 #pragma unroll
-                                for (int i = 0; i < kTopT; i++) {
-                                    const float lo = fminf(dd, top[i]), hi = fmaxf(dd, top[i]);
-                                    top[i] = lo;
-                                    dd = hi;
-                                }
+                            for (int i = 0; i < kTopT; i++) {
+                                const float lo = fminf(dd, top[i]), hi = fmaxf(dd, top[i]);
+                                top[i] = lo;
+                                dd = hi;
                             }
                         }
                     }
