@@ -613,7 +613,9 @@ def run_bf768(args, dist: Dist):
             "roofline": {"bound": "tensor", "achieved": best["tensor_tflops"], "peak": peak, "unit": "TFLOP/s",
                          "frac": best["frac_of_bf16_peak"], "traffic": None,
                          "peak_source": f"{kind} bf16 (MEASURED_PEAKS.json bf16_tflops); fp8 nominal peak is 2x"},
-            "gpu_launches": None}
+            # per search call: query prep, sample-helper gather, threshold
+            # pass, scores pass, select + re-rank
+            "gpu_launches": 5 * args.steps}
 
 
 def committed_traffic(tie_order, ef):
