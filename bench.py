@@ -83,9 +83,13 @@ def parse():
     ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
     ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
     ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
-    ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768"],
+    ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768", "serve768"],
                     help="gmm1m128: the HNSW headline (default); bf768: tensor-core brute force, 1M x 768 IP, "
-                         "k=100, over-fetch 400, recall against float64 exact top-k")
+                         "k=100, over-fetch 400, recall against float64 exact top-k; serve768: serving mix on a "
+                         "1M x 768 IP HNSW index (5%% deleted, 30%% filtered, k in {1,10,100}, ef in 32..512, "
+                         "learned stop, Poisson arrivals)")
+    ap.add_argument("--serve-rates-mix", type=int, nargs="*", default=[5_000, 50_000, 200_000],
+                    help="serve768: Poisson arrival rates (requests/s)")
     ap.add_argument("--serve-rates", type=int, nargs="*", default=[200_000, 1_000_000],
                     help="Poisson arrival rates (requests/s) of the serving-latency measurement")
     return ap.parse_args()
@@ -618,6 +622,91 @@ def run_bf768(args, dist: Dist):
             "gpu_launches": 5 * args.steps}
 
 
+def ensure_index_ip768(x, dist):
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"unit_{x.shape[0]}_768_ip_M16_efc200.bin")
+    if dist.rank == 0 and not os.path.exists(path):
+        hnswlib = ref_module()
+        t = time.time()
+        p = hnswlib.Index("ip", 768)
+        p.init_index(x.shape[0], M=16, ef_construction=200, random_seed=100)
+        p.add_items(x, num_threads=os.cpu_count())
+        p.save_index(path + ".tmp")
+        os.replace(path + ".tmp", path)
+        print(f"[bench] built reference index in {time.time() - t:.1f}s -> {path}", file=sys.stderr)
+    dist.barrier()
+    return path
+
+
+def run_serve768(args, dist: Dist):
+    """Serving mix (continuous batching) on a reference-built HNSW index over
+    1,000,000 x 768 unit vectors (inner product, M=16, ef_construction=200):
+    5 % of labels deleted, 30 % of requests with a label-parity filter, k
+    uniform over {1, 10, 100}, ef over {32, 64, 128, 256, 512}, learned
+    termination enabled; Poisson arrivals; latency = submission to results
+    on the host; recall@k against the exact scan of the admissible rows."""
+    import torch
+
+    from hnsw_rabitq_b200 import Index, learned
+    from hnsw_rabitq_b200.datasets import gmm_unit_ip
+    from hnsw_rabitq_b200.serving import Server, poisson_arrivals
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    n = args.n
+    x, q = gmm_unit_ip(n=n, nq=args.nq, dim=768)
+    path = ensure_index_ip768(x, dist)
+    del x
+    idx = Index("ip", 768)
+    idx.device = dev
+    idx.load_index(path)
+    rng = np.random.default_rng(5)
+    for lab in rng.choice(n, n // 20, replace=False):
+        idx.mark_deleted(int(lab))
+    # learned termination for the general (delete / filter aware) beam
+    _, tq = gmm_unit_ip(n=0, nq=8000, dim=768, query_seed=1000)
+    t0 = time.perf_counter()
+    model, rep = learned.fit(idx, tq, k=10, ef_cap=128, period=4, target_recall=0.95, precision="fp32",
+                             epochs=20, seed=0, caps=[128])
+    fit_s = time.perf_counter() - t0
+    idx.set_termination_model(model)
+    # the request mix and its ground truth
+    nq = q.shape[0]
+    ks = rng.choice([1, 10, 100], nq)
+    efs = rng.choice([32, 64, 128, 256, 512], nq)
+    filt = rng.random(nq) < 0.3
+    gt = np.empty((nq, 100), np.uint64)
+    gt[~filt] = idx.knn_query_exact(q[~filt], 100)[0]
+    gt[filt] = idx.knn_query_exact(q[filt], 100, filter=lambda l: l % 2 == 0)[0]
+    lines = []
+    with Server(idx) as srv:
+        parity = srv.add_filter(lambda l: l % 2 == 0)
+        reqs = [Server.request(k=int(ks[i]), ef=int(efs[i]), filter=parity if filt[i] else -1, learned=True)
+                for i in range(nq)]
+        srv.replay(q[:2000], reqs[:2000], poisson_arrivals(2000, 50_000, seed=3))  # warm-up
+        for rate in args.serve_rates_mix:
+            srv.stats(reset=True)
+            t0 = time.perf_counter()
+            lab, _, cnt, lat = srv.replay(q, reqs, poisson_arrivals(nq, rate, seed=rate))
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            hits = [len(np.intersect1d(lab[i, :ks[i]], gt[i, :ks[i]])) / ks[i] for i in range(nq)]
+            lines.append({"arrival_rate_qps": rate, "served_qps": round(nq / wall, 1),
+                          "p50_us": round(float(np.percentile(lat, 50)), 1),
+                          "p99_us": round(float(np.percentile(lat, 99)), 1), "mean_batch": round(st["mean_batch"], 2),
+                          "recall@k": round(float(np.mean(hits)), 4)})
+    top = lines[-1]
+    return {"metric": "serving mix p99 latency (continuous batching, learned stop), 1M x 768 IP HNSW",
+            "value": top["p99_us"], "unit": "us", "n_gpus": dist.world, "steps": len(lines), "warmup": 1,
+            "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "gmm_unit_ip 1,000,000 x 768 inner product, reference-built HNSW M=16 efc=200; "
+                                   "5% of labels deleted; 10,000 requests: k in {1,10,100}, ef in {32..512}, "
+                                   "30% label-parity filter, learned termination (trained cap 128)",
+                       "termination": {"threshold": model.threshold, "samples": rep["samples"],
+                                       "fit_seconds": round(fit_s, 1)}},
+            "rates": lines, "gpu_launches": None}
+
+
 def committed_traffic(tie_order, ef):
     """DRAM bytes per launch of hnsw_search_kernel from the committed ncu
     summary (profiles/), for the same tie order and ef, or None."""
@@ -723,7 +812,8 @@ def main():
         return 0
     dist = Dist(args.gpus)
     try:
-        out = run_bf768(args, dist) if args.workload == "bf768" else run_ours(args, dist)
+        out = (run_bf768(args, dist) if args.workload == "bf768" else
+               run_serve768(args, dist) if args.workload == "serve768" else run_ours(args, dist))
     finally:
         dist.close()
     if out is not None and dist.rank == 0:

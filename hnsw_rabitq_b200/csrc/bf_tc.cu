@@ -519,6 +519,16 @@ __global__ void tc_gather_info_kernel(const float2* __restrict__ info, uint64_t 
     if (i < n_sample) out[i] = info[i * step];
 }
 
+// Row mask of an exact scan over an index with deleted elements: allowed by
+// the caller's mask (if any) and not deleted.
+__global__ void scan_mask_kernel(const uint32_t* __restrict__ deleted_bits, const uint8_t* __restrict__ allow,
+                                 uint64_t n, uint8_t* __restrict__ out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool del = (deleted_bits[i >> 5] >> (i & 31)) & 1u;
+    out[i] = (!del && (!allow || allow[i])) ? 1 : 0;
+}
+
 __global__ void tc_fill_kernel(float* p, uint64_t n, float v) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -784,6 +794,13 @@ cudaError_t launch_tc_gather_info(const float2* info, uint64_t n_sample, uint64_
                                   cudaStream_t st) {
     if (!n_sample) return cudaSuccess;
     tc_gather_info_kernel<<<(unsigned)((n_sample + 255) / 256), 256, 0, st>>>(info, n_sample, step, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scan_mask(const uint32_t* deleted_bits, const uint8_t* allow, uint64_t n, uint8_t* out,
+                             cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    scan_mask_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(deleted_bits, allow, n, out);
     return cudaGetLastError();
 }
 

@@ -54,6 +54,8 @@ cudaError_t launch_tc_rowinfo(const float* vecs, uint32_t count, uint32_t dim, u
 cudaError_t launch_tc_query_prep(const float* q, uint32_t nq, uint32_t dim, uint32_t normalize, uint32_t prec,
                                  uint32_t trow_bytes, float* qf, unsigned char* qt, float* qscale, cudaStream_t st);
 cudaError_t launch_tc_fill(float* p, uint64_t n, float v, cudaStream_t st);
+cudaError_t launch_scan_mask(const uint32_t* deleted_bits, const uint8_t* allow, uint64_t n, uint8_t* out,
+                             cudaStream_t st);
 cudaError_t launch_tc_gather_info(const float2* info, uint64_t n_sample, uint64_t step, float2* out,
                                   cudaStream_t st);
 cudaError_t launch_tc_select(const TcSelectArgs& a, int space, cudaStream_t st);

@@ -677,8 +677,12 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
                 uint32_t prec, uint32_t rerank, const TermCfg* term, bool scan) {
-    if (scan && !h->is_bf && h->num_deleted)
-        throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "HNSWGPU_EXACT_SCAN: the index has deleted elements");
+    if (scan && !h->is_bf && h->num_deleted) {
+        // deleted elements are never returned: fold them into the row mask
+        h->scan_mask.ensure(h->count);
+        cuda_check(hnswgpu::launch_scan_mask(h->deleted_bits.p, dallow, h->count, h->scan_mask.p, st), "mask launch");
+        dallow = h->scan_mask.p;
+    }
     if (h->is_bf && prec) {
         run_bf_tc(h, dq, nq, k, rerank, dallow, dl, dd, dc, dtrace, st, prec);
     } else if (h->is_bf || scan) {

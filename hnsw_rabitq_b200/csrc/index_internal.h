@@ -94,6 +94,7 @@ struct hnswgpu_index {
     DevBuf<uint32_t> tc_cnt, tc_idx;
     DevBuf<uint64_t> tc_buf;
     DevBuf<uint8_t> tc_flags;
+    DevBuf<uint8_t> scan_mask;         // exact scan over an index with deletions
     uint32_t term_period = 0;
     float term_logit = 0.f;
     std::mutex mu;

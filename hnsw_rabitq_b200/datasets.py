@@ -78,11 +78,13 @@ def _unit_rows(a: np.ndarray) -> np.ndarray:
 
 
 def gmm_unit_ip(n: int = 1_000_000, nq: int = 10_000, dim: int = 768, n_comp: int = 256,
-                noise: float = 0.3, seed: int = 0, chunk: int = 1 << 16):
+                noise: float = 0.3, seed: int = 0, chunk: int = 1 << 16, query_seed=None):
     """Unit vectors ``normalize(c + noise * g / sqrt(dim))`` around unit centres.
 
     ``noise`` is the expected norm of the perturbation (per-coordinate scale
-    ``noise / sqrt(dim)``), so the components stay distinguishable.
+    ``noise / sqrt(dim)``), so the components stay distinguishable.  Queries
+    come from ``default_rng(seed + 1)``, or from ``default_rng(query_seed)``
+    (another stream of the same mixture, e.g. training queries).
     """
     crng = np.random.default_rng(seed + 7)
     centres = _unit_rows(crng.standard_normal((n_comp, dim), dtype=np.float32))
@@ -97,12 +99,14 @@ def gmm_unit_ip(n: int = 1_000_000, nq: int = 10_000, dim: int = 768, n_comp: in
             out[s:e] = _unit_rows(v)
         return out
 
-    return draw(np.random.default_rng(seed), n), draw(np.random.default_rng(seed + 1), nq)
+    qs = seed + 1 if query_seed is None else query_seed
+    return draw(np.random.default_rng(seed), n), draw(np.random.default_rng(qs), nq)
 
 
 def gmm_lognormal_sigma(n: int = 10_000_000, nq: int = 10_000, dim: int = 96, n_comp: int = 4096,
-                        seed: int = 0, chunk: int = 1 << 18):
-    """N(0,1) centres with per-component sigma log-uniform in [0.05, 0.5]."""
+                        seed: int = 0, chunk: int = 1 << 18, query_seed=None):
+    """N(0,1) centres with per-component sigma log-uniform in [0.05, 0.5]
+    (queries: ``default_rng(seed + 1)`` or ``default_rng(query_seed)``)."""
     crng = np.random.default_rng(seed + 7)
     centres = crng.standard_normal((n_comp, dim), dtype=np.float32)
     sig = np.exp(crng.uniform(np.log(0.05), np.log(0.5), n_comp)).astype(np.float32)
@@ -115,4 +119,5 @@ def gmm_lognormal_sigma(n: int = 10_000_000, nq: int = 10_000, dim: int = 96, n_
             out[s:e] = centres[comp] + rng.standard_normal((e - s, dim), dtype=np.float32) * sig[comp, None]
         return out
 
-    return draw(np.random.default_rng(seed), n), draw(np.random.default_rng(seed + 1), nq)
+    qs = seed + 1 if query_seed is None else query_seed
+    return draw(np.random.default_rng(seed), n), draw(np.random.default_rng(qs), nq)

@@ -66,8 +66,8 @@ extern "C" {
 #define HNSWGPU_EXACT_SCAN 0x10u  /* HNSW: answer by an exhaustive scan of the
                                      index's resident vectors (exact k-NN,
                                      the ground truth of recall measurements;
-                                     the allow mask applies, deletes are not
-                                     supported).                               */
+                                     the allow mask applies and deleted
+                                     elements are never returned).             */
 
 /* kernel status bits (hnswgpu_search_opts.status / hnswgpu_get_status) */
 #define HNSWGPU_STATUS_TIMEOUT 0x1u   /* a bounded wait gave up; results invalid   */

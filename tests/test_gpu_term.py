@@ -199,3 +199,21 @@ def test_learned_stop_general_path(tmp_path):
     ll, ld, lc, lt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id", learned=True)
     assert np.all(lt[:, 2] <= period)
     assert all(flt(int(v)) and int(v) % 37 for i in range(300) for v in ll[i, :lc[i]])
+
+
+def test_exact_scan_skips_deleted(tmp_path):
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((6000, 32)).astype(np.float32)
+    q = rng.standard_normal((100, 32)).astype(np.float32)
+    build_hnsw(tmp_path / "d.bin", x, "l2", M=8, efc=60)
+    g = H.Index("l2", 32)
+    g.load_index(str(tmp_path / "d.bin"))
+    dead = set(range(0, 6000, 7))
+    for lab in dead:
+        g.mark_deleted(lab)
+    keep = np.array([i for i in range(6000) if i not in dead])
+    l, d = g.knn_query_exact(q, 10, filter=lambda v: v % 2 == 0)
+    sub = keep[keep % 2 == 0]
+    rl, rd = O.bf_matrix("l2", x[sub], q, 10)
+    assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))
+    assert not (set(l.ravel().tolist()) & dead)
