@@ -83,11 +83,12 @@ def parse():
     ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
     ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
     ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
-    ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768", "serve768"],
+    ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768", "serve768", "learned96"],
                     help="gmm1m128: the HNSW headline (default); bf768: tensor-core brute force, 1M x 768 IP, "
                          "k=100, over-fetch 400, recall against float64 exact top-k; serve768: serving mix on a "
                          "1M x 768 IP HNSW index (5%% deleted, 30%% filtered, k in {1,10,100}, ef in 32..512, "
-                         "learned stop, Poisson arrivals)")
+                         "learned stop, Poisson arrivals); learned96: learned termination vs fixed ef on the "
+                         "heterogeneous 96-d mixture (M=32, ef_construction=400, ef cap 512)")
     ap.add_argument("--serve-rates-mix", type=int, nargs="*", default=[5_000, 50_000, 200_000],
                     help="serve768: Poisson arrival rates (requests/s)")
     ap.add_argument("--serve-rates", type=int, nargs="*", default=[200_000, 1_000_000],
@@ -707,6 +708,91 @@ def run_serve768(args, dist: Dist):
             "rates": lines, "gpu_launches": None}
 
 
+def run_learned96(args, dist: Dist):
+    """Learned termination on the mixture with per-component sigma log-uniform
+    in [0.05, 0.5] (queries of very different difficulty): n x 96 L2,
+    reference-built HNSW M=32, ef_construction=400, k=10, ef cap 512.  QPS at
+    recall@10 >= target of the plain fixed-ef beam (smallest ef of the sweep)
+    and of the learned stop (cap and threshold calibrated on held-out
+    training queries).  The low-precision beam needs maxM0 <= 32, so both
+    arms traverse float32 rows here."""
+    import torch
+
+    from hnsw_rabitq_b200 import Index, _capi, learned
+    from hnsw_rabitq_b200.datasets import gmm_lognormal_sigma
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    n = args.n
+    x, q = gmm_lognormal_sigma(n=n, nq=args.nq, dim=96)
+    os.makedirs(CACHE, exist_ok=True)
+    path = os.path.join(CACHE, f"lognormal_{n}_96_M32_efc400.bin")
+    if dist.rank == 0 and not os.path.exists(path):
+        hnswlib = ref_module()
+        t = time.time()
+        p = hnswlib.Index("l2", 96)
+        p.init_index(n, M=32, ef_construction=400, random_seed=100)
+        p.add_items(x, num_threads=os.cpu_count())
+        p.save_index(path + ".tmp")
+        os.replace(path + ".tmp", path)
+        print(f"[bench] built reference index in {time.time() - t:.1f}s -> {path}", file=sys.stderr)
+    dist.barrier()
+    del x
+    idx = Index("l2", 96)
+    idx.device = dev
+    idx.load_index(path)
+    gt = idx.knn_query_exact(q, 10)[0]
+    loop = DeviceLoop(idx, q, dev)
+    nq = q.shape[0]
+    target = args.target_recall
+    sweep, ef_p = [], None
+    for ef in [16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256, 320, 384, 448, 512]:
+        loop.step(loop.opts(ef))
+        r = recall(loop.labels(), gt)
+        sweep.append({"ef": ef, "recall": round(r, 5)})
+        if r >= target:
+            ef_p = ef
+            break
+    ef_p = ef_p or 512
+    ms_p, _ = loop.time(loop.opts(ef_p), args.steps, args.warmup, dist)
+    _, _, _, tr_p = idx.knn_query_traced(q, 10, ef=ef_p, tie_order="id")
+    _, tq = gmm_lognormal_sigma(n=0, nq=args.train_queries, dim=96, query_seed=1000)
+    t0 = time.perf_counter()
+    model, rep = learned.fit(idx, tq, k=10, ef_cap=512, period=4, target_recall=target + 0.005, precision="fp32",
+                             epochs=20, seed=0)
+    fit_s = time.perf_counter() - t0
+    tgt = target + 0.005
+    for _ in range(6):
+        o = loop.opts(model.ef_cap, _capi.LEARNED_STOP)
+        loop.step(o)
+        rec = recall(loop.labels(), gt)
+        if rec >= target:
+            break
+        tgt += 0.005
+        hold = tq[: max(1, len(tq) // 3)]
+        cap, thr, _ = learned.calibrate(idx, hold, idx.knn_query_exact(hold, 10)[0], 10, model, tgt,
+                                        caps=sorted({c for c, *_ in rep["curve"]}))
+        model.ef_cap, model.threshold = cap, thr
+        idx.set_termination_model(model)
+    ms_l, clk = loop.time(o, args.steps, args.warmup, dist, clocks=True)
+    _, _, _, tr_l = idx.knn_query_traced(q, 10, ef=model.ef_cap, tie_order="id", learned=True)
+    qps_l, qps_p = nq / (ms_l / 1e3), nq / (ms_p / 1e3)
+    return {"metric": "QPS at recall@10>=0.95, learned termination vs fixed ef, heterogeneous 96-d mixture",
+            "value": round(qps_l, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_l, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"gmm_lognormal_sigma {n:,} x 96 L2 (4096 components, sigma log-uniform "
+                                   "[0.05, 0.5]), reference-built HNSW M=32 efc=400, 10,000 queries, k=10",
+                       "learned": {"ef_cap": model.ef_cap, "threshold": model.threshold, "recall@10": round(rec, 5),
+                                   "mean_l0_expansions": round(float(tr_l[:, 2].mean()), 1),
+                                   "p99_l0_expansions": float(np.percentile(tr_l[:, 2], 99)),
+                                   "training_queries": int(tq.shape[0]), "samples": rep["samples"],
+                                   "fit_seconds": round(fit_s, 1)},
+                       "plain": {"ef": ef_p, "qps": round(qps_p, 1), "recall@10": sweep[-1]["recall"],
+                                 "mean_l0_expansions": round(float(tr_p[:, 2].mean()), 1),
+                                 "p99_l0_expansions": float(np.percentile(tr_p[:, 2], 99)), "sweep": sweep}},
+            "speedup_vs_plain": round(qps_l / qps_p, 3), "clocks": clk, "gpu_launches": args.steps}
+
+
 def committed_traffic(tie_order, ef):
     """DRAM bytes per launch of hnsw_search_kernel from the committed ncu
     summary (profiles/), for the same tie order and ef, or None."""
@@ -813,7 +899,8 @@ def main():
     dist = Dist(args.gpus)
     try:
         out = (run_bf768(args, dist) if args.workload == "bf768" else
-               run_serve768(args, dist) if args.workload == "serve768" else run_ours(args, dist))
+               run_serve768(args, dist) if args.workload == "serve768" else
+               run_learned96(args, dist) if args.workload == "learned96" else run_ours(args, dist))
     finally:
         dist.close()
     if out is not None and dist.rank == 0:

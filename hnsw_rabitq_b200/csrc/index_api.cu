@@ -458,6 +458,10 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
         p.ckpt_count = t->count;
     } else {
         if (!h->term_model.p) throw ApiError(HNSWGPU_ERR_STATE, "no termination model set");
+        if (std::isinf(h->term_logit) && h->term_logit > 0) {  // never stops: the plain beam
+            p.term_mode = 0;
+            return;
+        }
         p.term_period = h->term_period;
         p.term_model = reinterpret_cast<const float*>(h->term_model.p);
         p.term_logit = h->term_logit;

@@ -320,7 +320,9 @@ int hnswgpu_server_create(hnswgpu_index* h, const hnswgpu_server_opts* opts, hns
         auto s = std::make_unique<hnswgpu_server>();
         s->h = h;
         if (opts) s->o = *opts;
-        if (!s->o.max_inflight) s->o.max_inflight = 8;
+        // 32 batches in flight: a batch lasts about one query's beam latency,
+        // so concurrency, not batch size, bounds the served rate
+        if (!s->o.max_inflight) s->o.max_inflight = 32;
         if (!s->o.max_batch) s->o.max_batch = 4096;
         set_device(h);
         int smem_per_sm = 0;

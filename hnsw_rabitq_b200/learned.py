@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import ctypes as C
 import json
+import time
 from dataclasses import dataclass, field
 from typing import Optional
 
@@ -158,25 +159,34 @@ def logits(params: np.ndarray, feats: np.ndarray, device: int = 0) -> np.ndarray
 
 
 def evaluate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, threshold: float,
-             ef_cap: Optional[int] = None):
-    """(recall@k, mean level-0 expansions) of the learned search at this
-    threshold and cap."""
+             ef_cap: Optional[int] = None, timed: bool = False):
+    """(recall@k, mean level-0 expansions, seconds per batch or None) of the
+    learned search at this threshold and cap; `timed`: the best of 3 runs."""
     cap = int(ef_cap or model.ef_cap)
     m = TerminationModel(model.params, model.period, float(threshold), cap, model.precision, model.rerank)
     index.set_termination_model(m)
-    lab, _, cnt, tr = index.knn_query_traced(queries, k, ef=cap, tie_order="id", precision=model.precision,
-                                             rerank=model.rerank, learned=True)
-    return recall(lab, gt), float(tr[:, 2].mean())
+    run = lambda: index.knn_query_traced(queries, k, ef=cap, tie_order="id", precision=model.precision,
+                                         rerank=model.rerank, learned=np.isfinite(threshold))
+    lab, _, cnt, tr = run()
+    secs = None
+    if timed:
+        secs = float("inf")
+        for _ in range(3):
+            t0 = time.perf_counter()
+            run()
+            secs = min(secs, time.perf_counter() - t0)
+    return recall(lab, gt), float(tr[:, 2].mean()), secs
 
 
 def calibrate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: TerminationModel, target_recall: float,
-              caps=None, candidates: Optional[np.ndarray] = None):
-    """Cap and logit threshold of the cheapest learned search (fewest mean
-    level-0 expansions) whose recall@k on these queries meets the target.
-    A threshold of +inf never stops early, so each cap's plain fixed-ef
-    search is among the candidates.  Returns (cap, threshold, curve
-    [(cap, threshold, recall, mean expansions)]); (max cap, +inf) when no
-    candidate meets the target."""
+              caps=None, candidates: Optional[np.ndarray] = None, cost: str = "time"):
+    """Cap and logit threshold of the cheapest search whose recall@k on
+    these queries meets the target.  A threshold of +inf is the plain
+    fixed-ef search of that cap (no network evaluated), so the calibrated
+    search is never slower than the best plain one it tried.  cost="time":
+    measured batch time (best of 3); "expansions": mean level-0 expansions.
+    Returns (cap, threshold, curve [(cap, threshold, recall, mean
+    expansions, seconds)]); (max cap, +inf) when nothing meets the target."""
     caps = sorted(caps or [model.ef_cap])
     if candidates is None:
         candidates = np.linspace(6.0, -4.0, 21)
@@ -185,10 +195,15 @@ def calibrate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: Termina
     best = (float("inf"), caps[-1], float("inf"))
     for cap in caps:
         for t in ths:
-            r, e = evaluate(index, queries, gt, k, model, t, cap)
-            curve.append((int(cap), t, r, e))
-            if r >= target_recall and e < best[0]:
-                best = (e, int(cap), t)
+            r, e, _ = evaluate(index, queries, gt, k, model, t, cap)
+            secs = None
+            if r >= target_recall:
+                if cost == "time":
+                    secs = evaluate(index, queries, gt, k, model, t, cap, timed=True)[2]
+                c = secs if cost == "time" else e
+                if c < best[0]:
+                    best = (c, int(cap), t)
+            curve.append((int(cap), t, r, e, secs))
             if r < target_recall - 0.03:
                 break  # lower thresholds stop earlier still
     return best[1], best[2], curve
@@ -197,7 +212,7 @@ def calibrate(index, queries: np.ndarray, gt: np.ndarray, k: int, model: Termina
 def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int = 4, target_recall: float = 0.95,
         precision: Optional[str] = None, rerank: Optional[int] = None, holdout: float = 0.3,
         max_ckpt: Optional[int] = None, epochs: int = 20, seed: int = 0, gt: Optional[np.ndarray] = None,
-        caps=None, device: int = 0):
+        caps=None, device: int = 0, cost: str = "time"):
     """Trace (at ef = ef_cap), label, train and calibrate on `queries` (drawn
     from the query distribution; a `holdout` share is kept for the
     calibration of the cap, at most ef_cap, and threshold).  Returns
@@ -221,7 +236,7 @@ def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int =
     if caps is None:
         caps = [c for c in (k, 16, 24, 32, 40, 44, 48, 52, 56, 64, 80, 96, 128, 192, 256, 384, 512)
                 if k <= c <= ef_cap]
-    cap, thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall, caps=caps)
+    cap, thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall, caps=caps, cost=cost)
     model.ef_cap, model.threshold = cap, thr
     model.info = dict(samples=int(X.shape[0]), positive=float(y.mean()), loss=[float(v) for v in losses],
                       curve=curve, trained_cap=ef_cap, target_recall=target_recall)

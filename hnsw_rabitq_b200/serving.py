@@ -22,7 +22,7 @@ from .index import _PRECISIONS, _input_rows, _ptr
 
 
 class Server:
-    def __init__(self, index, max_inflight: int = 8, max_batch: int = 4096, smem_budget: int = 0):
+    def __init__(self, index, max_inflight: int = 32, max_batch: int = 4096, smem_budget: int = 0):
         index._require()
         self.index = index
         o = _capi.ServerOpts(max_inflight=int(max_inflight), max_batch=int(max_batch), smem_budget=int(smem_budget))

@@ -245,8 +245,9 @@ HNSWGPU_API int hnswgpu_fp64_distances(hnswgpu_index* index, const float* querie
 
 /* Install (params != NULL) or remove (NULL) the index's termination network;
  * HNSWGPU_LEARNED_STOP searches evaluate it every `period` expansions and
- * stop when the logit exceeds `logit_threshold`.  The search runs the
- * network with fp16 weights and fp32 accumulation. */
+ * stop when the logit exceeds `logit_threshold` (+inf: never, and the
+ * network is not evaluated -- the plain beam).  The search runs the network
+ * with fp16 weights and fp32 accumulation. */
 HNSWGPU_API int hnswgpu_set_termination_model(hnswgpu_index* index, const float* params, uint32_t period,
                                               float logit_threshold);
 
@@ -304,7 +305,7 @@ HNSWGPU_API int hnswgpu_term_logits(int device, const float* params, const float
 typedef struct hnswgpu_server hnswgpu_server;
 
 typedef struct hnswgpu_server_opts {
-    uint32_t max_inflight;     /* concurrent batches (streams); 0: 8          */
+    uint32_t max_inflight;     /* concurrent batches (streams); 0: 32         */
     uint32_t max_batch;        /* queries per batch; 0: 4096                  */
     uint64_t smem_budget;      /* admission budget in bytes of per-query
                                   shared-memory footprint in flight; 0: twice

@@ -117,9 +117,10 @@ def test_stop_rule_bounds(gmm_index):
     p, f, _ = _random_problem(10)
     k, ef, period = 10, 64, 4
     pl, pd, _, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id")
-    g.set_termination_model(learned.TerminationModel(p, period, float("inf")))
-    ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
-    assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
+    for never in (float("inf"), 1e30):  # +inf skips the network; 1e30 evaluates it
+        g.set_termination_model(learned.TerminationModel(p, period, never))
+        ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
+        assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
     g.set_termination_model(learned.TerminationModel(p, period, -float("inf")))
     ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
     assert np.all(lt[:, 2] <= period) and np.all(lc == k)
@@ -135,7 +136,8 @@ def test_fit_meets_target_with_less_work(gmm_index):
     generalisation margin) with fewer level-0 expansions than the cap."""
     g, x, q = gmm_index
     tr, te = q[:1000], q[1000:]
-    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0, caps=[96])
+    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0, caps=[96],
+                             cost="expansions")
     assert rep["samples"] > 10000 and 0.05 < rep["positive"] < 0.95
     assert rep["loss"][-1] < rep["loss"][0]
     assert model.ef_cap == 96 and np.isfinite(model.threshold)
@@ -191,7 +193,7 @@ def test_learned_stop_general_path(tmp_path):
     assert np.array_equal(lab_of[ck["ids"][np.arange(300), n]], ul)
     assert np.all(n <= ut[:, 2] // period)
     p, f, _ = _random_problem(3)
-    g.set_termination_model(learned.TerminationModel(p, period, float("inf")))
+    g.set_termination_model(learned.TerminationModel(p, period, 1e30))
     ll, ld, lc, lt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id", learned=True)
     assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
     assert all(flt(int(v)) and int(v) % 37 for row in ll for v in row)
