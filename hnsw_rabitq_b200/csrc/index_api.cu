@@ -466,6 +466,14 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
         p.term_model = reinterpret_cast<const float*>(h->term_model.p);
         p.term_logit = h->term_logit;
     }
+    // A learned stop usually ends a query long before a large cap: size the
+    // visited cache for that (at most 2^11 entries; a miss only repeats a
+    // distance, results do not depend on it) so that a large cap does not
+    // cost occupancy.
+    if (p.log2_vis > 11) {
+        p.log2_vis = 11;
+        hnswgpu::warp_smem_layout(p);
+    }
 }
 
 // One HNSW search launch on device buffers, scratch from the index.
