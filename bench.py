@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--target-recall", type=float, default=0.95)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", action="store_true", help="only run the timed loop (for ncu)")
+    ap.add_argument("--profile-precision", default="fp32", choices=["fp32", "bf16", "fp8"],
+                    help="traversal precision of --profile-steps")
     ap.add_argument("--profile-learned", type=float, default=None, metavar="LOGIT",
                     help="train the termination network, then only run the learned + FP8 loop with this logit "
                          "threshold at ef = --term-cap (for ncu; no calibration sweep)")
@@ -404,8 +406,9 @@ def run_ours(args, dist: Dist):
     if args.profile_steps:
         if not args.ef:
             raise SystemExit("--profile-steps needs --ef")
-        tie = _capi.EXACT_TIES if args.tie_order == "reference" else 0
-        loop.time(loop.opts(args.ef, tie), args.steps, args.warmup, dist)
+        prec = {"fp32": 0, "bf16": 1, "fp8": 2}[args.profile_precision]
+        tie = _capi.EXACT_TIES if args.tie_order == "reference" and prec == 0 else 0
+        loop.time(loop.opts(args.ef, tie, prec), args.steps, args.warmup, dist)
         return None
 
     # ---- plain FP32 beam (the comparison), both tie orders
@@ -459,11 +462,15 @@ def run_ours(args, dist: Dist):
               + trace[:, 3] * fp8_row).mean() + min(rr, model.ef_cap) * 512
         achieved = bq * nq / (ms_step / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": committed_traffic("learned_fp8", model.ef_cap),
+                "frac": round(achieved / peak, 4),
+                # with threshold +inf the calibrated search is the plain fp8 beam
+                "traffic": committed_traffic("learned_fp8" if np.isfinite(model.threshold) else "fp8",
+                                             model.ef_cap),
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_query": round(float(bq), 1),
-                "kernel": "hnsw_search_kernel<L2, fp8 traversal, learned stop>"}
+                "kernel": "hnsw_search_kernel<L2, fp8 traversal, " +
+                          ("learned stop>" if np.isfinite(model.threshold) else "fixed ef (calibrated: no stop)>")}
         cpu, bytes_q = (cpu_baseline(args, path, q, plain["id"]["ef"], info) if not args.no_cpu_baseline
                         else (None, None))
         if bytes_q:

@@ -1205,7 +1205,8 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
 }
 
 template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, kMinBlocks) hnsw_search_kernel(SearchParams p) {
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP : kMinBlocks)
+    hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* base = smem + (size_t)warp * p.warp_smem;
