@@ -125,3 +125,50 @@ def test_datasets_deterministic_and_shaped():
     assert np.allclose(np.linalg.norm(x, axis=1), 1, atol=1e-5)
     x, q = D.gmm_lognormal_sigma(n=1000, nq=10)
     assert x.shape == (1000, 96)
+
+
+def test_newer_entry_points_reject_bad_arguments():
+    """Argument checks that run before any device work (no GPU needed)."""
+    lib = _capi.lib()
+    u64 = C.c_uint64()
+    # learned termination
+    assert lib.hnswgpu_set_termination_model(None, None, 4, C.c_float(0.0)) == _capi.ERR_ARG
+    opts = _capi.SearchOpts()
+    assert lib.hnswgpu_search_checkpoints(None, None, 1, 10, C.byref(opts), 4, 8, None, None, None, None, None,
+                                          None) == _capi.ERR_ARG
+    to = _capi.TermTrainOpts(epochs=1, batch=16, lr=1e-3, pos_weight=1.0, weight_decay=0.0, reserved=0, seed=0)
+    assert lib.hnswgpu_term_train(0, None, None, 0, C.byref(to), None, None) == _capi.ERR_ARG
+    assert lib.hnswgpu_term_loss_grad(0, None, None, None, 0, C.c_float(1.0), None, None) == _capi.ERR_ARG
+    assert lib.hnswgpu_term_logits(0, None, None, 3, None) == _capi.ERR_ARG
+    # float64 oracle, serving loop
+    assert lib.hnswgpu_fp64_distances(None, None, 1, None, 1, None) == _capi.ERR_ARG
+    srv = C.c_void_p()
+    assert lib.hnswgpu_server_create(None, None, C.byref(srv)) == _capi.ERR_ARG
+    req = _capi.Request(k=10, ef=0, filter=-1, flags=0, precision=0, rerank=0)
+    assert lib.hnswgpu_server_submit(None, None, C.byref(req), C.byref(u64)) == _capi.ERR_ARG
+    assert lib.hnswgpu_server_wait(None, 1, None, None, None, None) == _capi.ERR_ARG
+    st = _capi.ServerStats()
+    assert lib.hnswgpu_server_get_stats(None, C.byref(st), 0) == _capi.ERR_ARG
+    assert lib.hnswgpu_server_destroy(None) == _capi.ERR_ARG
+    assert lib.hnswgpu_build_traversal_copy(None, 2) == _capi.ERR_ARG
+    assert lib.hnswgpu_last_error() != b""
+
+
+def test_termination_model_file_round_trip(tmp_path):
+    from hnsw_rabitq_b200 import learned
+    rng = np.random.default_rng(0)
+    m = learned.TerminationModel(learned.init_params(rng.normal(size=(50, 6)), 1), 8, 1.25, 96, "fp8", 40,
+                                 {"note": "x"})
+    m.save(str(tmp_path / "t.npz"))
+    r = learned.TerminationModel.load(str(tmp_path / "t.npz"))
+    assert np.array_equal(r.params, m.params)
+    assert (r.period, r.threshold, r.ef_cap, r.precision, r.rerank, r.info) == (8, 1.25, 96, "fp8", 40, {"note": "x"})
+
+
+def test_serving_helpers():
+    from hnsw_rabitq_b200.serving import Server, poisson_arrivals
+    a = poisson_arrivals(20000, 100_000, seed=1)
+    assert np.all(np.diff(a) > 0) and abs(a[-1] / 20000 - 10.0) < 0.5  # mean gap 10 us
+    r = Server.request(k=5, ef=64, filter=2, tie_order="reference", precision="bf16", rerank=7)
+    assert (r.k, r.ef, r.filter, r.flags, r.precision, r.rerank) == (5, 64, 2, _capi.EXACT_TIES, _capi.PREC_BF16, 7)
+    assert Server.request(learned=True).flags == _capi.LEARNED_STOP
