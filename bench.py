@@ -421,6 +421,15 @@ def run_ours(args, dist: Dist):
         ms_p, _ = loop.time(o, args.steps, args.warmup, dist)
         plain[order] = {"ef": ef_p, "recall@10": round(recall(lab_p, gt), 5), "ms_per_step": round(ms_p, 4),
                         "qps": round(dist.world * nq / (ms_p / 1e3), 1), "sweep": sw}
+        if order == "reference":
+            # the same results by the one-pass heap replay of every query (the
+            # default replays only the queries whose id-order run met a tie)
+            o = loop.opts(ef_p, fl_p | _capi.REPLAY_ALL)
+            loop.step(o)
+            same = bool(np.array_equal(loop.labels(), lab_p))
+            ms_r, _ = loop.time(o, args.steps, args.warmup, dist)
+            plain[order]["replay_all"] = {"ms_per_step": round(ms_r, 4), "qps": round(dist.world * nq / (ms_r / 1e3), 1),
+                                          "same_labels": same}
 
     # ---- learned termination + FP8 traversal + FP32 re-rank (the headline)
     model, rep, tq, fit_s = train_termination(idx, args)

@@ -21,6 +21,7 @@ TRACE = 0x2
 EXACT_TIES = 0x4
 LEARNED_STOP = 0x8
 EXACT_SCAN = 0x10
+REPLAY_ALL = 0x20
 TERM_FEATURES = 6
 TERM_HIDDEN = 64
 TERM_PARAMS = 4685

@@ -195,6 +195,20 @@ __device__ __forceinline__ int find_unexpanded(const uint64_t* a, int n, int& hi
     return -1;
 }
 
+// Unexpanded entries of the sorted array a[from, n) whose distance key is dk,
+// where a[from] is the first unexpanded entry (so all such entries follow it).
+__device__ __forceinline__ int unexpanded_with_dist(const uint64_t* a, int n, int from, uint32_t dk, int lane) {
+    int c = 0;
+    for (int b = from; b < n; b += 32) {
+        const int i = b + lane;
+        const uint64_t e = i < n ? a[i] : ~0ull;
+        const bool same = i < n && khi(e) == dk;
+        c += __popc(__ballot_sync(FULL, same && !((uint32_t)e & EXP_BIT)));
+        if (!__shfl_sync(FULL, same, 31)) break;
+    }
+    return c;
+}
+
 // Insert the keys held by the lanes of `amask` (distinct, not present in the
 // array; `pos` = lower_bound_key of the lane's key) into the sorted array a[0,
 // size), keeping at most cap entries.  Returns the smallest insertion index.
@@ -611,7 +625,15 @@ __device__ __forceinline__ void term_final_row(const SearchParams& p, const Warp
     if (lane == 0) p.ckpt_count[qi] = r + 1;
 }
 
-template <int SPACE, bool EXACT, int PREC, int TERM>
+// TIES (id order only): flag the query (status kTieBit) when its run meets a
+// distance tie that can make the reference's heaps decide differently from the
+// (distance, id) order.  With acceptance by counting (independent of heap
+// layout), the two runs agree step by step unless (a) the candidate popped next
+// shares its distance with another unexpanded candidate, or (b) the entries
+// dropped from the full pool tie with its new worst entry (an evicted entry that
+// stays in candidate_set at lowerBound would still be expanded); (c), the
+// top-k boundary tie, is checked by the caller.
+template <int SPACE, bool EXACT, int PREC, int TERM, bool TIES = false>
 __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
                                PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
                                uint32_t& status, uint32_t qi, float qn) {
@@ -675,6 +697,11 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             if (kp != ~0ull || kmin != ~0ull) {
                 have_next = true;
                 next_dk = khi(kmin < kp ? kmin : kp);
+                if (TIES) {  // (a): candidate_set's top must be unique by distance
+                    int same = __popc(__ballot_sync(FULL, accept && dk == next_dk));
+                    if (ip >= 0) same += unexpanded_with_dist(s.pool, psize, ip, next_dk, lane);
+                    if (same > 1) status |= kTieBit;
+                }
                 if (kmin < kp) {
                     next = (uint32_t)kmin;
                     if (accept && key == kmin) key |= EXP_BIT;  // inserted already expanded
@@ -733,6 +760,12 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         if (pmask) {
             const int m = merge_sorted(s.pool, psize, pcap, pmask, key, posP, lane);
             hint_p = min(hint_p, m);
+            if (TIES && psize > ef) {
+                // (b): the merge kept one entry more than ef (pool_cap is
+                // ef + 1): the first one dropped, next to the new worst
+                if (khi(s.pool[ef]) == khi(s.pool[ef - 1])) status |= kTieBit;
+                psize = ef;
+            }
         }
         if (EXACT && nev) remove_keys(s.pool, psize, s.evbuf, nev, lane);
         if (!EXACT) {
@@ -743,6 +776,15 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             if (nx >= 0 && lane == 0) prefetch_l2(p.links0 + (size_t)kid(s.pool[nx]) * p.maxM0);
         }
         PT_MARK(8);
+        if (TIES && (status & kTieBit)) {
+            // listed for the heap replay, which recomputes the whole query:
+            // drain the prefetched expansion and stop here
+            if (have_next && fn.n0 > 0) {
+                mbar_wait(s.bar, phase);
+                phase ^= 1u;
+            }
+            break;
+        }
         if (TERM && have_next && ct.l0_exp % p.term_period == 0 &&
             term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d0, qn, ts)) {
             // confident that the top-k is final: drain the prefetched
@@ -849,7 +891,7 @@ __device__ bool rerank_fp32(const SearchParams& p, WarpSmem& s, uint32_t& phase,
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES = false>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
                            Counters& ct, PhaseClock& pc) {
     pc.start();
@@ -916,7 +958,9 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     // (hnswalg.h:336-337) and never evaluated, so the exact-key lookup cannot
     // recognise it when the visited cache misses on it later: skip it by id.
     uint32_t skip_id = INVALID_ID;
-    const int pcap = (int)p.pool_cap;  // ef, or ef + 32 in tie-exact mode
+    // ef, or ef + 32 in tie-exact mode (ef + 1 in a tie-listing pass, for
+    // the pipelined beam only)
+    const int pcap = TIES ? (int)ef : (int)p.pool_cap;
     int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
     const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
     const bool pipe = FAST16 && bare && p.maxM0 <= 32;
@@ -949,11 +993,14 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
 #pragma unroll
         for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
-        if (!base_pipelined<SPACE, EXACT, PREC, TERM>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz, status,
-                                                      qi, qn))
+        if (!base_pipelined<SPACE, EXACT, PREC, TERM, TIES>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz,
+                                                            status, qi, qn))
             return false;
+        // (c): the reference pops top_candidates down to k by distance
+        if (TIES && psize > (int)p.k && khi(s.pool[p.k - 1]) == khi(s.pool[p.k])) status |= kTieBit;
         if (PREC != 0 && !rerank_fp32<SPACE>(p, s, phase, lane, qr, psize)) return false;
     } else {
+    if (TIES) status |= kTieBit;  // only the pipelined beam checks its ties
     if (bare || is_allowed(p, cur)) {
         float d0;
         if (!lane_distances<SPACE, FAST16>(p, s, phase, cur, 1, lane, d0, pc)) return false;
@@ -1196,6 +1243,8 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         olab[r] = ~0ull;
         odist[r] = __int_as_float(0x7f800000);
     }
+    if (TIES && (status & kTieBit) && lane == 0) p.tie_list[atomicAdd(p.tie_count, 1u)] = qi;
+    status &= ~kTieBit;
     if (lane == 0) {
         p.out_counts[qi] = kk;
         if (status) atomicOr(p.status, status);
@@ -1204,7 +1253,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP : kMinBlocks)
     hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -1232,13 +1281,19 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP 
     __syncwarp();
     uint32_t phase = 0;
     PhaseClock pc;
+    // a list pass runs the queries a previous launch on this stream listed
+    const uint32_t nrun = p.qcount ? min(*p.qcount, p.nq) : p.nq;
     while (true) {
         uint32_t qi = 0;
-        if (lane == 0) qi = atomicAdd(p.work_counter, 1u);
+        if (lane == 0) {
+            qi = atomicAdd(p.work_counter, 1u);
+            if (p.qlist && qi < nrun) qi = p.qlist[qi];
+            else if (qi >= nrun) qi = 0xffffffffu;
+        }
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE, FAST16, EXACT, PREC, TERM>(p, s, phase, qi, lane, ct, pc)) {
+        if (!search_one<SPACE, FAST16, EXACT, PREC, TERM, TIES>(p, s, phase, qi, lane, ct, pc)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
@@ -1304,13 +1359,13 @@ size_t warp_smem_layout(SearchParams& p) {
 }
 
 namespace {
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0, bool TIES = false>
 cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
     // per-instantiation cache of the opt-in shared-memory size and occupancy
     static int attr_smem = -1;
     static size_t occ_smem = 0;
     static int occ_per_sm = 0;
-    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM>;
+    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES>;
     const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
     if ((int)smem > attr_smem) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1328,7 +1383,7 @@ cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, in
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -1393,6 +1448,15 @@ cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
 }
 
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (p.tie_list) {
+        // id-order beam that lists its tie-steered queries (float32, 4-lane
+        // distances, no filter: checked by the host)
+        if (p.exact || p.prec || p.term_mode || !p.fast16 || !p.bare || p.maxM0 > 32 || p.pool_cap != p.ef + 1 ||
+            !p.tie_count)
+            return cudaErrorInvalidValue;
+        return space == 0 ? launch_t<0, true, false, 0, 0, true>(p, num_sms, stream, blocks_out)
+                          : launch_t<1, true, false, 0, 0, true>(p, num_sms, stream, blocks_out);
+    }
     if (p.term_mode) return space == 0 ? launch_term<0>(p, num_sms, stream, blocks_out)
                                        : launch_term<1>(p, num_sms, stream, blocks_out);
     if (p.prec) return space == 0 ? launch_lowp<0>(p, num_sms, stream, blocks_out)

@@ -59,6 +59,7 @@ cudaError_t term_logits(const float* params, const float* feats, uint64_t n, flo
 constexpr int kMinBlocks = HNSWGPU_MINB;     // launch bound: resident CTAs per SM
 constexpr uint32_t HNSWGPU_STATUS_TIMEOUT_BIT = 0x1u;
 constexpr uint32_t HNSWGPU_STATUS_OVERFLOW_BIT = 0x2u;
+constexpr uint32_t kTieBit = 0x80000000u;  // per-query, never reported: the run met a steering tie
 
 struct SearchParams {
     // index (device pointers)
@@ -93,6 +94,13 @@ struct SearchParams {
     uint32_t* work_counter;       // zero at launch; reset to zero by the last block
     uint32_t* done_counter;       // blocks finished (same slot discipline)
     uint32_t* status;
+    // tie-exact mode in two passes: the id-order beam lists the queries whose
+    // run met a distance tie that can steer the reference's heaps, then the
+    // heap replay runs on those queries only
+    uint32_t* tie_list;           // first pass: flagged query indices (null: no listing)
+    uint32_t* tie_count;          // first pass: entries appended to tie_list (zero at launch)
+    const uint32_t* qlist;        // second pass: query indices to run (null: 0 .. nq - 1)
+    const uint32_t* qcount;       // second pass: device word holding the entries of qlist
     unsigned long long* phase_cycles;  // 10 counters, profiling builds only (may be null)
     // learned early termination (mode 1 = record checkpoints, 2 = stop early)
     uint32_t term_mode;

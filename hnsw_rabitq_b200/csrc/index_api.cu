@@ -41,6 +41,13 @@ static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feat
 
 #include "index_internal.h"
 
+// staging slots of the float32 beam (dim % 16 == 0): rows gathered per TMA
+// batch.  On 1M x 128 at ef 52, 12 or 10 slots with 18-20 resident CTAs per SM
+// measured no faster than 16 slots with 16 CTAs (6.03-6.24 vs 6.26 M QPS).
+#ifndef HNSWGPU_FP32_SLOTS
+#define HNSWGPU_FP32_SLOTS 16
+#endif
+
 #ifdef HNSWGPU_TC_TIMING
 namespace hnswgpu {
 cudaError_t tc_timing_read(unsigned long long* out);
@@ -391,7 +398,7 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     p.links_unique = h->links_unique ? 1u : 0u;
     p.stage_stride = h->row_floats + (p.fast16 ? 16u : 4u);
     uint32_t slots = (uint32_t)((9u * 1024u + 512u) / (p.stage_stride * 4));
-    p.stage_slots = std::max(1u, std::min(p.fast16 ? 16u : 32u, slots));
+    p.stage_slots = std::max(1u, std::min(p.fast16 ? (uint32_t)HNSWGPU_FP32_SLOTS : 32u, slots));
     p.extra_cap = p.bare ? 0u : std::max<uint32_t>(128u, 4u * p.ef);
     p.exact = exact ? 1u : 0u;
     p.pool_cap = exact ? p.ef + 32u : p.ef;
@@ -476,14 +483,85 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
     }
 }
 
-// One HNSW search launch on device buffers, scratch from the index.
+static void take_counter_slot(hnswgpu_index* h, hnswgpu::SearchParams& p) {
+    const uint32_t slot = h->next_counter++ % (uint32_t)(h->counters.n / 2);
+    p.work_counter = h->counters.p + 2 * slot;
+    p.done_counter = h->counters.p + 2 * slot + 1;
+}
+
+// Two-pass tie-exact mode: the replay pass runs one query per warp and takes
+// about one replayed query's latency, whatever the share listed.  Above this
+// share of listed queries (e.g. integer-valued data at large ef) the single
+// pass that replays every query is the faster one.
+constexpr float kTwoPassMaxShare = 0.3f;
+
+// Fold in the listed share of the last listing pass once its copy landed.
+static void poll_tie_share(hnswgpu_index* h) {
+    if (!h->tie_pending_nq) return;
+    const cudaError_t e = cudaEventQuery(h->tie_ev);
+    if (e == cudaErrorNotReady) {
+        if (cudaPeekAtLastError() == cudaErrorNotReady) (void)cudaGetLastError();
+        return;
+    }
+    cuda_check(e, "cudaEventQuery");
+    h->tie_share[h->tie_pending_ef] = {(float)*h->tie_host / (float)h->tie_pending_nq, 0u};
+    h->tie_pending_nq = 0;
+}
+
+// One HNSW search on device buffers, scratch from the index.  The tie-exact
+// mode of an unfiltered float32 beam runs in two launches: the id-order beam
+// answers every query and lists those whose run met a tie that can steer the
+// reference's heaps (for the others the two orders make the same decisions, so
+// the results are the reference's); the heap replay then reruns only the
+// listed queries, reading the list's length on the device.
 void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
               uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact, uint32_t prec,
-              uint32_t rerank, const TermCfg* term) {
+              uint32_t rerank, const TermCfg* term, bool replay_all) {
     if (prec) ensure_traversal_copy(h, prec);
     hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank, true);
     apply_term(h, p, term);
     p.status = h->status.p;
+    const int space = h->space == HNSWGPU_SPACE_L2 ? 0 : 1;
+    hnswgpu::SearchParams p1{};
+    bool two_pass = exact && !replay_all && p.fast16 && p.bare && p.maxM0 <= 32;
+    if (two_pass) {
+        // a share measured above the bound picks the single pass; every 64th
+        // call at that ef measures it again
+        poll_tie_share(h);
+        auto it = h->tie_share.find(p.ef);
+        if (it != h->tie_share.end() && it->second.share > kTwoPassMaxShare && ++it->second.calls % 64 != 0)
+            two_pass = false;
+    }
+    if (two_pass) {
+        // the listing pass merges into ef + 1 slots to see the first entry dropped
+        p1 = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, false);
+        p1.pool_cap = p1.ef + 1;
+        int max_optin = 0;
+        cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+        two_pass = hnswgpu::warp_smem_layout(p1) * hnswgpu::kWarpsPerBlock <= (size_t)max_optin;
+    }
+    if (two_pass) {
+        p1.status = h->status.p;
+        if (h->tie_list.n < nq + 1) {
+            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            h->tie_list.alloc(nq + 1);
+        }
+        cuda_check(cudaMemsetAsync(h->tie_list.p, 0, 4, st), "cudaMemsetAsync");
+        p1.tie_count = h->tie_list.p;
+        p1.tie_list = h->tie_list.p + 1;
+        take_counter_slot(h, p1);
+        cuda_check(hnswgpu::launch_hnsw_search(p1, space, h->num_sms, st, nullptr), "hnsw_search launch");
+        p.qcount = h->tie_list.p;
+        p.qlist = h->tie_list.p + 1;
+        if (!h->tie_pending_nq) {
+            if (!h->tie_host) cuda_check(cudaHostAlloc((void**)&h->tie_host, 4, cudaHostAllocDefault), "cudaHostAlloc");
+            if (!h->tie_ev) cuda_check(cudaEventCreateWithFlags(&h->tie_ev, cudaEventDisableTiming), "cudaEventCreate");
+            cuda_check(cudaMemcpyAsync(h->tie_host, h->tie_list.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+            cuda_check(cudaEventRecord(h->tie_ev, st), "cudaEventRecord");
+            h->tie_pending_ef = p.ef;
+            h->tie_pending_nq = nq;
+        }
+    }
     if (exact) {
         // one tail per resident warp: at most 32 CTAs per SM
         const uint64_t warps = (uint64_t)h->num_sms * 32u * hnswgpu::kWarpsPerBlock;
@@ -504,11 +582,8 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     p.phase_cycles = phase_buf;
     g_phase_buf = phase_buf;
 #endif
-    uint32_t slot = h->next_counter++ % (uint32_t)(h->counters.n / 2);
-    p.work_counter = h->counters.p + 2 * slot;
-    p.done_counter = h->counters.p + 2 * slot + 1;
-    cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
-               "hnsw_search launch");
+    take_counter_slot(h, p);
+    cuda_check(hnswgpu::launch_hnsw_search(p, space, h->num_sms, st, nullptr), "hnsw_search launch");
 }
 
 // Exact brute force of a batch on device buffers (bf_search.cu).
@@ -688,7 +763,7 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
 
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
-                uint32_t prec, uint32_t rerank, const TermCfg* term, bool scan) {
+                uint32_t prec, uint32_t rerank, const TermCfg* term, bool scan, bool replay_all) {
     if (scan && !h->is_bf && h->num_deleted) {
         // deleted elements are never returned: fold them into the row mask
         h->scan_mask.ensure(h->count);
@@ -716,7 +791,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
         cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
                    "bf_search launch");
     } else {
-        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank, term);
+        run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank, term, replay_all);
     }
 }
 
@@ -865,6 +940,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         const bool want_trace = (o.flags & HNSWGPU_TRACE) && o.trace;
         const bool exact = (o.flags & HNSWGPU_EXACT_TIES) != 0;
         const bool scan = (o.flags & HNSWGPU_EXACT_SCAN) != 0;
+        const bool replay_all = (o.flags & HNSWGPU_REPLAY_ALL) != 0;
         TermCfg term;
         if (o.flags & HNSWGPU_LEARNED_STOP) term.mode = 2;
         if (scan && term.mode) return fail(HNSWGPU_ERR_ARG, "HNSWGPU_EXACT_SCAN excludes HNSWGPU_LEARNED_STOP");
@@ -890,7 +966,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         }
         if (dev) {
             run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
-                       want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank, &term, scan);
+                       want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank, &term, scan, replay_all);
             return HNSWGPU_OK;
         }
         // host pointers: stage through the index's device I/O buffer
@@ -911,7 +987,8 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             dallow = h->allow.p;
         }
         cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
-        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact, o.precision, o.rerank, &term, scan);
+        run_search(h, dq, nq, k, ef, dallow, dl, dd, dc, dt, st, exact, o.precision, o.rerank, &term, scan,
+                   replay_all);
         cuda_check(cudaMemcpyAsync(out_labels, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
@@ -1063,7 +1140,8 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
         term.feat = df.p;
         term.ids = di.p;
         term.count = dn.p;
-        run_hnsw(h, dq.p, nq, k, ef, nullptr, dl.p, dd.p, dc.p, nullptr, st, false, o.precision, o.rerank, &term);
+        run_hnsw(h, dq.p, nq, k, ef, nullptr, dl.p, dd.p, dc.p, nullptr, st, false, o.precision, o.rerank, &term,
+                 false);
         cuda_check(cudaMemcpyAsync(out_labels, dl.p, nq * k * 8, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_dists, dd.p, nq * k * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc.p, nq * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");

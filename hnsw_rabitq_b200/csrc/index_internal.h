@@ -86,6 +86,17 @@ struct hnswgpu_index {
     DevBuf<unsigned char> tcopy[3];  // low-precision traversal copies (index 1 bf16, 2 fp8)
     DevBuf<unsigned char> term_model;  // learned termination: packed network
     DevBuf<uint64_t> cand_spill;       // tie-exact mode: candidate-heap tails
+    DevBuf<uint32_t> tie_list;         // tie-exact mode: [0] count, then the queries to replay
+    // share of listed queries per ef, read back without blocking: the word
+    // tie_list[0] is copied to pinned memory after a listing pass
+    uint32_t* tie_host = nullptr;
+    cudaEvent_t tie_ev = nullptr;
+    uint64_t tie_pending_ef = 0, tie_pending_nq = 0;
+    struct TieShare {
+        float share = 0.f;
+        uint32_t calls = 0;  // one-pass calls since the share was measured
+    };
+    std::unordered_map<uint64_t, TieShare> tie_share;
     DevBuf<float2> tc_rowinfo[3];      // tensor-core brute force: (|x|^2, scale) per row and precision
     // tensor-core brute force: per-call workspace
     DevBuf<float> tc_qf, tc_qscale, tc_tau;
@@ -98,6 +109,10 @@ struct hnswgpu_index {
     uint32_t term_period = 0;
     float term_logit = 0.f;
     std::mutex mu;
+    ~hnswgpu_index() {
+        if (tie_host) cudaFreeHost(tie_host);
+        if (tie_ev) cudaEventDestroy(tie_ev);
+    }
     uint64_t device_bytes() const {
         return vecs.bytes() + links0.bytes() + upper_off.bytes() + upper_links.bytes() + deleted_bits.bytes() +
                dlabels.bytes() + bf_norms.bytes() + tcopy[1].bytes() + tcopy[2].bytes();
@@ -142,6 +157,7 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
 // buffers on stream `st`; the caller holds h->mu.
 void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64_t ef, const uint8_t* dallow,
                 uint64_t* dl, float* dd, int32_t* dc, uint32_t* dtrace, cudaStream_t st, bool exact,
-                uint32_t prec = 0, uint32_t rerank = 0, const TermCfg* term = nullptr, bool scan = false);
+                uint32_t prec = 0, uint32_t rerank = 0, const TermCfg* term = nullptr, bool scan = false,
+                bool replay_all = false);
 
 }  // namespace hnswgpu_host

@@ -125,6 +125,8 @@ class _GpuIndex:
         opts.flags = int(flags)
         if exact_ties and opts.precision == _capi.PREC_FP32 and not flags & _capi.LEARNED_STOP:
             opts.flags |= _capi.EXACT_TIES
+            if exact_ties == "replay":
+                opts.flags |= _capi.REPLAY_ALL
         mask = self._allow_mask(filter)
         opts.allow = mask.ctypes.data if mask is not None else None
         tr = None
@@ -308,11 +310,17 @@ class Index(_GpuIndex):
                          learned: Optional[bool] = None):
         """knn_query plus per-query work counters [upper link lists read,
         upper distances, level-0 expansions, level-0 distances] and counts;
-        no exception for short results."""
+        no exception for short results.  tie_order "replay" gives the
+        "reference" results by replaying the reference's heaps for every query
+        in one pass (the default reference order replays only the queries whose
+        id-order run met a steering tie)."""
         order = tie_order or self.tie_order
+        if order not in ("reference", "id", "replay"):
+            raise ValueError("tie_order must be 'reference', 'id' or 'replay'")
         prec = precision or self.precision
         rr = self.rerank if rerank is None else rerank
-        return self._search(data, k, filter, ef=ef, trace=True, exact_ties=order == "reference", precision=prec,
+        exact = "replay" if order == "replay" else order == "reference"
+        return self._search(data, k, filter, ef=ef, trace=True, exact_ties=exact, precision=prec,
                             rerank=rr, flags=self._flags(learned))
 
 

@@ -57,7 +57,14 @@ extern "C" {
 #define HNSWGPU_EXACT_TIES 0x4u   /* HNSW: replay the reference's heap order so
                                      that exact distance ties resolve as in
                                      hnswlib (results identical to searchKnn);
-                                     without it ties break by internal id.     */
+                                     without it ties break by internal id.
+                                     Runs in two passes: the id-order beam for
+                                     every query, then the heap replay only for
+                                     the queries whose run met a distance tie
+                                     that can steer the reference's heaps.     */
+#define HNSWGPU_REPLAY_ALL 0x20u  /* with HNSWGPU_EXACT_TIES: one pass, the
+                                     heap replay for every query (same results;
+                                     for testing and measurement).             */
 #define HNSWGPU_LEARNED_STOP 0x8u /* HNSW: end each query's level-0 beam when
                                      the termination network set by
                                      hnswgpu_set_termination_model judges its
@@ -203,7 +210,9 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
  *
  * Same search as hnswgpu_search with HNSWGPU_DEVICE_PTRS: queries, outputs and
  * the optional allow mask are device pointers, `ef` 0 means the index's ef,
- * flags may only hold HNSWGPU_EXACT_TIES; the call is asynchronous on `stream`.
+ * flags may only hold HNSWGPU_EXACT_TIES (which here always runs the one-pass
+ * heap replay: the two-pass form needs a per-query list); the call is
+ * asynchronous on `stream`.
  * The kernel's scratch (work counter, finished-CTA counter, status word) is a
  * fixed 256-byte array in the library's device image instead of per-index
  * memory; nq >= 2^31 is rejected.  Every GPU that loads the library holds that

@@ -172,3 +172,19 @@ def test_serving_helpers():
     r = Server.request(k=5, ef=64, filter=2, tie_order="reference", precision="bf16", rerank=7)
     assert (r.k, r.ef, r.filter, r.flags, r.precision, r.rerank) == (5, 64, 2, _capi.EXACT_TIES, _capi.PREC_BF16, 7)
     assert Server.request(learned=True).flags == _capi.LEARNED_STOP
+
+
+def test_flag_and_status_constants_match_header():
+    src = open(HEADER).read()
+    defs = {m.group(1): int(m.group(2), 16) for m in re.finditer(r"#define HNSWGPU_(\w+)\s+0x([0-9a-fA-F]+)u", src)}
+    for name in ("DEVICE_PTRS", "TRACE", "EXACT_TIES", "LEARNED_STOP", "EXACT_SCAN", "REPLAY_ALL", "STATUS_TIMEOUT",
+                 "STATUS_OVERFLOW"):
+        assert defs[name] == getattr(_capi, name), name
+    flags = [defs[n] for n in ("DEVICE_PTRS", "TRACE", "EXACT_TIES", "LEARNED_STOP", "EXACT_SCAN", "REPLAY_ALL")]
+    assert len(set(flags)) == len(flags) and all(f & (f - 1) == 0 for f in flags)
+
+
+def test_tie_order_values():
+    idx = H.Index("l2", 8)
+    with pytest.raises(ValueError, match="tie_order"):
+        idx.knn_query_traced(np.zeros((1, 8), np.float32), tie_order="heap")

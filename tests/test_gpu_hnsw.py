@@ -19,8 +19,10 @@ def gpu_index(path, space, dim):
 
 def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.999):
     """Both tie orders through the C ABI:
-    * tie_order="reference" (heap replay): labels, distances and counts
-      identical to the reference algorithm, same number of expansions;
+    * tie_order="reference" (id-order beam, heap replay of the queries it
+      lists) and "replay" (heap replay of every query): labels, distances
+      and counts identical to the reference algorithm, same number of
+      expansions;
     * tie_order="id": bit-identical to the oracle's canonical mode, and equal
       to the reference on every query whose reference run made no tie
       decision."""
@@ -43,6 +45,10 @@ def check_parity(path, space, q, k, ef, allow_fn=None, deleted=(), min_same=0.99
     assert np.array_equal(xl, rl), np.nonzero(~np.all(xl == rl, axis=1))[0][:10]
     assert np.array_equal(xd.view(np.uint32), rd.view(np.uint32))
     assert np.array_equal(xt[:, :3].astype(np.int64), rt[:, :3])
+    yl, yd, yc, yt = g.knn_query_traced(q, k, filter=allow_fn, tie_order="replay")
+    assert g.get_status() == 0
+    assert np.array_equal(yc, rc) and np.array_equal(yl, rl) and np.array_equal(yd.view(np.uint32), rd.view(np.uint32))
+    assert np.array_equal(yt[:, :3].astype(np.int64), rt[:, :3])
     # id tie order == the canonical oracle
     gl, gd, gc, gt = g.knn_query_traced(q, k, filter=allow_fn, tie_order="id")
     assert g.get_status() == 0, "candidate list overflow or timeout"
@@ -238,6 +244,11 @@ def test_full_size_parity_1m():
         xl, xd = g.knn_query(qs, k=10)
         assert g.get_status() == 0, "candidate heap overflow"
         assert np.array_equal(xl, rl) and np.array_equal(xd.view(np.uint32), rd.view(np.uint32))
+        # the listing pass's expansion counts: every unlisted query matches the reference's
+        tl, td, _, tt = g.knn_query_traced(qs, k=10, tie_order="reference")
+        assert np.array_equal(tl, rl) and np.array_equal(tt[:, 2].astype(np.int64), rt[:, 2])
+        yl, yd, _, _ = g.knn_query_traced(qs, k=10, tie_order="replay")
+        assert np.array_equal(yl, rl) and np.array_equal(yd.view(np.uint32), rd.view(np.uint32))
         g.tie_order = "id"
         gl, gd = g.knn_query(qs, k=10)
         cl, cd, _ = o.search(qs, 10, ef, mode=O.CANONICAL)
