@@ -338,8 +338,8 @@ __device__ __forceinline__ bool lane_distances(const SearchParams& p, WarpSmem& 
 }
 
 // ------------------------------------------------------------------------
-// Pipelined level-0 beam for the common case (no deletes, no filter,
-// dim % 16 == 0, maxM0 <= 32).  Same decisions as the general loop; the
+// Pipelined level-0 beam for dim % 16 == 0 and maxM0 <= 32 (with deletes or a
+// filter in the id tie order only).  Same decisions as the general loop; the
 // difference is scheduling: as soon as the acceptance of the current
 // expansion is known, the next candidate is fixed (id tie order: the first
 // unexpanded of pool + accepted; tie-exact order: the candidate heap's top,
@@ -384,14 +384,19 @@ struct Fetch {
     int nnew;        // number of fresh lanes
     uint32_t cid2;   // id of the lane-th fresh neighbour (lanes < nnew)
     int n0;          // rows of the first staging batch in flight
+    bool allowed;    // FILTER: this lane's neighbour may be returned (not deleted, passes the filter)
 };
 
-template <int PREC>
-__device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, uint32_t c, int lane, Fetch& f) {
+// FILTER: also read each fresh neighbour's delete bit and filter byte (used
+// only after the row gather, so their latency overlaps it) and never admit
+// `skip` (a disallowed entry point, never stored with its distance).
+template <int PREC, bool FILTER = false>
+__device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, uint32_t c, int lane, Fetch& f,
+                                            uint32_t skip = INVALID_ID) {
     const RowSrc rs = trav_src<PREC>(p);
     const uint32_t* lrow = p.links0 + (size_t)c * p.maxM0;
     const uint32_t id = lane < (int)p.maxM0 ? __ldg(lrow + lane) : INVALID_ID;
-    bool fresh = id != INVALID_ID;
+    bool fresh = id != INVALID_ID && (!FILTER || id != skip);
     if (!p.links_unique) {
         unsigned peers = __match_any_sync(FULL, id);
         fresh = fresh && (__ffs(peers) - 1 == lane);
@@ -402,6 +407,7 @@ __device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, 
     if (fresh) s.vis[slot] = id;
     f.id = id;
     f.fresh = fresh;
+    f.allowed = !FILTER || !fresh || is_allowed(p, id);
     f.nmask = __ballot_sync(FULL, fresh);
     f.nnew = __popc(f.nmask);
     const int src = (int)__fns(f.nmask, 0, lane + 1);
@@ -633,25 +639,37 @@ __device__ __forceinline__ void term_final_row(const SearchParams& p, const Warp
 // dropped from the full pool tie with its new worst entry (an evicted entry that
 // stays in candidate_set at lowerBound would still be expanded); (c), the
 // top-k boundary tie, is checked by the caller.
-template <int SPACE, bool EXACT, int PREC, int TERM, bool TIES = false>
+//
+// FILTER (id order only): deletions and / or an allow mask, as in the
+// reference's non-bare-bone loop (hnswalg.h:330-440).  Accepted neighbours that
+// may not be returned go to the sorted list s.extra instead of the pool: they
+// are candidates (expanded in distance order) but never results.  A candidate
+// taken from that list ends the search when the pool is full and its distance
+// is above lowerBound; list entries beyond lowerBound are dropped, since they
+// can only end the search.  A disallowed entry point (ep_ok false) is expanded
+// first and never stored.
+template <int SPACE, bool EXACT, int PREC, int TERM, bool TIES = false, bool FILTER = false>
 __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& phase, int lane, Counters& ct,
                                PhaseClock& pc, const float4* qr, uint32_t ep, float d0, int& psize, int& tsz,
-                               uint32_t& status, uint32_t qi, float qn) {
+                               uint32_t& status, uint32_t qi, float qn, bool ep_ok = true) {
     const int ef = (int)p.ef;
     const int kq = (int)p.k;
     TermState ts;
     const int pcap = (int)p.pool_cap;
     int hint_p = 0, csz = 0;
+    int xsize = 0, hint_x = 0;  // FILTER: the list of disallowed candidates
+    const int xcap = (int)p.extra_cap;
+    const uint32_t skip_id = FILTER && !ep_ok ? ep : INVALID_ID;
     // the entry point is pushed and popped at once (hnswalg.h:325-359)
-    if (lane == 0) {
+    if (lane == 0 && (!FILTER || ep_ok)) {
         s.pool[0] = mkkey(d0, ep) | (EXACT ? 0u : EXP_BIT);
         if (EXACT) s.topheap[0] = mkkey(d0, ep);
     }
-    psize = 1;
+    psize = !FILTER || ep_ok ? 1 : 0;
     tsz = EXACT ? 1 : 0;
     __syncwarp();
     Fetch f;
-    fetch_links<PREC>(p, s, ep, lane, f);
+    fetch_links<PREC, FILTER>(p, s, ep, lane, f, skip_id);
     ct.l0_exp += 1;
     PT_MARK(3);
     while (true) {
@@ -664,14 +682,16 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         const uint32_t lbk = full ? khi(s.pool[psize - 1]) : 0xffffffffu;
         bool live = f.fresh && !(full && dk >= lbk);
         uint64_t key = ((uint64_t)dk << 32) | f.id;
-        int posP = 0, cntP = 0;
+        int posP = 0, cntP = 0, posX = 0;
         if (live) {
             bool dup = false;
             cntP = upper_bound_hi(s.pool, psize, dk);
             posP = insert_pos(s.pool, cntP, dk, f.id, dup);
+            if (FILTER && !dup) posX = insert_pos(s.extra, upper_bound_hi(s.extra, xsize, dk), dk, f.id, dup);
             if (dup) live = false;
         }
-        const unsigned amask = __ballot_sync(FULL, live);
+        const bool allowed = !FILTER || f.allowed;
+        const unsigned amask = __ballot_sync(FULL, live && allowed);
         int cntN = 0;
         for (unsigned m = amask; m; m &= m - 1) {
             const int src2 = __ffs(m) - 1;
@@ -679,8 +699,9 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             cntN += (src2 < lane && dk2 <= dk);
         }
         const bool accept = live && cntP + cntN < ef;
-        const unsigned pmask = __ballot_sync(FULL, accept);
-        if (TERM && __any_sync(FULL, accept && cntP + cntN < kq)) ts.last_change = ct.l0_exp;
+        const unsigned pmask = __ballot_sync(FULL, accept && allowed);
+        const unsigned xmask = FILTER ? __ballot_sync(FULL, accept && !allowed) : 0u;
+        if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < kq)) ts.last_change = ct.l0_exp;
         PT_MARK(6);
         // ---- the next candidate
         uint64_t kmin = accept ? key : ~0ull;  // smallest accepted key
@@ -689,12 +710,27 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             uint64_t other = shfl64(kmin, lane ^ o);
             kmin = other < kmin ? other : kmin;
         }
-        bool have_next = false, spec = false;
+        bool have_next = false, spec = false, next_extra = false;
         uint32_t next = INVALID_ID, next_dk = 0xffffffffu;
         if (!EXACT) {
             int ip = find_unexpanded(s.pool, psize, hint_p, lane);
             const uint64_t kp = ip >= 0 ? (s.pool[ip] & KEY_MASK) : ~0ull;
-            if (kp != ~0ull || kmin != ~0ull) {
+            int ix = -1;
+            uint64_t kx = ~0ull;
+            if (FILTER) {
+                ix = find_unexpanded(s.extra, xsize, hint_x, lane);
+                kx = ix >= 0 ? (s.extra[ix] & KEY_MASK) : ~0ull;
+            }
+            if (kx < kp && kx < kmin) {
+                // a disallowed candidate from the list (FILTER only)
+                have_next = true;
+                next_extra = true;
+                next_dk = khi(kx);
+                next = kid(kx);
+                __syncwarp();
+                if (lane == 0) s.extra[ix] |= EXP_BIT;
+                __syncwarp();
+            } else if (kp != ~0ull || kmin != ~0ull) {
                 have_next = true;
                 next_dk = khi(kmin < kp ? kmin : kp);
                 if (TIES) {  // (a): candidate_set's top must be unique by distance
@@ -704,6 +740,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
                 }
                 if (kmin < kp) {
                     next = (uint32_t)kmin;
+                    if (FILTER) next_extra = __any_sync(FULL, accept && !allowed && key == kmin);
                     if (accept && key == kmin) key |= EXP_BIT;  // inserted already expanded
                 } else {
                     next = kid(kp);
@@ -729,7 +766,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             }
         }
         Fetch fn;
-        if (have_next || spec) fetch_links<PREC>(p, s, next, lane, fn);
+        if (have_next || spec) fetch_links<PREC, FILTER>(p, s, next, lane, fn, skip_id);
         PT_MARK(2);
         // ---- bookkeeping of this expansion, under the latency of the next fetch
         int nev = 0;
@@ -765,6 +802,39 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
                 // ef + 1): the first one dropped, next to the new worst
                 if (khi(s.pool[ef]) == khi(s.pool[ef - 1])) status |= kTieBit;
                 psize = ef;
+            }
+        }
+        if (FILTER) {
+            if (xmask) {
+                if (xsize + __popc(xmask) > xcap) status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+                const int m = merge_sorted(s.extra, xsize, xcap, xmask, key, posX, lane);
+                hint_x = min(hint_x, m);
+            }
+            if (psize == ef && xsize > 0) {
+                // list entries beyond lowerBound can never be expanded
+                xsize = upper_bound_hi(s.extra, xsize, khi(s.pool[psize - 1]));
+                hint_x = min(hint_x, xsize);
+            }
+            if (next_extra && psize == ef && next_dk > khi(s.pool[ef - 1])) {
+                // the reference pops it and stops (hnswalg.h:345-347): drain
+                // the speculative fetch
+                if (fn.n0 > 0) {
+                    mbar_wait(s.bar, phase);
+                    phase ^= 1u;
+                }
+                break;
+            }
+            if (have_next && ct.l0_exp >= p.max_expansions) {
+                // Entries dropped from a full list can be re-admitted after a
+                // visited-cache miss, and a search that never fills its pool
+                // (a filter that rejects almost everything) keeps dropping
+                // them: bound the expansions and flag the query.
+                status |= HNSWGPU_STATUS_OVERFLOW_BIT;
+                if (fn.n0 > 0) {
+                    mbar_wait(s.bar, phase);
+                    phase ^= 1u;
+                }
+                break;
             }
         }
         if (EXACT && nev) remove_keys(s.pool, psize, s.evbuf, nev, lane);
@@ -891,7 +961,7 @@ __device__ bool rerank_fp32(const SearchParams& p, WarpSmem& s, uint32_t& phase,
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES = false>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES = false, bool FILTER = false>
 __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, uint32_t qi, int lane,
                            Counters& ct, PhaseClock& pc) {
     pc.start();
@@ -963,7 +1033,8 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     const int pcap = TIES ? (int)ef : (int)p.pool_cap;
     int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
     const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
-    const bool pipe = FAST16 && bare && p.maxM0 <= 32;
+    // FILTER kernels run the id order only (the host never pairs it with EXACT)
+    const bool pipe = FAST16 && (bare || FILTER) && p.maxM0 <= 32;
     float qn = 0.f;
     if (TERM) {  // |q|^2, a feature of the termination network
         for (uint32_t i = lane; i < p.dim; i += 32) qn = fmaf(s.q[i], s.q[i], qn);
@@ -993,8 +1064,8 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
 #pragma unroll
         for (int c = 0; c < 8; c++) qr[c] = c < n16 ? q4[4 * c + (lane & 3)] : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
-        if (!base_pipelined<SPACE, EXACT, PREC, TERM, TIES>(p, s, phase, lane, ct, pc, qr, cur, d0, psize, tsz,
-                                                            status, qi, qn))
+        if (!base_pipelined<SPACE, EXACT, PREC, TERM, TIES, FILTER>(p, s, phase, lane, ct, pc, qr, cur, d0, psize,
+                                                                    tsz, status, qi, qn, bare || is_allowed(p, cur)))
             return false;
         // (c): the reference pops top_candidates down to k by distance
         if (TIES && psize > (int)p.k && khi(s.pool[p.k - 1]) == khi(s.pool[p.k])) status |= kTieBit;
@@ -1253,7 +1324,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     return true;
 }
 
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM, bool TIES, bool FILTER>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP : kMinBlocks)
     hnsw_search_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -1293,7 +1364,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP 
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         Counters ct = {0, 0, 0, 0};
-        if (!search_one<SPACE, FAST16, EXACT, PREC, TERM, TIES>(p, s, phase, qi, lane, ct, pc)) {
+        if (!search_one<SPACE, FAST16, EXACT, PREC, TERM, TIES, FILTER>(p, s, phase, qi, lane, ct, pc)) {
             if (lane == 0) atomicOr(p.status, HNSWGPU_STATUS_TIMEOUT_BIT);
             // wait (bounded) for this warp's copies still in flight, then leave
             mbar_wait(s.bar, phase);
@@ -1359,13 +1430,13 @@ size_t warp_smem_layout(SearchParams& p) {
 }
 
 namespace {
-template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0, bool TIES = false>
+template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0, bool TIES = false, bool FILTER = false>
 cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
     // per-instantiation cache of the opt-in shared-memory size and occupancy
     static int attr_smem = -1;
     static size_t occ_smem = 0;
     static int occ_per_sm = 0;
-    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES>;
+    const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES, FILTER>;
     const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
     if ((int)smem > attr_smem) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1383,7 +1454,8 @@ cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, in
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES><<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES, FILTER>
+        <<<(unsigned)blocks, kWarpsPerBlock * 32, smem, stream>>>(p);
     return cudaGetLastError();
 }
 
@@ -1447,10 +1519,27 @@ cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
     return cudaSuccess;
 }
 
+// Pipelined beam over an index with deletions and / or a filter (id order,
+// dim % 16 == 0, maxM0 <= 32; learned stop or none).
+template <int SPACE, int TERM>
+cudaError_t launch_filter_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (p.prec == 0) return launch_t<SPACE, true, false, 0, TERM, false, true>(p, num_sms, stream, blocks_out);
+    return p.prec == 1 ? launch_t<SPACE, true, false, 1, TERM, false, true>(p, num_sms, stream, blocks_out)
+                       : launch_t<SPACE, true, false, 2, TERM, false, true>(p, num_sms, stream, blocks_out);
+}
+template <int SPACE>
+cudaError_t launch_filter(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
+    return p.term_mode == 2 ? launch_filter_t<SPACE, 2>(p, num_sms, stream, blocks_out)
+                            : launch_filter_t<SPACE, 0>(p, num_sms, stream, blocks_out);
+}
+
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (!p.bare && !p.exact && p.fast16 && p.maxM0 <= 32 && p.term_mode != 1 && !p.tie_list)
+        return space == 0 ? launch_filter<0>(p, num_sms, stream, blocks_out)
+                          : launch_filter<1>(p, num_sms, stream, blocks_out);
     if (p.tie_list) {
         // id-order beam that lists its tie-steered queries (float32, 4-lane
-        // distances, no filter: checked by the host)
+        // distances, no filter or deletes: checked by the host)
         if (p.exact || p.prec || p.term_mode || !p.fast16 || !p.bare || p.maxM0 > 32 || p.pool_cap != p.ef + 1 ||
             !p.tie_count)
             return cudaErrorInvalidValue;

@@ -415,10 +415,9 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     }
     p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
     if (prec) {
-        if (!p.fast16 || !p.bare || p.maxM0 > 32 || exact)
+        if (!p.fast16 || p.maxM0 > 32 || exact)
             throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
-                           "low-precision traversal needs dim % 16 == 0, maxM0 <= 32, no filter / deletes and the id "
-                           "tie order");
+                           "low-precision traversal needs dim % 16 == 0, maxM0 <= 32 and the id tie order");
         if (!h->tcopy[prec].p) throw ApiError(HNSWGPU_ERR_ARG, "traversal copy not built");
         p.prec = prec;
         p.tvecs = h->tcopy[prec].p;
@@ -458,6 +457,10 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
     p.term_mode = t->mode;
     if (t->mode == 1) {
         if (t->period == 0) throw ApiError(HNSWGPU_ERR_ARG, "checkpoint period must be > 0");
+        if (p.prec && !p.bare)
+            throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
+                           "checkpoint recording over a low-precision copy needs an index without deletes and no "
+                           "filter");
         p.term_period = t->period;
         p.term_max_ckpt = t->max_ckpt;
         p.ckpt_feat = t->feat;

@@ -98,6 +98,39 @@ def test_parity_filter_and_deletes(tmp_path):
     check_parity(path, "l2", q, 5, 50, deleted=dele, allow_fn=lambda l: l % 2 == 1)
 
 
+@pytest.mark.parametrize("space,dim", [("l2", 32), ("ip", 64), ("l2", 128)])
+def test_parity_filter_and_deletes_pipelined(tmp_path, space, dim):
+    """dim % 16 == 0 and maxM0 <= 32: the id order runs the pipelined beam
+    with its list of disallowed candidates (the reference order replays the
+    heaps in the general loop).  Both filter parities, so that one of them
+    excludes the entry point."""
+    rng = np.random.default_rng(dim)
+    x = rng.standard_normal((6000, dim)).astype(np.float32)
+    q = rng.standard_normal((400, dim)).astype(np.float32)
+    path = tmp_path / "fp.bin"
+    build_hnsw(path, x, space, M=16, efc=80)
+    check_parity(path, space, q, 10, 32, allow_fn=lambda l: l % 2 == 0)
+    check_parity(path, space, q, 10, 32, allow_fn=lambda l: l % 2 == 1)
+    check_parity(path, space, q, 10, 100, allow_fn=lambda l: l % 3 == 0)
+    dele = rng.choice(6000, 300, replace=False)
+    check_parity(path, space, q, 10, 50, deleted=dele)
+    g = check_parity(path, space, q, 5, 50, deleted=dele, allow_fn=lambda l: l % 2 == 1)
+    _, _, c, _ = g.knn_query_traced(x[:4], k=3, filter=lambda l: False, tie_order="id")
+    assert (c == 0).all()
+
+
+def test_parity_filter_integer_data(tmp_path):
+    """Integer-valued 128-d vectors (many exact ties) with deletes and a
+    filter: the pipelined filtered beam against the oracle's canonical order."""
+    from hnsw_rabitq_b200.datasets import gmm_1m_128
+    x, q = gmm_1m_128(n=20000, nq=600)
+    path = tmp_path / "gmmf.bin"
+    build_hnsw(path, x, "l2", M=16, efc=100, num_threads=8)
+    dele = np.arange(0, 20000, 19)
+    for ef in (16, 64, 200):
+        check_parity(path, "l2", q, 10, ef, deleted=dele, allow_fn=lambda l: l % 4 != 1, min_same=0.995)
+
+
 def test_golden_fixtures():
     """Against the reference's own recorded outputs: the default (tie-exact)
     mode reproduces them exactly, the integer fixture with its many ties

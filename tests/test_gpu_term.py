@@ -170,14 +170,16 @@ def test_exact_scan_is_ground_truth(gmm_index):
     assert np.array_equal(d.view(np.uint32), rd.view(np.uint32))
 
 
-def test_learned_stop_general_path(tmp_path):
-    """Filters, deletes and dims that are not multiples of 16 take the general
-    beam; its checkpoints and stop rule behave as the pipelined beam's."""
+@pytest.mark.parametrize("dim", [20, 32])
+def test_learned_stop_general_path(tmp_path, dim):
+    """Filters and deletes: at dim 20 the general beam, at dim 32 the
+    pipelined beam with its list of disallowed candidates; checkpoints and the
+    stop rule behave as on an unfiltered index."""
     rng = np.random.default_rng(11)
-    x = rng.standard_normal((8000, 20)).astype(np.float32)
-    q = rng.standard_normal((300, 20)).astype(np.float32)
+    x = rng.standard_normal((8000, dim)).astype(np.float32)
+    q = rng.standard_normal((300, dim)).astype(np.float32)
     build_hnsw(tmp_path / "g.bin", x, "l2", M=12, efc=100)
-    g = H.Index("l2", 20)
+    g = H.Index("l2", dim)
     g.load_index(str(tmp_path / "g.bin"))
     for lab in range(0, 8000, 37):
         g.mark_deleted(lab)
