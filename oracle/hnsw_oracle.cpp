@@ -260,6 +260,7 @@ Hnsw* load_hnsw(const char* path, int space, uint64_t dim) {
 
 struct Trace {
     int64_t upper_hops = 0, upper_dists = 0, l0_expansions = 0, l0_dists = 0, ties = 0, max_cand = 0;
+    int64_t listed = 0;  // mode 1: the run met a tie that can steer the reference's heaps (see below)
 };
 
 // Upper-layer greedy descent (hnswalg.h:1274-1302).  Shared by both modes.
@@ -407,6 +408,14 @@ struct Ent {
 //    lowerBound while the pool is full (hnswalg.h:353);
 //  * evicted pool entries are forgotten: in the reference they stay in the
 //    candidate heap but can only be expanded when they tie lowerBound.
+// Trace::listed marks a bare run that meets one of the ties after which the
+// reference's heaps may decide differently (the rule the GPU's two-pass
+// tie-exact search lists queries by; the caller adds the top-k boundary):
+//  (a) the entry popped next shares its distance with another unexpanded one;
+//  (b) the entries dropped from the full pool by one expansion's insertions
+//      include one whose distance equals the pool's new worst.
+// A run with neither (and no boundary tie) makes the reference's decisions.
+// A filtered run is always listed.
 std::vector<Ent> base_layer_canonical(const Hnsw& h, uint32_t ep, const float* q, size_t ef, bool bare,
                                       const uint8_t* allow, std::vector<uint32_t>& vis, uint32_t tag, Trace& tr) {
     std::vector<Ent> pool, extra;
@@ -423,6 +432,7 @@ std::vector<Ent> base_layer_canonical(const Hnsw& h, uint32_t ep, const float* q
         extra.push_back({std::numeric_limits<float>::max(), ep, false});
     }
     vis[ep] = tag;
+    if (!bare) tr.listed = 1;
     while (true) {
         Ent* cp = nullptr;
         bool from_extra = false;
@@ -435,11 +445,16 @@ std::vector<Ent> base_layer_canonical(const Hnsw& h, uint32_t ep, const float* q
         if (!cp) break;
         float lb = pool.empty() ? std::numeric_limits<float>::max() : pool.back().d;
         if (!bare && from_extra && cp->d > lb && pool.size() == ef) break;
+        if (bare)
+            for (auto& e : pool)
+                if (&e != cp && !e.exp && e.d == cp->d) tr.listed = 1;  // (a)
         cp->exp = true;
         uint32_t cid = cp->id;
         const uint32_t* ll = h.links0(cid);
         size_t size = Hnsw::count(ll);
         tr.l0_expansions++;
+        bool dropped = false;
+        float min_dropped = 0.f;
         for (size_t j = 1; j <= size; j++) {
             uint32_t c = ll[j];
             if (vis[c] == tag) continue;
@@ -450,12 +465,17 @@ std::vector<Ent> base_layer_canonical(const Hnsw& h, uint32_t ep, const float* q
             if (pool.size() < ef || lbn > d) {
                 if (bare || allowed(c)) {
                     ins(pool, {d, c, false});
-                    if (pool.size() > ef) pool.pop_back();
+                    if (pool.size() > ef) {
+                        if (!dropped || pool.back().d < min_dropped) min_dropped = pool.back().d;
+                        dropped = true;
+                        pool.pop_back();
+                    }
                 } else {
                     ins(extra, {d, c, false});
                 }
             }
         }
+        if (dropped && pool.back().d == min_dropped) tr.listed = 1;  // (b)
     }
     return pool;
 }
@@ -494,6 +514,7 @@ void search_one(const Hnsw& h, const float* q, size_t k, size_t ef, int mode, co
         while (!result.empty()) { out.res[--n] = result.top(); result.pop(); }
     } else {
         std::vector<Ent> pool = base_layer_canonical(h, cur, q, ef2, bare, allow, vis, tag, tr);
+        if (pool.size() > k && pool[k - 1].d == pool[k].d) tr.listed = 1;  // the top-k boundary
         size_t n = std::min(k, pool.size());
         for (size_t i = 0; i < n; i++) out.res.emplace_back(pool[i].d, h.label(pool[i].id));
         std::sort(out.res.begin(), out.res.end());
@@ -639,9 +660,10 @@ int orc_hnsw_set_deleted(void* p, uint64_t label, int flag) {
 // Batched searchKnn.  mode 0 = reference heaps, 1 = canonical pool.
 // allow: optional per-internal-id byte mask (the filter functor evaluated on
 // each node's label).  Outputs are closest first; counts[i] = results found.
-// trace (optional) receives 6 int64 per query: upper-layer link lists read,
+// trace (optional) receives 7 int64 per query: upper-layer link lists read,
 // upper-layer distances, level-0 expansions, level-0 distances, tie events
-// (mode 0 only; see base_layer_reference), largest candidate-heap size (mode 0).
+// (mode 0 only; see base_layer_reference), largest candidate-heap size (mode 0),
+// listed for the heap replay (mode 1; see base_layer_canonical).
 int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t ef, int mode,
                     const uint8_t* allow, uint64_t* labels, float* dists, int32_t* counts,
                     int64_t* trace, int nthreads) {
@@ -667,12 +689,13 @@ int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t e
             dists[i * k + j] = j < r.size() ? r[j].first : std::numeric_limits<float>::infinity();
         }
         if (trace) {
-            trace[i * 6 + 0] = tr.upper_hops;
-            trace[i * 6 + 1] = tr.upper_dists;
-            trace[i * 6 + 2] = tr.l0_expansions;
-            trace[i * 6 + 3] = tr.l0_dists;
-            trace[i * 6 + 4] = tr.ties;
-            trace[i * 6 + 5] = tr.max_cand;
+            trace[i * 7 + 0] = tr.upper_hops;
+            trace[i * 7 + 1] = tr.upper_dists;
+            trace[i * 7 + 2] = tr.l0_expansions;
+            trace[i * 7 + 3] = tr.l0_dists;
+            trace[i * 7 + 4] = tr.ties;
+            trace[i * 7 + 5] = tr.max_cand;
+            trace[i * 7 + 6] = tr.listed;
         }
     });
     if (failed) { g_err = "cand error"; return -1; }

@@ -136,7 +136,7 @@ class Hnsw:
         labels = np.empty((nq, k), np.uint64)
         dists = np.empty((nq, k), np.float32)
         counts = np.empty(nq, np.int32)
-        tr = np.zeros((nq, 6), np.int64) if trace else None
+        tr = np.zeros((nq, 7), np.int64) if trace else None
         if allow is not None:
             allow = np.ascontiguousarray(allow, np.uint8)
         rc = lib().orc_hnsw_search(self._h, _ptr(q), nq, k, ef, mode, _ptr(allow), _ptr(labels), _ptr(dists),

@@ -148,3 +148,42 @@ def test_tie_witness_on_integer_fixture():
         total += differ.sum()
         assert not (differ & (rt[:, 4] == 0)).any()
     assert total > 0
+
+
+def test_listing_rule_covers_every_divergence(tmp_path):
+    """The two-pass tie-exact search runs the id order for every query and
+    replays the reference's heaps only for the queries its run lists: the
+    entry popped next ties another unexpanded entry, an expansion drops an
+    entry that ties the pool's new worst, or the k-th and (k+1)-th entries tie.
+    On tie-heavy data every unlisted query must have the reference's labels,
+    distances, counts and expansion count, and the rule must not list all."""
+    from hnsw_rabitq_b200.datasets import gmm_1m_128
+    ref_or_skip()
+    g = golden()
+    cases = [(O.Hnsw(f"{GOLDEN}/hnsw_l2_d7_int.bin", "l2", 7), g["hnsw_l2_d7_int/queries"])]
+    rng = np.random.default_rng(5)
+    # small-integer vectors: distances tie often (about a third to a half of
+    # the queries listed at ef 10, a few percent of them steered)
+    for hi, dim in ((16, 16), (32, 8)):
+        x = rng.integers(0, hi, size=(4000, dim)).astype(np.float32)
+        q = rng.integers(0, hi, size=(300, dim)).astype(np.float32)
+        build_hnsw(tmp_path / f"i{hi}.bin", x, "l2", M=8, efc=60)
+        cases.append((O.Hnsw(str(tmp_path / f"i{hi}.bin"), "l2", dim), q))
+    x, q = gmm_1m_128(n=5000, nq=300)  # the 1M workload's distribution, few ties
+    build_hnsw(tmp_path / "gmm.bin", x, "l2", M=8, efc=60)
+    cases.append((O.Hnsw(str(tmp_path / "gmm.bin"), "l2", 128), q))
+    listed = total = differ_total = 0
+    for o, qs in cases:
+        for ef, k in ((10, 1), (10, 10), (32, 10), (100, 10)):
+            rl, rd, rc, rt = o.search(qs, k, ef, mode=O.REFERENCE, trace=True)
+            cl, cd, cc, ct = o.search(qs, k, ef, mode=O.CANONICAL, trace=True)
+            unl = ct[:, 6] == 0
+            assert np.array_equal(cl[unl], rl[unl]) and np.array_equal(cc[unl], rc[unl])
+            assert np.array_equal(cd[unl].view(np.uint32), rd[unl].view(np.uint32))
+            assert np.array_equal(ct[unl, 2], rt[unl, 2])
+            differ = ~np.all(cl == rl, axis=1)
+            differ_total += int(differ.sum())
+            listed += int((~unl).sum())
+            total += len(qs)
+    assert differ_total > 0  # the data does steer the heaps
+    assert listed < total
