@@ -108,7 +108,10 @@ typedef struct hnswgpu_search_opts {
                                   copy (sampled threshold, fused candidate
                                   filter; synchronises).  Both re-rank the
                                   best `rerank` candidates with exact FP32
-                                  distances before returning k.                */
+                                  distances before returning k.  The HNSW
+                                  form needs dim % 16 == 0, maxM0 <= 32 and
+                                  the id tie order; deletes and `allow` are
+                                  honoured.                                    */
     uint64_t ef;               /* 0: use the index's ef_ (setEf)               */
     const uint8_t* allow;      /* optional per-internal-id byte mask: nonzero =
                                   the filter functor accepts that node's label.
