@@ -14,9 +14,12 @@
 //   its share at once, so requests that arrive while others are on the GPU
 //   are admitted as slots and memory free up;
 // * each batch is one search launch on one of max_inflight CUDA streams with
-//   its own pinned staging and device buffers, so batches of different
-//   configurations overlap on the device; completion is seen through a CUDA
-//   event per batch;
+//   its own pinned staging and device buffers (sized up front, grown
+//   geometrically), so batches of different configurations overlap on the
+//   device; completion is seen through a CUDA event per batch, polled from
+//   the oldest batch in flight;
+// * the scheduler releases the server lock while it copies and launches, so
+//   submissions never wait for a launch (their arrival times stay exact);
 // * latency is measured from submission to the moment the scheduler sees
 //   the batch's results on the host.
 // Tie-exact batches share the index's candidate-heap spill area, so at most
@@ -49,8 +52,11 @@ struct Key {
         return std::tie(k, ef, flags, precision, rerank, filter) <
                std::tie(o.k, o.ef, o.flags, o.precision, o.rerank, o.filter);
     }
-    bool operator==(const Key& o) const { return !(*this < o) && !(o < *this); }
 };
+
+// Buffer sizes grow geometrically: a reallocation frees device memory, and a
+// free waits for the whole device, which stalls every batch in flight.
+size_t grown(size_t need, size_t have) { return need <= have ? need : std::max(need, 2 * have); }
 
 enum State { kPending = 0, kInflight = 1, kDone = 2, kFailed = 3 };
 
@@ -108,8 +114,13 @@ struct hnswgpu_server {
     uint64_t budget = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
+    // Tickets by id.  A waiter keeps a pointer to its ticket while it waits:
+    // element addresses survive the rehashing of later insertions.
     std::unordered_map<uint64_t, Ticket> tickets;
-    std::deque<uint64_t> pending;
+    // waiting requests by configuration, each queue in arrival (= id) order
+    std::map<Key, std::deque<uint64_t>> queues;
+    uint64_t npending = 0;
+    std::deque<Slot*> inflight;  // busy slots in launch order
     std::vector<std::unique_ptr<Slot>> slots;
     std::vector<std::unique_ptr<DevBuf<uint8_t>>> filters;
     std::map<Key, uint64_t> footprint;  // per-query bytes of each configuration
@@ -144,36 +155,25 @@ uint64_t query_footprint(hnswgpu_server* s, const Key& key) {
     return f;
 }
 
-void launch(hnswgpu_server* s, Slot& sl, const Key& key, const std::vector<uint64_t>& ids, uint64_t fq) {
+// Stage a batch into a free slot and launch it.  Called by the worker with
+// the server lock held; the lock is released around the copies and the
+// search launch, so that submissions are not held up by them (only the
+// worker thread touches slots).
+void launch(hnswgpu_server* s, std::unique_lock<std::mutex>& lk, Slot& sl, const Key& key,
+            const std::vector<uint64_t>& ids, uint64_t fq) {
     hnswgpu_index* h = s->h;
     const uint64_t n = ids.size(), dim = h->dim;
-    sl.hq.ensure(n * dim);
-    sl.hl.ensure(n * key.k);
-    sl.hd.ensure(n * key.k);
-    sl.hc.ensure(n);
-    sl.dq.ensure(n * dim);
-    sl.dl.ensure(n * key.k);
-    sl.dd.ensure(n * key.k);
-    sl.dc.ensure(n);
+    sl.hq.ensure(grown(n * dim, sl.hq.n));
+    sl.hl.ensure(grown(n * key.k, sl.hl.n));
+    sl.hd.ensure(grown(n * key.k, sl.hd.n));
+    sl.hc.ensure(grown(n, sl.hc.n));
     for (uint64_t i = 0; i < n; i++) {
         Ticket& t = s->tickets[ids[i]];
         std::memcpy(sl.hq.p + i * dim, t.q.data(), dim * sizeof(float));
         t.state = kInflight;
     }
-    cuda_check(cudaMemcpyAsync(sl.dq.p, sl.hq.p, n * dim * 4, cudaMemcpyHostToDevice, sl.st), "cudaMemcpyAsync");
     const uint8_t* allow = key.filter >= 0 ? s->filters[key.filter]->p : nullptr;
-    TermCfg term;
-    if (key.flags & HNSWGPU_LEARNED_STOP) term.mode = 2;
-    {
-        std::lock_guard<std::mutex> g(h->mu);
-        set_device(h);
-        run_search(h, sl.dq.p, n, key.k, key.ef, allow, sl.dl.p, sl.dd.p, sl.dc.p, nullptr, sl.st,
-                   (key.flags & HNSWGPU_EXACT_TIES) != 0, key.precision, key.rerank, &term, false);
-    }
-    cuda_check(cudaMemcpyAsync(sl.hl.p, sl.dl.p, n * key.k * 8, cudaMemcpyDeviceToHost, sl.st), "cudaMemcpyAsync");
-    cuda_check(cudaMemcpyAsync(sl.hd.p, sl.dd.p, n * key.k * 4, cudaMemcpyDeviceToHost, sl.st), "cudaMemcpyAsync");
-    cuda_check(cudaMemcpyAsync(sl.hc.p, sl.dc.p, n * 4, cudaMemcpyDeviceToHost, sl.st), "cudaMemcpyAsync");
-    cuda_check(cudaEventRecord(sl.ev, sl.st), "cudaEventRecord");
+    // reserve the slot and the footprint before letting go of the lock
     sl.tickets = ids;
     sl.key = key;
     sl.footprint = fq * n;
@@ -183,6 +183,38 @@ void launch(hnswgpu_server* s, Slot& sl, const Key& key, const std::vector<uint6
     if (sl.exact) s->exact_inflight = true;
     s->batches++;
     s->batched_queries += n;
+    s->inflight.push_back(&sl);
+    lk.unlock();
+    try {
+        sl.dq.ensure(grown(n * dim, sl.dq.n));
+        sl.dl.ensure(grown(n * key.k, sl.dl.n));
+        sl.dd.ensure(grown(n * key.k, sl.dd.n));
+        sl.dc.ensure(grown(n, sl.dc.n));
+        cuda_check(cudaMemcpyAsync(sl.dq.p, sl.hq.p, n * dim * 4, cudaMemcpyHostToDevice, sl.st), "cudaMemcpyAsync");
+        TermCfg term;
+        if (key.flags & HNSWGPU_LEARNED_STOP) term.mode = 2;
+        {
+            std::lock_guard<std::mutex> g(h->mu);
+            set_device(h);
+            run_search(h, sl.dq.p, n, key.k, key.ef, allow, sl.dl.p, sl.dd.p, sl.dc.p, nullptr, sl.st,
+                       (key.flags & HNSWGPU_EXACT_TIES) != 0, key.precision, key.rerank, &term, false);
+        }
+        cuda_check(cudaMemcpyAsync(sl.hl.p, sl.dl.p, n * key.k * 8, cudaMemcpyDeviceToHost, sl.st),
+                   "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(sl.hd.p, sl.dd.p, n * key.k * 4, cudaMemcpyDeviceToHost, sl.st),
+                   "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(sl.hc.p, sl.dc.p, n * 4, cudaMemcpyDeviceToHost, sl.st), "cudaMemcpyAsync");
+        cuda_check(cudaEventRecord(sl.ev, sl.st), "cudaEventRecord");
+    } catch (...) {
+        lk.lock();
+        s->inflight_bytes -= sl.footprint;
+        if (sl.exact) s->exact_inflight = false;
+        sl.busy = false;
+        sl.tickets.clear();
+        s->inflight.pop_back();
+        throw;
+    }
+    lk.lock();
 }
 
 void finish(hnswgpu_server* s, Slot& sl, cudaError_t e) {
@@ -219,44 +251,49 @@ void fail_tickets(hnswgpu_server* s, const std::vector<uint64_t>& ids, int code,
     }
 }
 
-// Next batch: the oldest waiting request's configuration (skipping tie-exact
-// ones while one is in flight), all waiting requests of it up to max_batch
-// and the footprint left in the budget.
-bool try_launch(hnswgpu_server* s) {
+// Next batch: the configuration of the oldest waiting request (skipping
+// tie-exact ones while one is in flight), its waiting requests in arrival
+// order up to max_batch and the footprint left in the budget.  Costs one look
+// per configuration, however long the queues are.
+bool try_launch(hnswgpu_server* s, std::unique_lock<std::mutex>& lk) {
     Slot* free_slot = nullptr;
     for (auto& sl : s->slots)
         if (!sl->busy) {
             free_slot = sl.get();
             break;
         }
-    if (!free_slot || s->pending.empty()) return false;
-    for (size_t scan = 0; scan < s->pending.size(); scan++) {
-        const Key key = s->tickets[s->pending[scan]].key;
-        if ((key.flags & HNSWGPU_EXACT_TIES) && s->exact_inflight) continue;
-        const uint64_t fq = s->footprint[key];
-        const uint64_t room = s->budget > s->inflight_bytes ? (s->budget - s->inflight_bytes) / fq : 0;
-        if (room == 0) return false;  // wait for a batch to finish
-        const uint64_t cap = std::min<uint64_t>(room, s->o.max_batch);
-        std::vector<uint64_t> ids;
-        std::deque<uint64_t> rest;
-        for (size_t i = 0; i < s->pending.size(); i++) {
-            const uint64_t id = s->pending[i];
-            if (ids.size() < cap && i >= scan && s->tickets[id].key == key) ids.push_back(id);
-            else rest.push_back(id);
+    if (!free_slot || s->npending == 0) return false;
+    std::deque<uint64_t>* q = nullptr;
+    Key key{};
+    for (auto& kv : s->queues) {
+        if (kv.second.empty()) continue;
+        if ((kv.first.flags & HNSWGPU_EXACT_TIES) && s->exact_inflight) continue;
+        if (!q || kv.second.front() < q->front()) {
+            q = &kv.second;
+            key = kv.first;
         }
-        s->pending.swap(rest);
-        try {
-            launch(s, *free_slot, key, ids, fq);
-        } catch (const ApiError& e) {
-            fail_tickets(s, ids, e.code, e.what());
-            s->cv_done.notify_all();
-        } catch (const std::exception& e) {
-            fail_tickets(s, ids, HNSWGPU_ERR_NOMEM, e.what());
-            s->cv_done.notify_all();
-        }
-        return true;
     }
-    return false;
+    if (!q) return false;
+    const uint64_t fq = s->footprint[key];
+    const uint64_t room = s->budget > s->inflight_bytes ? (s->budget - s->inflight_bytes) / fq : 0;
+    if (room == 0) return false;  // wait for a batch to finish
+    const uint64_t cap = std::min<uint64_t>(room, s->o.max_batch);
+    std::vector<uint64_t> ids;
+    while (!q->empty() && ids.size() < cap) {
+        ids.push_back(q->front());
+        q->pop_front();
+    }
+    s->npending -= ids.size();
+    try {
+        launch(s, lk, *free_slot, key, ids, fq);
+    } catch (const ApiError& e) {
+        fail_tickets(s, ids, e.code, e.what());
+        s->cv_done.notify_all();
+    } catch (const std::exception& e) {
+        fail_tickets(s, ids, HNSWGPU_ERR_NOMEM, e.what());
+        s->cv_done.notify_all();
+    }
+    return true;
 }
 
 void worker_loop(hnswgpu_server* s) {
@@ -264,23 +301,30 @@ void worker_loop(hnswgpu_server* s) {
     std::unique_lock<std::mutex> lk(s->mu);
     while (true) {
         bool any_busy = false, progressed = false;
-        for (auto& sl : s->slots) {
-            if (!sl->busy) continue;
+        // Batches mostly finish in launch order: poll from the oldest and
+        // stop after two still running, so that a poll costs a few event
+        // queries, not one per slot.
+        int running = 0;
+        for (size_t i = 0; i < s->inflight.size() && running < 2;) {
+            Slot* sl = s->inflight[i];
             const cudaError_t e = cudaEventQuery(sl->ev);
             if (e == cudaErrorNotReady) {
-                any_busy = true;
+                running++;
+                i++;
                 continue;
             }
             finish(s, *sl, e);
+            s->inflight.erase(s->inflight.begin() + (std::ptrdiff_t)i);
             progressed = true;
         }
+        any_busy = !s->inflight.empty();
         if (progressed) s->cv_done.notify_all();
-        while (try_launch(s)) any_busy = true;
-        if (s->stop && s->pending.empty() && !any_busy) break;
+        while (try_launch(s, lk)) any_busy = true;
+        if (s->stop && s->npending == 0 && !any_busy) break;
         if (any_busy)
             s->cv_work.wait_for(lk, std::chrono::microseconds(10));
         else
-            s->cv_work.wait(lk, [&] { return s->stop || !s->pending.empty(); });
+            s->cv_work.wait(lk, [&] { return s->stop || s->npending != 0; });
     }
 }
 
@@ -307,7 +351,8 @@ uint64_t submit_locked(hnswgpu_server* s, const float* query, const hnswgpu_requ
     t.key = key;
     t.q.assign(query, query + s->h->dim);
     t.t0 = Clock::now();
-    s->pending.push_back(id);
+    s->queues[key].push_back(id);
+    s->npending++;
     s->submitted++;
     return id;
 }
@@ -331,10 +376,21 @@ int hnswgpu_server_create(hnswgpu_index* h, const hnswgpu_server_opts* opts, hns
         // default: the device's shared memory twice over (one wave running,
         // one queued behind it)
         s->budget = s->o.smem_budget ? s->o.smem_budget : 2ull * (uint64_t)h->num_sms * (uint64_t)smem_per_sm;
+        // staging sized up front for batches of up to 256 queries with k <= 100,
+        // so that serving rarely reallocates
+        const uint64_t pq = std::min<uint64_t>(s->o.max_batch, 256), pk = 100;
         for (uint32_t i = 0; i < s->o.max_inflight; i++) {
             auto sl = std::make_unique<Slot>();
             cuda_check(cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking), "cudaStreamCreate");
             cuda_check(cudaEventCreateWithFlags(&sl->ev, cudaEventDisableTiming), "cudaEventCreate");
+            sl->hq.ensure(pq * h->dim);
+            sl->hl.ensure(pq * pk);
+            sl->hd.ensure(pq * pk);
+            sl->hc.ensure(pq);
+            sl->dq.ensure(pq * h->dim);
+            sl->dl.ensure(pq * pk);
+            sl->dd.ensure(pq * pk);
+            sl->dc.ensure(pq);
             s->slots.push_back(std::move(sl));
         }
         hnswgpu_server* raw = s.release();
@@ -379,9 +435,10 @@ int hnswgpu_server_wait(hnswgpu_server* s, uint64_t ticket, uint64_t* labels, fl
         std::unique_lock<std::mutex> lk(s->mu);
         auto it = s->tickets.find(ticket);
         if (it == s->tickets.end()) return fail(HNSWGPU_ERR_ARG, "unknown ticket");
-        s->cv_done.wait(lk, [&] { return it->second.state >= kDone; });
-        Ticket t = std::move(it->second);
-        s->tickets.erase(it);
+        const Ticket* tp = &it->second;
+        s->cv_done.wait(lk, [&] { return tp->state >= kDone; });
+        Ticket t = std::move(s->tickets[ticket]);
+        s->tickets.erase(ticket);
         if (t.state == kFailed) return fail(t.err, t.msg);
         if (labels) std::memcpy(labels, t.labels.data(), t.labels.size() * 8);
         if (dists) std::memcpy(dists, t.dists.data(), t.dists.size() * 4);
@@ -425,9 +482,8 @@ int hnswgpu_server_replay(hnswgpu_server* s, const float* queries, uint64_t n, c
         }
         for (uint64_t i = 0; i < n; i++) {
             std::unique_lock<std::mutex> lk(s->mu);
-            auto it = s->tickets.find(ids[i]);
-            s->cv_done.wait(lk, [&] { return it->second.state >= kDone; });
-            Ticket& t = it->second;
+            Ticket& t = s->tickets.find(ids[i])->second;
+            s->cv_done.wait(lk, [&] { return t.state >= kDone; });
             if (t.state == kFailed && err == HNSWGPU_OK) {
                 err = t.err;
                 msg = t.msg;
@@ -438,7 +494,7 @@ int hnswgpu_server_replay(hnswgpu_server* s, const float* queries, uint64_t n, c
             }
             counts[i] = t.count;
             if (latency_us) latency_us[i] = t.latency_us;
-            s->tickets.erase(it);
+            s->tickets.erase(ids[i]);
         }
         if (err != HNSWGPU_OK) return fail(err, msg);
         return HNSWGPU_OK;
