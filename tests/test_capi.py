@@ -188,3 +188,32 @@ def test_tie_order_values():
     idx = H.Index("l2", 8)
     with pytest.raises(ValueError, match="tie_order"):
         idx.knn_query_traced(np.zeros((1, 8), np.float32), tie_order="heap")
+
+
+def test_tie_order_flags_reach_the_c_abi(monkeypatch):
+    """knn_query / knn_query_traced pass the tie order as flags: "reference"
+    (default) -> HNSWGPU_EXACT_TIES, "replay" -> EXACT_TIES | REPLAY_ALL,
+    "id" -> neither; low precision and the learned stop use the id order.
+    The search call is replaced by a recorder, so no GPU is needed."""
+    seen = []
+
+    class FakeLib:
+        def hnswgpu_search(self, h, q, nq, k, opts, labels, dists, counts):
+            o = opts._obj
+            seen.append(o.flags)
+            C.memset(counts, 0, 4 * nq)
+            return 0
+
+    monkeypatch.setattr(_capi, "lib", lambda: FakeLib())
+    idx = H.Index("l2", 8)
+    idx._h = C.c_void_p(1)  # never dereferenced by the recorder
+    try:
+        q = np.zeros((2, 8), np.float32)
+        for order, want in (("reference", _capi.EXACT_TIES), ("replay", _capi.EXACT_TIES | _capi.REPLAY_ALL),
+                            ("id", 0)):
+            idx.knn_query_traced(q, k=3, tie_order=order)
+            assert seen[-1] & (_capi.EXACT_TIES | _capi.REPLAY_ALL) == want, order
+        idx.knn_query_traced(q, k=3, tie_order="reference", precision="fp8")
+        assert seen[-1] & _capi.EXACT_TIES == 0
+    finally:
+        idx._h = None
