@@ -898,10 +898,19 @@ def run_reference(args, dist: Dist):
 
 
 class _Solo:
+    """Rank 0 alone, no process group (the reference arm and setup helpers);
+    `world` is the launch's rank count, which the reference arm reports."""
     rank = 0
+    local = 0
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
 
     def barrier(self):
         pass
+
+    def max(self, v: float) -> float:
+        return v
 
 
 def main():
