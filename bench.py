@@ -68,8 +68,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1_000_000)
-    ap.add_argument("--nq", type=int, default=10_000)
+    # --rows / --queries: the same, for launchers whose own options start with --n
+    ap.add_argument("--n", "--rows", dest="n", type=int, default=1_000_000)
+    ap.add_argument("--nq", "--queries", dest="nq", type=int, default=10_000)
     ap.add_argument("--ef", type=int, default=0, help="fixed ef (skip the sweep)")
     ap.add_argument("--target-recall", type=float, default=0.95)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -101,19 +102,28 @@ def parse():
 
 # ----------------------------------------------------------------- plumbing
 class Dist:
-    def __init__(self, n_gpus):
+    """One process per GPU (replicas: no data-path collective).  The process
+    group only times the run: a barrier around the timed region and the max
+    over ranks.  NCCL on GPUs; gloo when the backend is given as "gloo" (the
+    CPU tests of this plumbing)."""
+
+    def __init__(self, n_gpus, backend: str = "nccl", timeout_s: int = 600):
         self.rank = int(os.environ.get("RANK", "0"))
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
             self.pg = dist
 
     def barrier(self):
@@ -124,7 +134,8 @@ class Dist:
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
