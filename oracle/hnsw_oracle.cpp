@@ -312,9 +312,25 @@ using HeapQ = std::priority_queue<std::pair<float, uint32_t>, std::vector<std::p
 //      equals lowerBound (mode 1 forgets evicted candidates).
 // They are counted in Trace::ties; a query without tie events returns the
 // same result in both modes.
+//
+// With `es` (searchStopConditionClosest with an EpsilonSearchStopCondition,
+// hnswalg.h:1326-1377 and stop_condition.h:219-275) the loop is the
+// non-bare-bone one (searchBaseLayerST<false>) with ef = max_num_candidates:
+// the stop condition's item count is top_candidates' size, its
+// should_consider_candidate and should_remove_extra are the ef tests, and its
+// stop test adds "candidate beyond epsilon once min_num_candidates are held".
+struct EpsStop {
+    float eps;
+    size_t min_c, max_c;
+};
 std::vector<std::pair<float, uint32_t>> base_layer_reference(const Hnsw& h, uint32_t ep, const float* q, size_t ef,
                                                              bool bare, const uint8_t* allow,
-                                                             std::vector<uint32_t>& vis, uint32_t tag, Trace& tr) {
+                                                             std::vector<uint32_t>& vis, uint32_t tag, Trace& tr,
+                                                             const EpsStop* es = nullptr) {
+    if (es) {
+        ef = es->max_c;
+        bare = false;
+    }
     using P = std::pair<float, uint32_t>;
     CompareByFirst cmp;
     std::vector<P> top, cand;
@@ -350,6 +366,7 @@ std::vector<std::pair<float, uint32_t>> base_layer_reference(const Hnsw& h, uint
         P cp = cand.front();
         float cd = -cp.first;
         bool stop = bare ? (cd > lb) : (cd > lb && top.size() == ef);
+        if (es && cd > es->eps && top.size() >= es->min_c) stop = true;
         if (stop) break;
         if (cd == lb && !in_top.count(cp.second) && (bare || allowed(cp.second))) tr.ties++;
         pop(cand);
@@ -483,6 +500,38 @@ std::vector<Ent> base_layer_canonical(const Hnsw& h, uint32_t ep, const float* q
 struct SearchOut {
     std::vector<std::pair<float, uint64_t>> res;  // closest first
 };
+
+// searchStopConditionClosest with an EpsilonSearchStopCondition: the same
+// upper-layer descent, the loop above, then top_candidates popped into a
+// vector filled from the back (closest first; equal distances in the heap's
+// pop order) and filter_results: trailing entries beyond epsilon dropped,
+// then at most max_num_candidates kept.  The reference copies
+// top_candidates' (distance, internal id) pairs into its (distance, label)
+// result unchanged (hnswalg.h:1367-1371), so the second member is the
+// internal id; it equals the label when labels were assigned 0, 1, 2, ... in
+// insertion order.
+void search_epsilon(const Hnsw& h, const float* q, const EpsStop& es, const uint8_t* allow, std::vector<uint32_t>& vis,
+                    uint32_t& tag, SearchOut& out) {
+    out.res.clear();
+    if (h.cur == 0) return;
+    Trace tr;
+    uint32_t cur = descend(h, q, tr);
+    tag++;
+    if (tag == 0) { std::fill(vis.begin(), vis.end(), 0u); tag = 1; }
+    std::vector<std::pair<float, uint32_t>> top =
+        base_layer_reference(h, cur, q, es.max_c, false, allow, vis, tag, tr, &es);
+    CompareByFirst cmp;
+    std::vector<std::pair<float, uint64_t>> res(top.size());
+    size_t sz = top.size();
+    while (!top.empty()) {
+        res[--sz] = {top.front().first, (uint64_t)top.front().second};
+        std::pop_heap(top.begin(), top.end(), cmp);
+        top.pop_back();
+    }
+    while (!res.empty() && res.back().first > es.eps) res.pop_back();
+    while (res.size() > es.max_c) res.pop_back();
+    out.res = std::move(res);
+}
 
 void search_one(const Hnsw& h, const float* q, size_t k, size_t ef, int mode, const uint8_t* allow,
                 std::vector<uint32_t>& vis, uint32_t& tag, Trace& tr, SearchOut& out) {
@@ -699,6 +748,31 @@ int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t e
         }
     });
     if (failed) { g_err = "cand error"; return -1; }
+    return 0;
+}
+
+// Batched epsilon search (searchStopConditionClosest with
+// EpsilonSearchStopCondition).  Outputs max_c slots per query in the
+// reference's result order; counts[i] = results kept.
+int orc_hnsw_search_epsilon(void* p, const float* q, uint64_t nq, float eps, uint64_t min_c, uint64_t max_c,
+                            const uint8_t* allow, uint64_t* labels, float* dists, int32_t* counts, int nthreads) {
+    auto* h = (Hnsw*)p;
+    if (min_c > max_c || max_c == 0) { g_err = "need 0 < max_num_candidates and min <= max"; return -1; }
+    if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
+    std::vector<std::vector<uint32_t>> vis(nthreads, std::vector<uint32_t>());
+    std::vector<uint32_t> tags(nthreads, 0);
+    std::vector<SearchOut> outs(nthreads);
+    const EpsStop es{eps, (size_t)min_c, (size_t)max_c};
+    parallel_for(nq, nthreads, [&](size_t i, int t) {
+        if (vis[t].size() != h->cur) vis[t].assign(h->cur + 1, 0);
+        search_epsilon(*h, q + i * h->dim, es, allow, vis[t], tags[t], outs[t]);
+        auto& r = outs[t].res;
+        counts[i] = (int32_t)r.size();
+        for (size_t j = 0; j < max_c; j++) {
+            labels[i * max_c + j] = j < r.size() ? r[j].second : ~0ull;
+            dists[i * max_c + j] = j < r.size() ? r[j].first : std::numeric_limits<float>::infinity();
+        }
+    });
     return 0;
 }
 

@@ -65,6 +65,8 @@ def lib():
         L.orc_hnsw_set_deleted.argtypes = [P, U64, C.c_int]
         L.orc_hnsw_search.restype = C.c_int
         L.orc_hnsw_search.argtypes = [P, P, U64, U64, U64, C.c_int, P, P, P, P, P, C.c_int]
+        L.orc_hnsw_search_epsilon.restype = C.c_int
+        L.orc_hnsw_search_epsilon.argtypes = [P, P, U64, F32, U64, U64, P, P, P, P, C.c_int]
         L.orc_bf_load.restype = P
         L.orc_bf_load.argtypes = [C.c_char_p, C.c_int, U64]
         L.orc_bf_free.argtypes = [P]
@@ -145,6 +147,24 @@ class Hnsw:
             raise RuntimeError(lib().orc_last_error().decode())
         return (labels, dists, counts, tr) if trace else (labels, dists, counts)
 
+    def search_epsilon(self, q, epsilon, min_candidates, max_candidates, allow=None, nthreads=0):
+        """searchStopConditionClosest with EpsilonSearchStopCondition(epsilon,
+        min_candidates, max_candidates) per query: (ids, dists) of
+        max_candidates slots in the reference's result order, counts.  As in
+        the reference, the ids are internal ids, not labels."""
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        nq, m = q.shape[0], int(max_candidates)
+        labels = np.empty((nq, m), np.uint64)
+        dists = np.empty((nq, m), np.float32)
+        counts = np.empty(nq, np.int32)
+        if allow is not None:
+            allow = np.ascontiguousarray(allow, np.uint8)
+        rc = lib().orc_hnsw_search_epsilon(self._h, _ptr(q), nq, float(epsilon), int(min_candidates), m, _ptr(allow),
+                                           _ptr(labels), _ptr(dists), _ptr(counts), nthreads)
+        if rc != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return labels, dists, counts
+
 
 class Bf:
     """A reference-format brute-force index file loaded by the oracle."""
@@ -183,6 +203,37 @@ def bf_matrix(space: str, x: np.ndarray, q: np.ndarray, k: int, nthreads: int = 
     lib().orc_bf_matrix(SPACES[space], _ptr(x), x.shape[0], x.shape[1], _ptr(q), q.shape[0], k, _ptr(labels),
                         _ptr(dists), nthreads)
     return labels, dists
+
+
+def ref_stopcond():
+    """ctypes handle of oracle/_ref/libref_stopcond.so (the reference's own
+    searchStopConditionClosest), or None where it was not built."""
+    path = os.path.join(HERE, "_ref", "libref_stopcond.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    P, U64 = C.c_void_p, C.c_uint64
+    L.ref_epsilon_search.restype = C.c_int
+    L.ref_epsilon_search.argtypes = [C.c_char_p, C.c_int, U64, P, U64, P, U64, P, U64, C.c_float, U64, U64, P, P, P]
+    return L
+
+
+def ref_epsilon_search(path, space, q, epsilon, min_candidates, max_candidates, deleted=(), allow_by_label=None):
+    """Run the reference's epsilon search (needs ref_stopcond())."""
+    L = ref_stopcond()
+    q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+    nq, dim, m = q.shape[0], q.shape[1], int(max_candidates)
+    dele = np.ascontiguousarray(np.asarray(deleted, np.uint64))
+    labels = np.empty((nq, m), np.uint64)
+    dists = np.empty((nq, m), np.float32)
+    counts = np.empty(nq, np.int32)
+    allow = None if allow_by_label is None else np.ascontiguousarray(allow_by_label, np.uint8)
+    rc = L.ref_epsilon_search(str(path).encode(), SPACES[space], dim, _ptr(dele), dele.size, _ptr(allow),
+                              0 if allow is None else allow.size, _ptr(q), nq, float(epsilon), int(min_candidates), m,
+                              _ptr(labels), _ptr(dists), _ptr(counts))
+    if rc != 0:
+        raise RuntimeError("reference epsilon search failed")
+    return labels, dists, counts
 
 
 def ref_module():

@@ -187,3 +187,64 @@ def test_listing_rule_covers_every_divergence(tmp_path):
             total += len(qs)
     assert differ_total > 0  # the data does steer the heaps
     assert listed < total
+
+
+def _epsilon_cases():
+    e = np.load(f"{GOLDEN}/epsilon.npz")
+    names = sorted({k.rsplit("/", 1)[0] for k in e.keys()})
+    return e, names
+
+
+def test_oracle_epsilon_search_matches_golden():
+    """The oracle's searchStopConditionClosest (EpsilonSearchStopCondition)
+    against the reference's own outputs recorded in tests/golden/epsilon.npz:
+    labels, distances, result order (equal distances in the reference's heap
+    pop order) and counts, bit-exact; with a filter and with deletions."""
+    g = golden()
+    e, names = _epsilon_cases()
+    spaces = {"hnsw_l2_d16": ("l2", 16), "hnsw_ip_d20": ("ip", 20), "hnsw_l2_d7_int": ("l2", 7)}
+    for key in names:
+        name, _, variant = key.split("/")
+        space, dim = spaces[name]
+        o = O.Hnsw(f"{GOLDEN}/{name}.bin", space, dim)
+        labels = o.labels()
+        allow = None
+        if variant == "even":
+            allow = (labels % 2 == 0).astype(np.uint8)
+        if variant == "del":
+            for lab in g[f"{name}/deleted"]:
+                assert o.set_deleted(int(lab), True) == 0
+        eps, mn, mx = e[key + "/params"]
+        ol, od, oc = o.search_epsilon(g[f"{name}/queries"], np.float32(eps), int(mn), int(mx), allow=allow)
+        assert np.array_equal(oc, e[key + "/counts"]), key
+        assert np.array_equal(ol, e[key + "/labels"]), key
+        assert np.array_equal(od.view(np.uint32), e[key + "/dists"].view(np.uint32)), key
+
+
+def test_oracle_epsilon_search_vs_reference_fresh(tmp_path):
+    """Fresh indexes against the live reference harness (skipped where it was
+    not built): uniform L2, inner product and small-integer L2 with ties."""
+    if O.ref_stopcond() is None:
+        pytest.skip("oracle/_ref/libref_stopcond.so not built")
+    rng = np.random.default_rng(21)
+    for space, dim, kind in (("l2", 24, "u"), ("ip", 32, "n"), ("l2", 8, "i")):
+        if kind == "u":
+            x = rng.random((2500, dim), dtype=np.float32)
+            q = rng.random((60, dim), dtype=np.float32)
+        elif kind == "n":
+            x = rng.standard_normal((2500, dim), dtype=np.float32)
+            q = rng.standard_normal((60, dim), dtype=np.float32)
+        else:
+            x = rng.integers(0, 5, (2500, dim)).astype(np.float32)
+            q = rng.integers(0, 5, (60, dim)).astype(np.float32)
+        path = tmp_path / f"{space}{dim}.bin"
+        build_hnsw(path, x, space, M=12, efc=80)
+        o = O.Hnsw(str(path), space, dim)
+        ex = np.stack([O.distances(space, q[i], x) for i in range(q.shape[0])])
+        for quant, mn, mx in ((0.01, 10, 48), (0.05, 40, 200), (0.2, 0, 150)):
+            eps = np.float32(np.quantile(ex, quant))
+            rl, rd, rc = O.ref_epsilon_search(path, space, q, eps, mn, mx)
+            ol, od, oc = o.search_epsilon(q, eps, mn, mx)
+            assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
+            assert np.array_equal(od.view(np.uint32), rd.view(np.uint32))
+            assert all(np.all(od[i, :oc[i]] <= eps) for i in range(q.shape[0]))
