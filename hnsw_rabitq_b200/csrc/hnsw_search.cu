@@ -1034,7 +1034,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     int tsz = 0, csz = 0;               // tie-exact mode: heap sizes (warp-uniform)
     const uint64_t sentinel = mkkey(__int_as_float(0x7f7fffff), cur);
     // FILTER kernels run the id order only (the host never pairs it with EXACT)
-    const bool pipe = FAST16 && (bare || FILTER) && p.maxM0 <= 32;
+    const bool pipe = FAST16 && (bare || FILTER) && p.maxM0 <= 32 && !p.eps_mode;
     float qn = 0.f;
     if (TERM) {  // |q|^2, a feature of the termination network
         for (uint32_t i = lane; i < p.dim; i += 32) qn = fmaf(s.q[i], s.q[i], qn);
@@ -1106,7 +1106,10 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         if (csz == 0) break;
         const uint64_t c = s.candheap[0];
         const uint32_t lbk = psize > 0 ? khi(s.pool[psize - 1]) : fkey(__int_as_float(0x7f7fffff));
-        const bool stop = bare ? (khi(c) > lbk) : (khi(c) > lbk && psize == (int)ef);
+        bool stop = bare ? (khi(c) > lbk) : (khi(c) > lbk && psize == (int)ef);
+        // EpsilonSearchStopCondition::should_stop_search (stop_condition.h:242-253):
+        // its item count is top_candidates' size, which the pool mirrors here
+        if (p.eps_mode && khi(c) > fkey(p.eps) && psize >= (int)p.eps_min) stop = true;
         if (stop) break;
         __syncwarp();
         if (lane == 0) {
@@ -1262,6 +1265,35 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
     }  // general loop
 
     const uint32_t k = p.k;
+    if (EXACT && p.eps_mode) {
+        // searchStopConditionClosest (hnswalg.h:1365-1374): top_candidates
+        // popped into the result from its back (closest first, equal
+        // distances in the heap's pop order), then filter_results drops the
+        // trailing entries beyond epsilon.  The result carries internal ids,
+        // as the reference's does.
+        int tn = tsz;
+        if (lane == 0)
+            for (int i = tn - 1; i >= 0; i--) s.pool[i] = ref_heap_pop(s.topheap, tn, TopLess());
+        __syncwarp();
+        const uint32_t ek = fkey(p.eps);
+        int cnt = 0;
+        for (int base = 0; base < tsz; base += 32) {
+            const int i = base + lane;
+            cnt += __popc(__ballot_sync(FULL, i < tsz && khi(s.pool[i]) <= ek));
+        }
+        cnt = min(cnt, (int)k);
+        uint64_t* oid = p.out_labels + (size_t)qi * k;
+        float* odist = p.out_dists + (size_t)qi * k;
+        for (int r = lane; r < (int)k; r += 32) {
+            oid[r] = r < cnt ? (uint64_t)kid(s.pool[r]) : ~0ull;
+            odist[r] = r < cnt ? funkey(khi(s.pool[r])) : __int_as_float(0x7f800000);
+        }
+        if (lane == 0) {
+            p.out_counts[qi] = cnt;
+            if (status) atomicOr(p.status, status);
+        }
+        return true;
+    }
     if (EXACT) {
         // the reference pops top_candidates down to k (hnswalg.h:1314-1316);
         // keep in the pool exactly the entries left in the heap

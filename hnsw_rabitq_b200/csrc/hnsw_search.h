@@ -81,6 +81,11 @@ struct SearchParams {
     uint32_t fast16;              // dim % 16 == 0: 4-lanes-per-row distance path
     uint32_t links_unique;        // no level-0 list repeats an id (checked at load)
     uint32_t exact;               // replay the reference's heaps (tie order exact)
+    // epsilon search (searchStopConditionClosest with EpsilonSearchStopCondition;
+    // tie-exact general loop only): k = ef = max_num_candidates
+    uint32_t eps_mode;            // 1: stop once a candidate lies beyond eps with eps_min items held
+    float eps;                    // epsilon (a distance, squared for L2)
+    uint32_t eps_min;             // min_num_candidates
     uint32_t pool_cap;            // ef (canonical) or ef + 32 (tie-exact)
     uint32_t cand_cap;            // tie-exact: candidate heap entries in shared memory
     uint32_t cand_spill_cap;      // tie-exact: further entries per warp in cand_spill

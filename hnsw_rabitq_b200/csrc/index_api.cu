@@ -486,6 +486,19 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
     }
 }
 
+// Global tails of the tie-exact candidate heaps, one per resident warp (at
+// most 32 CTAs per SM), owned by the index.
+static void attach_spill(hnswgpu_index* h, hnswgpu::SearchParams& p, cudaStream_t st) {
+    const uint64_t warps = (uint64_t)h->num_sms * 32u * hnswgpu::kWarpsPerBlock;
+    const uint64_t need = warps * p.cand_spill_cap;
+    if (h->cand_spill.n < need) {
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        h->cand_spill.alloc(need);
+    }
+    p.cand_spill = h->cand_spill.p;
+    p.cand_spill_warps = (uint32_t)warps;
+}
+
 static void take_counter_slot(hnswgpu_index* h, hnswgpu::SearchParams& p) {
     const uint32_t slot = h->next_counter++ % (uint32_t)(h->counters.n / 2);
     p.work_counter = h->counters.p + 2 * slot;
@@ -565,17 +578,7 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
             h->tie_pending_nq = nq;
         }
     }
-    if (exact) {
-        // one tail per resident warp: at most 32 CTAs per SM
-        const uint64_t warps = (uint64_t)h->num_sms * 32u * hnswgpu::kWarpsPerBlock;
-        const uint64_t need = warps * p.cand_spill_cap;
-        if (h->cand_spill.n < need) {
-            cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-            h->cand_spill.alloc(need);
-        }
-        p.cand_spill = h->cand_spill.p;
-        p.cand_spill_warps = (uint32_t)warps;
-    }
+    if (exact) attach_spill(h, p, st);
 #ifdef HNSWGPU_PHASE_TIMING
     static unsigned long long* phase_buf = nullptr;
     if (!phase_buf) {
@@ -587,6 +590,36 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
 #endif
     take_counter_slot(h, p);
     cuda_check(hnswgpu::launch_hnsw_search(p, space, h->num_sms, st, nullptr), "hnsw_search launch");
+}
+
+// Epsilon search of a batch on device buffers: searchStopConditionClosest
+// with EpsilonSearchStopCondition(eps, min_c, max_c), the tie-exact general
+// loop with ef = k = max_c (hnswalg.h:1326-1377, stop_condition.h:219-275).
+void run_epsilon(hnswgpu_index* h, const float* dq, uint64_t nq, float eps, uint64_t min_c, uint64_t max_c,
+                 const uint8_t* dallow, uint64_t* dl, float* dd, int32_t* dc, cudaStream_t st) {
+    hnswgpu::SearchParams p = hnsw_params(h, dq, nq, max_c, max_c, dallow, dl, dd, dc, nullptr, true, 0, 0, true);
+    if (!p.bare) {
+        // Until min_num_candidates allowed results are held the loop accepts
+        // every neighbour, so a selective filter queues many disallowed
+        // candidates: give their list room for up to 2048 (or the index)
+        // where shared memory allows.
+        const uint32_t want = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(2048, 4ull * p.ef), h->count + 1);
+        if (want > p.extra_cap) {
+            hnswgpu::SearchParams wider = p;
+            wider.extra_cap = want;
+            int max_optin = 0;
+            cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+            if (hnswgpu::warp_smem_layout(wider) * hnswgpu::kWarpsPerBlock <= (size_t)max_optin) p = wider;
+        }
+    }
+    p.eps_mode = 1;
+    p.eps = eps;
+    p.eps_min = (uint32_t)min_c;
+    p.status = h->status.p;
+    attach_spill(h, p, st);
+    take_counter_slot(h, p);
+    cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
+               "hnsw_search launch");
 }
 
 // Exact brute force of a batch on device buffers (bf_search.cu).
@@ -996,6 +1029,77 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         if (dt) cuda_check(cudaMemcpyAsync(o.trace, dt, tb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        uint32_t status = 0;
+        cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (status & HNSWGPU_STATUS_TIMEOUT) {
+            cudaMemsetAsync(h->status.p, 0, 4, st);
+            cudaStreamSynchronize(st);
+            return fail(HNSWGPU_ERR_KERNEL, "search kernel timed out waiting for a copy");
+        }
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_search_epsilon(hnswgpu_index* h, const float* queries, uint64_t nq, float epsilon,
+                           uint64_t min_candidates, uint64_t max_candidates, const hnswgpu_search_opts* opts,
+                           uint64_t* out_ids, float* out_dists, int32_t* out_counts) {
+    return guarded([&] {
+        if (!h || h->is_bf || (nq && (!queries || !out_ids || !out_dists || !out_counts)))
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (max_candidates == 0 || min_candidates > max_candidates)
+            return fail(HNSWGPU_ERR_ARG, "need 0 < max_num_candidates and min_num_candidates <= max_num_candidates");
+        if (std::isnan(epsilon)) return fail(HNSWGPU_ERR_ARG, "epsilon is NaN");
+        if (nq > 0xffffffffull || max_candidates > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "batch too large");
+        hnswgpu_search_opts o{};
+        if (opts) o = *opts;
+        if ((o.flags & ~(uint32_t)HNSWGPU_DEVICE_PTRS) || o.precision)
+            return fail(HNSWGPU_ERR_UNSUPPORTED,
+                        "epsilon search: only HNSWGPU_DEVICE_PTRS may be set, float32 only (it always replays the "
+                        "reference's heaps)");
+        const bool dev = (o.flags & HNSWGPU_DEVICE_PTRS) != 0;
+        const uint64_t m = max_candidates;
+        cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (nq == 0) return HNSWGPU_OK;
+        if (h->count == 0) {
+            if (dev) {
+                cuda_check(cudaMemsetAsync(out_counts, 0, nq * 4, st), "cudaMemsetAsync");
+                cuda_check(cudaMemsetAsync(out_ids, 0xff, nq * m * 8, st), "cudaMemsetAsync");
+                cuda_check(cudaMemsetAsync(out_dists, 0x7f, nq * m * 4, st), "cudaMemsetAsync");
+            } else {
+                memset(out_counts, 0, nq * 4);
+                for (uint64_t i = 0; i < nq * m; i++) {
+                    out_ids[i] = ~0ull;
+                    out_dists[i] = __builtin_inff();
+                }
+            }
+            return HNSWGPU_OK;
+        }
+        if (dev) {
+            run_epsilon(h, queries, nq, epsilon, min_candidates, m, o.allow, out_ids, out_dists, out_counts, st);
+            return HNSWGPU_OK;
+        }
+        const size_t qb = nq * h->dim * 4, lb = nq * m * 8, db = nq * m * 4, cb = nq * 4;
+        auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+        h->io.ensure(al(qb) + al(lb) + al(db) + al(cb));
+        unsigned char* base = h->io.p;
+        float* dq = (float*)base;
+        uint64_t* dl = (uint64_t*)(base + al(qb));
+        float* dd = (float*)(base + al(qb) + al(lb));
+        int32_t* dc = (int32_t*)(base + al(qb) + al(lb) + al(db));
+        const uint8_t* dallow = nullptr;
+        if (o.allow) {
+            h->allow.ensure(h->count);
+            cuda_check(cudaMemcpyAsync(h->allow.p, o.allow, h->count, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+            dallow = h->allow.p;
+        }
+        cuda_check(cudaMemcpyAsync(dq, queries, qb, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+        run_epsilon(h, dq, nq, epsilon, min_candidates, m, dallow, dl, dd, dc, st);
+        cuda_check(cudaMemcpyAsync(out_ids, dl, lb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_dists, dd, db, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_counts, dc, cb, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         uint32_t status = 0;
         cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
         cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");

@@ -286,6 +286,28 @@ class Index(_GpuIndex):
             _ptr(out["ids"]), _ptr(out["nckpt"]), _ptr(out["labels"]), _ptr(out["dists"]), _ptr(out["counts"])))
         return out
 
+    def search_epsilon(self, data, epsilon: float, min_candidates: int, max_candidates: int,
+                       filter: Optional[Callable[[int], bool]] = None):
+        """The C++ API's searchStopConditionClosest with an
+        EpsilonSearchStopCondition(epsilon, min_candidates, max_candidates)
+        (hnswalg.h:1326-1377), per query: (ids uint64 [N, max_candidates],
+        distances float32 [N, max_candidates], counts int32 [N]), closest
+        first in the reference's result order.  As in the reference, the ids
+        are internal ids (labels_by_internal_id() maps them to labels)."""
+        q, _ = self._queries(data, 1)
+        nq, m = q.shape[0], int(max_candidates)
+        if m <= 0 or int(min_candidates) < 0 or int(min_candidates) > m:
+            raise RuntimeError("need 0 < max_candidates and 0 <= min_candidates <= max_candidates")
+        ids = np.empty((nq, m), np.uint64)
+        dists = np.empty((nq, m), np.float32)
+        counts = np.empty(nq, np.int32)
+        opts = _capi.SearchOpts()
+        mask = self._allow_mask(filter)
+        opts.allow = mask.ctypes.data if mask is not None else None
+        _capi.check(_capi.lib().hnswgpu_search_epsilon(self._h, _ptr(q), nq, float(epsilon), int(min_candidates), m,
+                                                       C.byref(opts), _ptr(ids), _ptr(dists), _ptr(counts)))
+        return ids, dists, counts
+
     def knn_query_exact(self, data, k: int = 1, filter: Optional[Callable[[int], bool]] = None):
         """Exact k-NN by an exhaustive GPU scan of the index's vectors (the
         ground truth of recall measurements): (labels, distances)."""

@@ -204,6 +204,24 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
                    const hnswgpu_search_opts* opts, uint64_t* out_labels, float* out_dists,
                    int32_t* out_counts);
 
+/* Replaces HierarchicalNSW::searchStopConditionClosest with an
+ * EpsilonSearchStopCondition(epsilon, min_candidates, max_candidates)
+ * (hnswlib/hnswalg.h:1326-1377, hnswlib/stop_condition.h:219-275): every
+ * query's beam runs with ef = max_candidates and also stops at a candidate
+ * beyond epsilon once min_candidates results are held; the results within
+ * epsilon are returned.  epsilon is a distance (squared for L2).  Outputs:
+ * nq x max_candidates ids and distances in the reference's result order
+ * (closest first; equal distances in the order its heap pops them), counts[i]
+ * = results kept, unused slots UINT64_MAX / +inf.  As in the reference, the
+ * ids are INTERNAL ids (searchStopConditionClosest copies top_candidates'
+ * internal ids into its result); they equal the labels when labels were
+ * assigned 0, 1, 2, ... in insertion order.  Always the reference's heap
+ * order.  opts: only HNSWGPU_DEVICE_PTRS, `allow` and `stream` apply. */
+HNSWGPU_API int hnswgpu_search_epsilon(hnswgpu_index* index, const float* queries, uint64_t nq, float epsilon,
+                                       uint64_t min_candidates, uint64_t max_candidates,
+                                       const hnswgpu_search_opts* opts, uint64_t* out_ids, float* out_dists,
+                                       int32_t* out_counts);
+
 /* HNSW search that allocates no memory, for callers that cannot call
  * cudaMalloc: code running under a device-memory budget it does not own (a
  * framework's caching allocator or a serving process that reserves all of its

@@ -38,6 +38,24 @@ class BaseFilterFunctor {
     virtual ~BaseFilterFunctor() {}
 };
 
+// The parameters of hnswlib::EpsilonSearchStopCondition
+// (hnswlib/stop_condition.h:219-233); the search itself runs on the GPU.
+class EpsilonSearchStopCondition {
+ public:
+    EpsilonSearchStopCondition(float epsilon, size_t min_num_candidates, size_t max_num_candidates)
+        : eps_(epsilon), min_(min_num_candidates), max_(max_num_candidates) {
+        if (min_num_candidates > max_num_candidates)
+            throw std::runtime_error("min_num_candidates must not exceed max_num_candidates");
+    }
+    float epsilon() const { return eps_; }
+    size_t min_num_candidates() const { return min_; }
+    size_t max_num_candidates() const { return max_; }
+
+ private:
+    float eps_;
+    size_t min_, max_;
+};
+
 class SpaceInterface {
  public:
     virtual int space_kind() const = 0;
@@ -174,6 +192,27 @@ class HierarchicalNSW : public detail::IndexBase {
     }
 
     void setEf(size_t ef) { detail::check(hnswgpu_set_ef(h_, ef)); }
+
+    // searchStopConditionClosest with an EpsilonSearchStopCondition
+    // (hnswlib/hnswalg.h:1326-1377): the results within epsilon, closest
+    // first, in the reference's order; like the reference, the second member
+    // is the internal id.
+    std::vector<std::pair<float, labeltype>> searchStopConditionClosest(const void* query,
+                                                                        const EpsilonSearchStopCondition& sc,
+                                                                        BaseFilterFunctor* f = nullptr) const {
+        std::vector<uint8_t> m = mask(f);
+        hnswgpu_search_opts o{};
+        o.allow = f ? m.data() : nullptr;
+        const size_t cap = sc.max_num_candidates();
+        std::vector<uint64_t> ids(cap);
+        std::vector<float> d(cap);
+        int32_t c = 0;
+        detail::check(hnswgpu_search_epsilon(h_, static_cast<const float*>(query), 1, sc.epsilon(),
+                                             sc.min_num_candidates(), cap, &o, ids.data(), d.data(), &c));
+        std::vector<std::pair<float, labeltype>> r((size_t)c);
+        for (int32_t i = 0; i < c; i++) r[(size_t)i] = {d[(size_t)i], (labeltype)ids[(size_t)i]};
+        return r;
+    }
     size_t getEf() const {
         hnswgpu_info info;
         detail::check(hnswgpu_get_info(h_, &info));

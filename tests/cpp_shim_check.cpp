@@ -3,7 +3,11 @@
 // tests/cpp/searchKnnWithFilter_test.cpp): prints the closest-first results
 // of searchKnn for every query so the Python side can compare them with the
 // reference's recorded outputs, and checks closer-first ordering, filter
-// functors and delete marks.  Usage: cpp_shim_check index.bin queries.f32 dim nq k ef
+// functors and delete marks.  With three more arguments it then prints a line
+// "EPS" and, per query, searchStopConditionClosest's results for an
+// EpsilonSearchStopCondition(eps, min, max) (tests/cpp/epsilon_search_test.cpp
+// drives the reference the same way).
+// Usage: cpp_shim_check index.bin queries.f32 dim nq k ef [eps min max]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -20,7 +24,7 @@ struct PickDivisible : public hnswgpu::BaseFilterFunctor {
 };
 
 int main(int argc, char** argv) {
-    if (argc != 7) return 2;
+    if (argc != 7 && argc != 10) return 2;
     const char* path = argv[1];
     size_t dim = atoi(argv[3]), nq = atoi(argv[4]), k = atoi(argv[5]), ef = atoi(argv[6]);
     std::vector<float> q(nq * dim);
@@ -41,6 +45,18 @@ int main(int argc, char** argv) {
         }
         for (auto& r : cf) printf("%llu %.9g ", (unsigned long long)r.second, r.first);
         printf("\n");
+    }
+    if (argc == 10) {
+        hnswgpu::EpsilonSearchStopCondition sc((float)atof(argv[7]), atoi(argv[8]), atoi(argv[9]));
+        printf("EPS\n");
+        for (size_t i = 0; i < nq; i++) {
+            auto r = alg->searchStopConditionClosest(q.data() + i * dim, sc);
+            for (size_t j = 0; j < r.size(); j++) {
+                if (r[j].first > sc.epsilon() || (j && r[j].first < r[j - 1].first)) return 13;
+                printf("%llu %.9g ", (unsigned long long)r[j].second, r[j].first);
+            }
+            printf("\n");
+        }
     }
     PickNothing none;
     if (!alg->searchKnn(q.data(), k, &none).empty()) return 6;

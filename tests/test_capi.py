@@ -151,6 +151,8 @@ def test_newer_entry_points_reject_bad_arguments():
     assert lib.hnswgpu_server_get_stats(None, C.byref(st), 0) == _capi.ERR_ARG
     assert lib.hnswgpu_server_destroy(None) == _capi.ERR_ARG
     assert lib.hnswgpu_build_traversal_copy(None, 2) == _capi.ERR_ARG
+    assert lib.hnswgpu_search_epsilon(None, None, 1, C.c_float(1.0), 1, 4, C.byref(opts), None, None,
+                                      None) == _capi.ERR_ARG
     assert lib.hnswgpu_last_error() != b""
 
 
