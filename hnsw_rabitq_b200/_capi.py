@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libhnswgpu.so")
 OK = 0
 ERR_ARG, ERR_IO, ERR_FORMAT, ERR_CUDA, ERR_NOMEM, ERR_LABEL, ERR_STATE, ERR_KERNEL, ERR_UNSUPPORTED = \
     -1, -2, -3, -4, -5, -6, -7, -8, -9
-SPACE_L2, SPACE_IP, SPACE_COSINE = 0, 1, 2
+SPACE_L2, SPACE_IP, SPACE_COSINE, SPACE_L2_UINT8 = 0, 1, 2, 3
 DEVICE_PTRS = 0x1
 TRACE = 0x2
 EXACT_TIES = 0x4

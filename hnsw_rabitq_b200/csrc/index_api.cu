@@ -130,7 +130,12 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
     in.clear();
     // layout consistency the kernels rely on
     const uint64_t size_links0 = maxM0 * 4 + 4, size_links = maxM * 4 + 4;
-    if (offsetLevel0 != 0 || offsetData != size_links0 || label_offset != offsetData + dim * 4 ||
+    // bytes per stored element: float32, or uint8 for L2SpaceI
+    const uint64_t elem = space == HNSWGPU_SPACE_L2_UINT8 ? 1 : 4;
+    if (space == HNSWGPU_SPACE_L2_UINT8 && dim * 65025ull >= (1ull << 24))
+        throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
+                       "uint8 L2 needs dim <= 258 (integer distances exact in float32)");
+    if (offsetLevel0 != 0 || offsetData != size_links0 || label_offset != offsetData + dim * elem ||
         size_data != label_offset + 8)
         throw ApiError(HNSWGPU_ERR_FORMAT,
                        "index layout does not match dim=" + std::to_string(dim) + " (" + corrupt + ")");
@@ -181,7 +186,12 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
                 h->deleted[i >> 5] |= 1u << (i & 31);
                 h->num_deleted++;
             }
-            memcpy(&hv[i * h->row_floats], rec + offsetData, dim * 4);
+            if (elem == 1) {
+                const unsigned char* u = reinterpret_cast<const unsigned char*>(rec + offsetData);
+                for (uint64_t c = 0; c < dim; c++) hv[i * h->row_floats + c] = (float)u[c];
+            } else {
+                memcpy(&hv[i * h->row_floats], rec + offsetData, dim * 4);
+            }
             uint64_t lab;
             memcpy(&lab, rec + label_offset, 8);
             h->labels[i] = lab;
@@ -537,7 +547,7 @@ void run_hnsw(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint64
     hnswgpu::SearchParams p = hnsw_params(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, exact, prec, rerank, true);
     apply_term(h, p, term);
     p.status = h->status.p;
-    const int space = h->space == HNSWGPU_SPACE_L2 ? 0 : 1;
+    const int space = kspace(h);
     hnswgpu::SearchParams p1{};
     bool two_pass = exact && !replay_all && p.fast16 && p.bare && p.maxM0 <= 32;
     if (two_pass) {
@@ -618,7 +628,7 @@ void run_epsilon(hnswgpu_index* h, const float* dq, uint64_t nq, float eps, uint
     p.status = h->status.p;
     attach_spill(h, p, st);
     take_counter_slot(h, p);
-    cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
+    cuda_check(hnswgpu::launch_hnsw_search(p, kspace(h), h->num_sms, st, nullptr),
                "hnsw_search launch");
 }
 
@@ -640,7 +650,7 @@ static void run_bf_exact(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_
     b.out_dists = dd;
     b.out_counts = dc;
     b.status = h->status.p;
-    cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st), "bf_search launch");
+    cuda_check(hnswgpu::launch_bf_search(b, kspace(h), h->num_sms, st), "bf_search launch");
 }
 
 static uint32_t pow2_at_least(uint64_t v) {
@@ -699,7 +709,7 @@ void run_bf_tc(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint3
     CUtensorMap qmap, xmap, smap;
     cuda_check(hnswgpu::tc_encode_map(h->tc_qt.p, prec, nq, dim, trow, 128, &qmap), "tensor map (queries)");
     cuda_check(hnswgpu::tc_encode_map(h->tcopy[prec].p, prec, n, dim, trow, 256, &xmap), "tensor map (rows)");
-    const int space = h->space == HNSWGPU_SPACE_L2 ? 0 : 1;
+    const int space = kspace(h);
     hnswgpu::TcArgs a{};
     a.nq = (uint32_t)nq;
     a.k_blocks = (dim * (prec == 1 ? 2u : 1u) + 127) / 128;
@@ -824,7 +834,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
         b.out_dists = dd;
         b.out_counts = dc;
         b.status = h->status.p;
-        cuda_check(hnswgpu::launch_bf_search(b, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st),
+        cuda_check(hnswgpu::launch_bf_search(b, kspace(h), h->num_sms, st),
                    "bf_search launch");
     } else {
         run_hnsw(h, dq, nq, k, ef, dallow, dl, dd, dc, dtrace, st, exact, prec, rerank, term, replay_all);
@@ -849,7 +859,7 @@ int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_el
                       hnswgpu_index** out) {
     return guarded([&] {
         if (!path || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
-        if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
+        if (space < 0 || space > 3) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
         *out = nullptr;
         std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
         init_common(h.get(), device);
@@ -862,6 +872,8 @@ int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_el
 int hnswgpu_load_bf(const char* path, int space, uint64_t dim, int device, hnswgpu_index** out) {
     return guarded([&] {
         if (!path || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space == HNSWGPU_SPACE_L2_UINT8)
+            return fail(HNSWGPU_ERR_UNSUPPORTED, "uint8 L2 (L2SpaceI) is supported for HNSW indexes only");
         if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
         *out = nullptr;
         std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
@@ -876,6 +888,8 @@ int hnswgpu_create_bf(int space, uint64_t dim, const float* data, const uint64_t
                       uint64_t max_elements, int device, hnswgpu_index** out) {
     return guarded([&] {
         if (!out || dim == 0 || (n && (!data || !labels))) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space == HNSWGPU_SPACE_L2_UINT8)
+            return fail(HNSWGPU_ERR_UNSUPPORTED, "uint8 L2 (L2SpaceI) is supported for HNSW indexes only");
         if (space < 0 || space > 2) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
         *out = nullptr;
         std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
@@ -1144,7 +1158,7 @@ int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint6
         // counters and status must start at zero: clear what a previous call
         // (or an interrupted one) may have left
         cuda_check(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), st), "cudaMemsetAsync");
-        cuda_check(hnswgpu::launch_hnsw_search(p, h->space == HNSWGPU_SPACE_L2 ? 0 : 1, h->num_sms, st, nullptr),
+        cuda_check(hnswgpu::launch_hnsw_search(p, kspace(h), h->num_sms, st, nullptr),
                    "hnsw_search launch");
         return HNSWGPU_OK;
     });
@@ -1172,7 +1186,7 @@ int hnswgpu_fp64_distances(hnswgpu_index* h, const float* queries, uint64_t nq, 
         cuda_check(cudaMemcpyAsync(dq.p, queries, nq * h->dim * 4, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
         cuda_check(cudaMemcpyAsync(dr.p, rows.data(), nq * m * 4, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
         cuda_check(hnswgpu::launch_fp64_distances(dq.p, nq, (uint32_t)m, (uint32_t)h->dim, h->vecs.p, h->row_floats, dr.p,
-                                                  h->space == HNSWGPU_SPACE_L2 ? 0 : 1,
+                                                  kspace(h),
                                                   h->space == HNSWGPU_SPACE_COSINE ? 1 : 0, dout.p, h->stream),
                    "fp64 distance launch");
         cuda_check(cudaMemcpyAsync(out, dout.p, nq * m * 8, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");

@@ -122,6 +122,12 @@ struct hnswgpu_index {
 
 namespace hnswgpu_host {
 
+// Kernel distance family of an index: 0 = squared L2 (float32 rows, or the
+// uint8 rows of L2SpaceI widened exactly to float32), 1 = inner product.
+inline int kspace(const hnswgpu_index* h) {
+    return h->space == HNSWGPU_SPACE_IP || h->space == HNSWGPU_SPACE_COSINE ? 1 : 0;
+}
+
 // Learned-termination settings of one launch (mode 1: record checkpoints,
 // 2: stop early with the index's network).
 struct TermCfg {

@@ -22,6 +22,10 @@ import numpy as np
 from . import _capi
 
 _SPACES = {"l2": _capi.SPACE_L2, "ip": _capi.SPACE_IP, "cosine": _capi.SPACE_COSINE}
+# An extension for the C++ API's HierarchicalNSW<int> over L2SpaceI: an index
+# of uint8 vectors (built with hnswlib's C++ API), queried with rows holding
+# uint8 values; distances are the reference's integers, as float32.
+_HNSW_ONLY_SPACES = {"l2_uint8": _capi.SPACE_L2_UINT8}
 _PRECISIONS = {"fp32": _capi.PREC_FP32, "bf16": _capi.PREC_BF16, "fp8": _capi.PREC_FP8}
 
 
@@ -41,8 +45,10 @@ def _ptr(a: Optional[np.ndarray]):
 
 
 class _GpuIndex:
+    _extra_spaces: dict = {}
+
     def __init__(self, space: str, dim: int):
-        if space not in _SPACES:
+        if space not in _SPACES and space not in self._extra_spaces:
             raise RuntimeError("Space name must be one of l2, ip, or cosine.")
         self.space = space
         self.dim = int(dim)
@@ -170,6 +176,8 @@ class _GpuIndex:
 class Index(_GpuIndex):
     """GPU-backed ``hnswlib.Index`` (query path)."""
 
+    _extra_spaces = _HNSW_ONLY_SPACES
+
     def __init__(self, space: str, dim: int):
         super().__init__(space, dim)
         self._default_ef = 10
@@ -197,7 +205,8 @@ class Index(_GpuIndex):
         10 as the reference does (hnswalg.h:794)."""
         self._free()
         h = C.c_void_p()
-        _capi.check(_capi.lib().hnswgpu_load_hnsw(str(path_to_index).encode(), _SPACES[self.space], self.dim,
+        space_id = _SPACES.get(self.space, self._extra_spaces.get(self.space))
+        _capi.check(_capi.lib().hnswgpu_load_hnsw(str(path_to_index).encode(), space_id, self.dim,
                                                   int(max_elements), self.device, C.byref(h)))
         self._h = h
         self._default_ef = 10

@@ -46,6 +46,12 @@ extern "C" {
 #define HNSWGPU_SPACE_L2 0
 #define HNSWGPU_SPACE_IP 1
 #define HNSWGPU_SPACE_COSINE 2
+/* hnswlib::L2SpaceI (hnswlib/space_l2.h:255-323): an HNSW index of uint8
+ * vectors with integer squared-L2 distances (HierarchicalNSW<int>).  Queries
+ * are passed as float32 rows holding the uint8 values; distances come back as
+ * float32 holding the reference's integer distances exactly (needs
+ * dim * 255^2 < 2^24, i.e. dim <= 258).  HNSW indexes only. */
+#define HNSWGPU_SPACE_L2_UINT8 3
 
 /* search flags */
 #define HNSWGPU_DEVICE_PTRS 0x1u  /* queries / outputs / allow mask are device

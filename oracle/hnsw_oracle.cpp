@@ -162,7 +162,20 @@ float dist_ip(const float* a, const float* b, size_t dim) {
     return 1.0f - ip_scalar(a, b, dim);
 }
 
+// L2SpaceI (space_l2.h:255-323): uint8 elements, integer sum of squared
+// differences, in any order exact; here over uint8 values held in floats.
+float dist_l2_u8(const float* a, const float* b, size_t dim) {
+    int64_t res = 0;
+    for (size_t i = 0; i < dim; i++) {
+        const int t = (int)(unsigned char)a[i] - (int)(unsigned char)b[i];
+        res += t * t;
+    }
+    return (float)(int)res;
+}
+
+// space: 0 L2, 1 and 2 inner product (cosine: normalised vectors), 3 uint8 L2
 inline float dist(int space, const float* a, const float* b, size_t dim) {
+    if (space == 3) return dist_l2_u8(a, b, dim);
     return space == 0 ? dist_l2(a, b, dim) : dist_ip(a, b, dim);
 }
 
@@ -183,8 +196,11 @@ struct Hnsw {
     uint64_t dim = 0;
     uint64_t num_deleted = 0;
 
+    std::vector<float> u8f;  // space 3: the uint8 elements widened to float
     const char* rec(uint32_t i) const { return l0.data() + (size_t)i * size_data; }
-    const float* vec(uint32_t i) const { return (const float*)(rec(i) + offsetData); }
+    const float* vec(uint32_t i) const {
+        return space == 3 ? u8f.data() + (size_t)i * dim : (const float*)(rec(i) + offsetData);
+    }
     uint64_t label(uint32_t i) const {
         uint64_t v;
         memcpy(&v, rec(i) + label_offset, 8);
@@ -255,6 +271,13 @@ Hnsw* load_hnsw(const char* path, int space, uint64_t dim) {
     }
     for (uint64_t i = 0; i < h->cur; i++)
         if (h->deleted((uint32_t)i)) h->num_deleted++;
+    if (space == 3) {
+        h->u8f.resize(h->cur * dim);
+        for (uint64_t i = 0; i < h->cur; i++) {
+            const unsigned char* u = (const unsigned char*)(h->rec((uint32_t)i) + h->offsetData);
+            for (uint64_t c = 0; c < dim; c++) h->u8f[i * dim + c] = (float)u[c];
+        }
+    }
     return h;
 }
 

@@ -23,7 +23,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 REFERENCE = 0
 CANONICAL = 1
-SPACES = {"l2": 0, "ip": 1, "cosine": 1}
+SPACES = {"l2": 0, "ip": 1, "cosine": 1, "l2_uint8": 3}
 
 _lib = None
 
@@ -233,6 +233,45 @@ def ref_epsilon_search(path, space, q, epsilon, min_candidates, max_candidates, 
                               _ptr(labels), _ptr(dists), _ptr(counts))
     if rc != 0:
         raise RuntimeError("reference epsilon search failed")
+    return labels, dists, counts
+
+
+def ref_l2u8():
+    """ctypes handle of oracle/_ref/libref_l2u8.so (the reference's
+    HierarchicalNSW<int> over L2SpaceI), or None where it was not built."""
+    path = os.path.join(HERE, "_ref", "libref_l2u8.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    P, U64 = C.c_void_p, C.c_uint64
+    L.ref_l2u8_build.restype = C.c_int
+    L.ref_l2u8_build.argtypes = [C.c_char_p, P, P, U64, U64, U64, U64, U64]
+    L.ref_l2u8_search.restype = C.c_int
+    L.ref_l2u8_search.argtypes = [C.c_char_p, U64, P, U64, U64, U64, P, U64, P, U64, P, P, P]
+    return L
+
+
+def ref_l2u8_build(path, x_u8, labels, M=16, efc=100, seed=100):
+    """Build and save a uint8 L2SpaceI index with the reference's addPoint."""
+    x = np.ascontiguousarray(x_u8, np.uint8)
+    lab = np.ascontiguousarray(labels, np.uint64)
+    if ref_l2u8().ref_l2u8_build(str(path).encode(), _ptr(x), _ptr(lab), x.shape[0], x.shape[1], M, efc, seed) != 0:
+        raise RuntimeError("reference L2SpaceI build failed")
+
+
+def ref_l2u8_search(path, q_u8, k, ef, deleted=(), allow_by_label=None):
+    """The reference's searchKnn on a uint8 index: (labels, int32 dists, counts)."""
+    q = np.ascontiguousarray(np.atleast_2d(q_u8), np.uint8)
+    nq, dim = q.shape
+    dele = np.ascontiguousarray(np.asarray(deleted, np.uint64))
+    allow = None if allow_by_label is None else np.ascontiguousarray(allow_by_label, np.uint8)
+    labels = np.empty((nq, k), np.uint64)
+    dists = np.empty((nq, k), np.int32)
+    counts = np.empty(nq, np.int32)
+    rc = ref_l2u8().ref_l2u8_search(str(path).encode(), dim, _ptr(q), nq, k, ef, _ptr(dele), dele.size, _ptr(allow),
+                                    0 if allow is None else allow.size, _ptr(labels), _ptr(dists), _ptr(counts))
+    if rc != 0:
+        raise RuntimeError("reference L2SpaceI search failed")
     return labels, dists, counts
 
 

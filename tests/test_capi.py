@@ -76,6 +76,9 @@ def test_python_surface_argument_checks():
         H.Index("hamming", 8)
     with pytest.raises(RuntimeError, match="Space name must be one of l2, ip, or cosine."):
         H.BFIndex("dot", 8)
+    with pytest.raises(RuntimeError, match="Space name must be one of l2, ip, or cosine."):
+        H.BFIndex("l2_uint8", 8)  # L2SpaceI: HNSW indexes only
+    assert H.Index("l2_uint8", 8).space == "l2_uint8"
     idx = H.Index("l2", 8)
     assert idx.ef == 10 and idx.get_current_count() == 0
     idx.set_ef(77)
@@ -153,6 +156,9 @@ def test_newer_entry_points_reject_bad_arguments():
     assert lib.hnswgpu_build_traversal_copy(None, 2) == _capi.ERR_ARG
     assert lib.hnswgpu_search_epsilon(None, None, 1, C.c_float(1.0), 1, 4, C.byref(opts), None, None,
                                       None) == _capi.ERR_ARG
+    h = C.c_void_p()
+    assert lib.hnswgpu_load_bf(b"none.bin", _capi.SPACE_L2_UINT8, 8, 0, C.byref(h)) == _capi.ERR_UNSUPPORTED
+    assert lib.hnswgpu_create_bf(_capi.SPACE_L2_UINT8, 8, None, None, 0, 0, 0, C.byref(h)) == _capi.ERR_UNSUPPORTED
     assert lib.hnswgpu_last_error() != b""
 
 

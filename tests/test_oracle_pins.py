@@ -248,3 +248,47 @@ def test_oracle_epsilon_search_vs_reference_fresh(tmp_path):
             assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
             assert np.array_equal(od.view(np.uint32), rd.view(np.uint32))
             assert all(np.all(od[i, :oc[i]] <= eps) for i in range(q.shape[0]))
+
+
+def test_oracle_l2_uint8_matches_reference_golden():
+    """hnswlib::L2SpaceI (uint8 vectors, integer squared L2): the oracle's
+    restatement against the reference's HierarchicalNSW<int> searchKnn
+    outputs recorded in tests/golden/l2u8.npz (plain, filtered, with
+    deletions; clustered integers, so many exact ties)."""
+    e = np.load(f"{GOLDEN}/l2u8.npz")
+    q = e["queries"].astype(np.float32)
+    keys = sorted({k.rsplit("/", 1)[0] for k in e.keys() if "/" in k})
+    assert len(keys) == 18
+    for key in keys:
+        ef, k, variant = key.split("_")
+        ef, k = int(ef[2:]), int(k[1:])
+        o = O.Hnsw(f"{GOLDEN}/hnsw_l2u8_d32.bin", "l2_uint8", 32)
+        allow = None
+        if variant == "even":
+            allow = (o.labels() % 2 == 0).astype(np.uint8)
+        if variant == "del":
+            for lab in e["deleted"]:
+                assert o.set_deleted(int(lab), True) == 0
+        ol, od, oc = o.search(q, k, ef, mode=O.REFERENCE, allow=allow)
+        rc = e[key + "/counts"]
+        assert np.array_equal(oc, rc), key
+        for i in range(q.shape[0]):
+            assert np.array_equal(ol[i, :rc[i]], e[key + "/labels"][i, :rc[i]]), (key, i)
+            assert np.array_equal(od[i, :rc[i]], e[key + "/dists"][i, :rc[i]].astype(np.float32)), (key, i)
+
+
+def test_oracle_l2_uint8_vs_reference_fresh(tmp_path):
+    if O.ref_l2u8() is None:
+        pytest.skip("oracle/_ref/libref_l2u8.so not built")
+    rng = np.random.default_rng(41)
+    for dim in (16, 20, 64):
+        x = rng.integers(0, 256, (2000, dim)).astype(np.uint8)
+        q = rng.integers(0, 256, (50, dim)).astype(np.uint8)
+        path = tmp_path / f"u{dim}.bin"
+        O.ref_l2u8_build(path, x, np.arange(2000, dtype=np.uint64), M=12, efc=80)
+        o = O.Hnsw(str(path), "l2_uint8", dim)
+        for ef, k in ((10, 10), (64, 5)):
+            rl, rd, rc = O.ref_l2u8_search(path, q, k, ef)
+            ol, od, oc = o.search(q.astype(np.float32), k, ef, mode=O.REFERENCE)
+            assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
+            assert np.array_equal(od, rd.astype(np.float32))
