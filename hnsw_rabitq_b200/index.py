@@ -15,6 +15,7 @@ Index construction (``init_index`` / ``add_items`` / ``save_index`` on an HNSW
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Callable, Optional
 
 import numpy as np
@@ -181,6 +182,9 @@ class Index(_GpuIndex):
     def __init__(self, space: str, dim: int):
         super().__init__(space, dim)
         self._default_ef = 10
+        self._source = None       # file the index was loaded from
+        self._state_bytes = None  # or its bytes (an index made from a pickled state)
+        self._marks = {}          # label -> deleted, for marks changed since the load
         # "reference": equal distances resolve exactly as hnswlib's heaps do
         # (results identical to searchKnn); "id": ties break by internal id
         # (identical except where distances tie exactly; faster).
@@ -210,6 +214,75 @@ class Index(_GpuIndex):
                                                   int(max_elements), self.device, C.byref(h)))
         self._h = h
         self._default_ef = 10
+        # the file the index came from, and the delete marks changed since:
+        # pickling and save_index rebuild the reference's state from them
+        self._source = os.path.abspath(str(path_to_index))
+        self._marks = {}
+
+    # -- the reference's pickled state and saved file (bindings.cpp:465-529, 1001-1008)
+    def _file_bytes(self) -> bytes:
+        from . import pickling
+        self._require()
+        if self._source is None:
+            buf = self._state_bytes
+        else:
+            with open(self._source, "rb") as f:
+                buf = f.read()
+        dele = {lab for lab, m in self._marks.items() if m}
+        keep = {lab for lab, m in self._marks.items() if not m}
+        return pickling.set_delete_marks(buf, dele, keep)
+
+    def save_index(self, path: str) -> None:
+        """HierarchicalNSW::saveIndex (hnswalg.h:685-712): the loaded index,
+        with the delete marks made since, in the reference's file layout."""
+        buf = self._file_bytes()
+        with open(path, "wb") as f:
+            f.write(buf)
+
+    def __getstate__(self):
+        """The reference's pickled state: (getIndexParams() dict,)."""
+        from . import pickling
+        if not self._h:
+            return ({"ser_version": pickling.SER_VERSION, "space": self.space, "dim": self.dim,
+                     "index_inited": False, "ep_added": False, "normalize": self.space == "cosine",
+                     "num_threads": self.num_threads, "seed": 100, "ef": self._default_ef},)
+        return (pickling.file_bytes_to_state(self._file_bytes(), self.space, self.dim, self.ef, self.num_threads),)
+
+    def __setstate__(self, state):
+        """createFromParams (bindings.cpp:485-519): also accepts the state of
+        a reference hnswlib.Index (``ref_index.__getstate__()``)."""
+        from . import pickling
+        if not isinstance(state, tuple) or len(state) != 1:
+            raise RuntimeError("Invalid state!")
+        d = state[0]
+        if int(d["ser_version"]) > pickling.SER_VERSION:
+            raise RuntimeError("Invalid serialization version!")
+        Index.__init__(self, d["space"], int(d["dim"]))
+        self.num_threads = int(d.get("num_threads", -1))
+        if not d.get("index_inited", False):
+            self._default_ef = int(d.get("ef", 10))
+            return
+        import tempfile
+        fd, tmp = tempfile.mkstemp(suffix=".bin")
+        try:
+            with os.fdopen(fd, "wb") as f:
+                f.write(pickling.state_to_file_bytes(d))
+            self.load_index(tmp)
+            # a later pickle or save_index rereads the source: keep it in memory
+            with open(tmp, "rb") as f:
+                self._state_bytes = f.read()
+        finally:
+            os.unlink(tmp)
+        self._source = None
+        self.set_ef(int(d["ef"]))
+
+    @classmethod
+    def from_params(cls, d: dict) -> "Index":
+        """Index from a getIndexParams dict (e.g. a reference hnswlib.Index's
+        ``__getstate__()[0]``): its index goes straight to the GPU."""
+        obj = cls.__new__(cls)
+        obj.__setstate__((d,))
+        return obj
 
     def init_index(self, *args, **kwargs):
         raise NotImplementedError(
@@ -218,9 +291,6 @@ class Index(_GpuIndex):
 
     def add_items(self, *args, **kwargs):
         self.init_index()
-
-    def save_index(self, *args, **kwargs):
-        raise NotImplementedError("this index is loaded read-only from an hnswlib file")
 
     # -- ef
     def set_ef(self, ef: int) -> None:
@@ -248,10 +318,12 @@ class Index(_GpuIndex):
     def mark_deleted(self, label: int) -> None:
         self._require()
         _capi.check(_capi.lib().hnswgpu_mark_deleted(self._h, int(label)))
+        self._marks[int(label)] = True
 
     def unmark_deleted(self, label: int) -> None:
         self._require()
         _capi.check(_capi.lib().hnswgpu_unmark_deleted(self._h, int(label)))
+        self._marks[int(label)] = False
 
     # -- learned early termination
     def set_termination_model(self, model) -> None:

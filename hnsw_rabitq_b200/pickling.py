@@ -1,0 +1,113 @@
+"""The reference's pickled state of an ``hnswlib.Index`` and its saved-index
+file, each built from the other.
+
+``hnswlib.Index.__getstate__`` returns ``(getIndexParams(),)``
+(python_bindings/bindings.cpp:465-482, 1001-1008): a dict of scalar
+parameters plus ``getAnnData()`` (bindings.cpp:351-462), which copies the
+level-0 block, the upper-level link lists, ``element_levels_`` and the label
+map.  ``HierarchicalNSW::saveIndex`` (hnswlib/hnswalg.h:685-712) writes the same
+fields in a fixed layout: a header, the level-0 block of the
+``cur_element_count`` elements, then per element its upper-level list size
+(uint32) and the list.  The GPU index loads that file layout, so a pickled
+state is turned back into file bytes (``state_to_file_bytes``) and a loaded
+file into a state (``file_bytes_to_state``).
+"""
+from __future__ import annotations
+
+import struct
+
+import numpy as np
+
+SER_VERSION = 1  # bindings.cpp:148
+# offsetLevel0_, max_elements_, cur_element_count, size_data_per_element_,
+# label_offset_, offsetData_ (size_t); maxlevel_ (int); enterpoint_node_
+# (uint32); maxM_, maxM0_, M_ (size_t); mult_ (double); ef_construction_
+_HEADER = struct.Struct("<QQQQQQiIQQQdQ")
+
+
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a)).view(np.uint8).reshape(-1)
+
+
+def state_to_file_bytes(d: dict) -> bytes:
+    """saveIndex's file for the index described by a getIndexParams dict."""
+    if not d.get("index_inited", True):
+        raise RuntimeError("the state holds no index (index_inited is false)")
+    cur = int(d["cur_element_count"])
+    size_data = int(d["size_data_per_element"])
+    size_links = int(d["size_links_per_element"])
+    head = _HEADER.pack(int(d["offset_level0"]), int(d["max_elements"]), cur, size_data, int(d["label_offset"]),
+                        int(d["offset_data"]), int(d["max_level"]), int(d["enterpoint_node"]), int(d["max_M"]),
+                        int(d["max_M0"]), int(d["M"]), float(d["mult"]), int(d["ef_construction"]))
+    level0 = _u8(d["data_level0"])[: cur * size_data]
+    if level0.size != cur * size_data:
+        raise RuntimeError("data_level0 is shorter than cur_element_count elements")
+    levels = np.asarray(d["element_levels"], np.int64)[:cur]
+    links = _u8(d["link_lists"])
+    parts = [head, level0.tobytes()]
+    off = 0
+    for lev in levels:
+        n = size_links * int(lev) if lev > 0 else 0
+        parts.append(struct.pack("<I", n))
+        if n:
+            if off + n > links.size:
+                raise RuntimeError("link_lists is shorter than element_levels requires")
+            parts.append(links[off:off + n].tobytes())
+        off += n
+    return b"".join(parts)
+
+
+def file_bytes_to_state(buf: bytes, space: str, dim: int, ef: int, num_threads: int = -1, seed: int = 100) -> dict:
+    """The getIndexParams dict of the index stored in a saveIndex file.
+    The label map lists elements in internal-id order (the reference lists it
+    in its hash map's order)."""
+    (off0, max_el, cur, size_data, label_off, data_off, maxlevel, ep, maxM, maxM0, M, mult,
+     efc) = _HEADER.unpack_from(buf, 0)
+    pos = _HEADER.size
+    level0 = np.frombuffer(buf, np.uint8, cur * size_data, pos)
+    pos += cur * size_data
+    size_links = maxM * 4 + 4
+    levels = np.zeros(max_el, np.int32)
+    chunks = []
+    for i in range(cur):
+        (n,) = struct.unpack_from("<I", buf, pos)
+        pos += 4
+        if n:
+            levels[i] = n // size_links
+            chunks.append(buf[pos:pos + n])
+            pos += n
+    if pos != len(buf):
+        raise RuntimeError("Index seems to be corrupted or unsupported")
+    rec = level0.reshape(cur, size_data) if cur else level0.reshape(0, max(size_data, 1))
+    labels = rec[:, label_off:label_off + 8].copy().view(np.uint64).reshape(-1)
+    deleted = (rec[:, off0 + 2] & 1) != 0 if cur else np.zeros(0, bool)
+    return {
+        "ser_version": SER_VERSION, "space": space, "dim": int(dim), "index_inited": True, "ep_added": cur > 0,
+        "normalize": space == "cosine", "num_threads": int(num_threads), "seed": int(seed),
+        "offset_level0": off0, "max_elements": max_el, "cur_element_count": cur, "size_data_per_element": size_data,
+        "label_offset": label_off, "offset_data": data_off, "max_level": maxlevel, "enterpoint_node": ep,
+        "max_M": maxM, "max_M0": maxM0, "M": M, "mult": mult, "ef_construction": efc, "ef": int(ef),
+        "has_deletions": bool(deleted.any()), "size_links_per_element": size_links, "allow_replace_deleted": False,
+        "label_lookup_external": labels, "label_lookup_internal": np.arange(cur, dtype=np.uint32),
+        "element_levels": levels, "data_level0": level0.view(np.int8).copy(),
+        "link_lists": np.frombuffer(b"".join(chunks), np.int8).copy(),
+    }
+
+
+def set_delete_marks(buf: bytes, deleted_labels: set, undeleted_labels: set) -> bytes:
+    """A copy of a saveIndex file with the delete mark (bit 0 of the third
+    byte of each element's level-0 list header, hnswalg.h:872-935) set for
+    `deleted_labels` and cleared for `undeleted_labels`."""
+    if not deleted_labels and not undeleted_labels:
+        return buf
+    (off0, _, cur, size_data, label_off, *_rest) = _HEADER.unpack_from(buf, 0)
+    out = bytearray(buf)
+    base = _HEADER.size
+    for i in range(cur):
+        r = base + i * size_data
+        (lab,) = struct.unpack_from("<Q", out, r + label_off)
+        if lab in deleted_labels:
+            out[r + off0 + 2] |= 1
+        elif lab in undeleted_labels:
+            out[r + off0 + 2] &= 0xFE
+    return bytes(out)

@@ -1,0 +1,44 @@
+"""Pickling, from_params and save_index of the GPU Index against the
+reference's recorded outputs (needs a B200)."""
+import pickle
+
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from hnsw_rabitq_b200 import pickling as PK
+from tests.helpers import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(idx, g, key, k=10):
+    l, d = idx.knn_query(g["hnsw_l2_d16/queries"], k=k)
+    assert np.array_equal(l, g[f"hnsw_l2_d16/{key}/labels"]), key
+    assert np.array_equal(d.view(np.uint32), g[f"hnsw_l2_d16/{key}/dists"].view(np.uint32)), key
+
+
+def test_pickle_from_params_and_save_index(tmp_path):
+    g = golden()
+    idx = H.Index("l2", 16)
+    idx.load_index(f"{GOLDEN}/hnsw_l2_d16.bin")
+    idx.set_ef(32)
+    # pickle round trip: same results, ef kept
+    j = pickle.loads(pickle.dumps(idx))
+    assert j.ef == 32
+    _check(j, g, "ef32_k10")
+    # a state dict (as a reference hnswlib.Index pickles it) goes to the GPU
+    buf = open(f"{GOLDEN}/hnsw_l2_d16.bin", "rb").read()
+    f = H.Index.from_params(PK.file_bytes_to_state(buf, "l2", 16, ef=32))
+    _check(f, g, "ef32_k10")
+    # delete marks travel through pickling and save_index
+    for lab in g["hnsw_l2_d16/deleted"]:
+        idx.mark_deleted(int(lab))
+    _check(idx, g, "ef32_k10_del")
+    _check(pickle.loads(pickle.dumps(idx)), g, "ef32_k10_del")
+    idx.save_index(str(tmp_path / "s.bin"))
+    s = H.Index("l2", 16)
+    s.load_index(str(tmp_path / "s.bin"))
+    s.set_ef(32)
+    _check(s, g, "ef32_k10_del")
+    assert s.get_current_count() == idx.get_current_count()

@@ -1,0 +1,83 @@
+"""The reference's pickled state of hnswlib.Index (getIndexParams) and its
+saveIndex file, each built from the other (hnsw_rabitq_b200/pickling.py),
+checked against the reference itself (oracle/_ref) on the CPU: byte-equal
+files, equal states, and reference indexes rebuilt from our states that
+answer queries exactly as the originals."""
+import pickle
+
+import numpy as np
+import pytest
+
+import hnsw_rabitq_b200 as H
+from hnsw_rabitq_b200 import pickling as PK
+from tests.helpers import ref_or_skip
+
+SCALARS = ["offset_level0", "max_elements", "cur_element_count", "size_data_per_element", "label_offset",
+           "offset_data", "max_level", "enterpoint_node", "max_M", "max_M0", "M", "mult", "ef_construction", "ef",
+           "has_deletions", "size_links_per_element", "space", "dim", "index_inited", "normalize"]
+
+
+def _ref_index(hnswlib, space, dim, n, extra, M, seed, deleted=()):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((n, dim)).astype(np.float32)
+    p = hnswlib.Index(space, dim)
+    p.init_index(n + extra, M=M, ef_construction=60, random_seed=seed)
+    p.add_items(x, np.arange(n) * 5 + 1, num_threads=1)
+    p.set_ef(37)
+    for lab in deleted:
+        p.mark_deleted(int(lab))
+    return p, x
+
+
+CASES = [("l2", 16, 700, 0, 8, ()), ("cosine", 12, 500, 300, 6, ()), ("ip", 20, 600, 50, 10, (1, 6, 101, 2996))]
+
+
+@pytest.mark.parametrize("space,dim,n,extra,M,deleted", CASES)
+def test_state_and_file_round_trip(tmp_path, space, dim, n, extra, M, deleted):
+    hnswlib = ref_or_skip()
+    p, x = _ref_index(hnswlib, space, dim, n, extra, M, seed=dim, deleted=deleted)
+    path = tmp_path / "i.bin"
+    p.save_index(str(path))
+    buf = path.read_bytes()
+    st = p.__getstate__()[0]
+    # reference state -> the reference's own file, byte for byte
+    assert PK.state_to_file_bytes(st) == buf
+    # the reference's file -> a state equal to the reference's
+    ours = PK.file_bytes_to_state(buf, space, dim, ef=37)
+    for key in SCALARS:
+        assert ours[key] == st[key], key
+    for key in ("data_level0", "link_lists", "element_levels"):
+        assert np.array_equal(np.asarray(ours[key]).view(np.uint8), np.asarray(st[key]).view(np.uint8)), key
+    ref_map = dict(zip(np.asarray(st["label_lookup_external"]).tolist(), np.asarray(st["label_lookup_internal"]).tolist()))
+    our_map = dict(zip(ours["label_lookup_external"].tolist(), ours["label_lookup_internal"].tolist()))
+    assert our_map == ref_map
+    assert PK.state_to_file_bytes(ours) == buf
+    # the reference accepts our state (createFromParams) and answers as before
+    r2 = hnswlib.Index.__new__(hnswlib.Index)
+    r2.__setstate__((ours,))
+    q = np.random.default_rng(1).standard_normal((50, dim)).astype(np.float32)
+    a = p.knn_query(q, k=5, num_threads=1)
+    b = r2.knn_query(q, k=5, num_threads=1)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_delete_marks_match_the_reference(tmp_path):
+    hnswlib = ref_or_skip()
+    p, _ = _ref_index(hnswlib, "l2", 16, 400, 0, 8, seed=3)
+    before = tmp_path / "a.bin"
+    p.save_index(str(before))
+    p.mark_deleted(6)
+    p.mark_deleted(11)
+    p.unmark_deleted(6)
+    after = tmp_path / "b.bin"
+    p.save_index(str(after))
+    assert PK.set_delete_marks(before.read_bytes(), {11}, {6}) == after.read_bytes()
+
+
+def test_unloaded_index_pickles():
+    i = H.Index("cosine", 7)
+    i.set_ef(55)
+    j = pickle.loads(pickle.dumps(i))
+    assert (j.space, j.dim, j.ef, j._h) == ("cosine", 7, 55, None)
+    with pytest.raises(RuntimeError, match="Invalid serialization version"):
+        H.Index.from_params({"ser_version": 2, "space": "l2", "dim": 4})
