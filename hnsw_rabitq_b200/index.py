@@ -149,6 +149,8 @@ class _GpuIndex:
         return self._info().count if self._h else 0
 
     def get_max_elements(self) -> int:
+        if getattr(self, "_max_elements", None) is not None:
+            return self._max_elements
         return self._info().max_elements if self._h else 0
 
     def get_ids_list(self):
@@ -179,12 +181,22 @@ class Index(_GpuIndex):
 
     _extra_spaces = _HNSW_ONLY_SPACES
 
-    def __init__(self, space: str, dim: int):
+    def __init__(self, space=None, dim=None, params: Optional[dict] = None, index: Optional["Index"] = None):
+        """Index(space, dim), or, as the reference's other constructors
+        (bindings.cpp:937-939), Index(params) from a getIndexParams dict and
+        Index(index) as a copy of another Index."""
+        if isinstance(space, dict) or params is not None:
+            self.__setstate__((params if params is not None else space,))
+            return
+        if isinstance(space, Index) or index is not None:
+            self.__setstate__((index if index is not None else space).__getstate__())
+            return
         super().__init__(space, dim)
         self._default_ef = 10
         self._source = None       # file the index was loaded from
         self._state_bytes = None  # or its bytes (an index made from a pickled state)
         self._marks = {}          # label -> deleted, for marks changed since the load
+        self._max_elements = None  # set by resize_index
         # "reference": equal distances resolve exactly as hnswlib's heaps do
         # (results identical to searchKnn); "id": ties break by internal id
         # (identical except where distances tie exactly; faster).
@@ -218,6 +230,7 @@ class Index(_GpuIndex):
         # pickling and save_index rebuild the reference's state from them
         self._source = os.path.abspath(str(path_to_index))
         self._marks = {}
+        self._max_elements = None
 
     # -- the reference's pickled state and saved file (bindings.cpp:465-529, 1001-1008)
     def _file_bytes(self) -> bytes:
@@ -230,7 +243,37 @@ class Index(_GpuIndex):
                 buf = f.read()
         dele = {lab for lab, m in self._marks.items() if m}
         keep = {lab for lab, m in self._marks.items() if not m}
-        return pickling.set_delete_marks(buf, dele, keep)
+        buf = pickling.set_delete_marks(buf, dele, keep)
+        if self._max_elements is not None:
+            buf = pickling.with_max_elements(buf, self._max_elements)
+        return buf
+
+    def get_items(self, ids=None, return_type: str = "numpy"):
+        """Stored vectors by label (bindings.cpp:307-338 -> getDataByLabel):
+        a numpy array or a list of lists; no ids gives none.  Read from the
+        index's saved form (for the cosine space these are the normalised
+        vectors the reference stores)."""
+        from . import pickling
+        if return_type not in ("numpy", "list"):
+            raise ValueError('return_type should be "numpy" or "list"')
+        ids = [] if ids is None else np.asarray(ids)
+        if isinstance(ids, np.ndarray) and ids.ndim == 0:
+            raise ValueError("get_items accepts a list of indices and returns a list of vectors")
+        elem = np.uint8 if self.space == "l2_uint8" else np.float32
+        rows = pickling.items_from_file(self._file_bytes(), list(ids), self.dim, elem)
+        return rows.tolist() if return_type == "list" else rows
+
+    def index_file_size(self) -> int:
+        """HierarchicalNSW::indexFileSize (hnswalg.h:658-683): bytes save_index writes."""
+        return len(self._file_bytes())
+
+    def resize_index(self, new_size: int) -> None:
+        """resizeIndex (hnswalg.h:633-656): the capacity recorded with the
+        index (max_elements); the GPU index itself holds exactly its elements."""
+        self._require()
+        if int(new_size) < self.get_current_count():
+            raise RuntimeError("Cannot resize, max element is less than the current number of elements")
+        self._max_elements = int(new_size)
 
     def save_index(self, path: str) -> None:
         """HierarchicalNSW::saveIndex (hnswalg.h:685-712): the loaded index,

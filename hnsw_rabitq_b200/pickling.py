@@ -111,3 +111,29 @@ def set_delete_marks(buf: bytes, deleted_labels: set, undeleted_labels: set) -> 
         elif lab in undeleted_labels:
             out[r + off0 + 2] &= 0xFE
     return bytes(out)
+
+
+def items_from_file(buf: bytes, ids, dim: int, elem_dtype=np.float32) -> np.ndarray:
+    """getDataByLabel (hnswalg.h:825-846) for each label of `ids`, read from a
+    saveIndex file: rows of `dim` elements.  A label that is absent or marked
+    deleted raises "Label not found", as the reference does."""
+    (off0, _, cur, size_data, label_off, data_off, *_rest) = _HEADER.unpack_from(buf, 0)
+    rec = np.frombuffer(buf, np.uint8, cur * size_data, _HEADER.size).reshape(cur, size_data)
+    labels = rec[:, label_off:label_off + 8].copy().view(np.uint64).reshape(-1)
+    where = {int(v): i for i, v in enumerate(labels.tolist())}
+    width = dim * np.dtype(elem_dtype).itemsize
+    out = np.empty((len(ids), dim), np.float32)
+    for r, lab in enumerate(ids):
+        i = where.get(int(lab))
+        if i is None or rec[i, off0 + 2] & 1:
+            raise RuntimeError("Label not found")
+        out[r] = rec[i, data_off:data_off + width].copy().view(elem_dtype)
+    return out
+
+
+def with_max_elements(buf: bytes, max_elements: int) -> bytes:
+    """A copy of a saveIndex file whose header records another max_elements_
+    (what resizeIndex changes, hnswalg.h:633-656)."""
+    out = bytearray(buf)
+    struct.pack_into("<Q", out, 8, int(max_elements))
+    return bytes(out)

@@ -42,3 +42,18 @@ def test_pickle_from_params_and_save_index(tmp_path):
     s.set_ef(32)
     _check(s, g, "ef32_k10_del")
     assert s.get_current_count() == idx.get_current_count()
+    # get_items: the stored rows of the returned labels give back their distances
+    from oracle import oracle as O
+    q = g["hnsw_l2_d16/queries"]
+    l, d = s.knn_query(q[:3], k=4)
+    for i in range(3):
+        rows = s.get_items(l[i])
+        assert np.array_equal(O.distances("l2", q[i], rows).view(np.uint32), d[i].view(np.uint32))
+    with pytest.raises(RuntimeError, match="Label not found"):
+        s.get_items([int(g["hnsw_l2_d16/deleted"][0])])
+    s.resize_index(5000)
+    assert s.get_max_elements() == 5000 and s.index_file_size() == len(open(tmp_path / "s.bin", "rb").read())
+    c = H.Index(s)  # the copy constructor
+    c.set_ef(32)
+    _check(c, g, "ef32_k10_del")
+    assert c.get_max_elements() == 5000

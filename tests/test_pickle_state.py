@@ -81,3 +81,33 @@ def test_unloaded_index_pickles():
     assert (j.space, j.dim, j.ef, j._h) == ("cosine", 7, 55, None)
     with pytest.raises(RuntimeError, match="Invalid serialization version"):
         H.Index.from_params({"ser_version": 2, "space": "l2", "dim": 4})
+
+
+def test_get_items_file_size_and_resize_match_the_reference(tmp_path):
+    hnswlib = ref_or_skip()
+    for space in ("l2", "cosine"):
+        p, x = _ref_index(hnswlib, space, 16, 300, 20, 8, seed=9)
+        p.mark_deleted(11)
+        path = tmp_path / f"{space}.bin"
+        p.save_index(str(path))
+        buf = path.read_bytes()
+        ids = [1, 6, 1496, 51]
+        assert np.array_equal(PK.items_from_file(buf, ids, 16), np.asarray(p.get_items(ids)))
+        for bad in (11, 2):  # deleted, absent
+            with pytest.raises(RuntimeError, match="Label not found"):
+                PK.items_from_file(buf, [bad], 16)
+            with pytest.raises(RuntimeError, match="Label not found"):
+                p.get_items([bad])
+        assert p.index_file_size() == len(buf)
+        p.resize_index(777)
+        p.save_index(str(path))
+        assert PK.with_max_elements(buf, 777) == path.read_bytes()
+
+
+def test_constructor_overloads_unloaded():
+    i = H.Index(params={"ser_version": 1, "space": "ip", "dim": 9, "index_inited": False, "ef": 21})
+    assert (i.space, i.dim, i.ef) == ("ip", 9, 21)
+    j = H.Index(i)
+    assert (j.space, j.dim, j.ef) == ("ip", 9, 21)
+    with pytest.raises(ValueError, match="return_type"):
+        H.Index("l2", 4).get_items([1], return_type="tuple")
