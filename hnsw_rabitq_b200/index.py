@@ -479,6 +479,7 @@ class BFIndex(_GpuIndex):
         self._row_labels = None
         self._maxel = 0
         self._dirty = False
+        self._source = None  # the file a loaded index came from
         self.cur_l = 0
         # "fp32": the reference's exact scan; "bf16" / "fp8": tensor-core scores
         # over a low-precision copy, the best `rerank` candidates (default
@@ -559,8 +560,16 @@ class BFIndex(_GpuIndex):
         self._dirty = True
 
     def _pull_rows(self):
-        raise NotImplementedError("rows of a file-loaded BFIndex are device-resident; add_items after load_index "
-                                  "is not supported")
+        """The rows of a file-loaded index, from its file, so that add_items /
+        delete_vector can change them (the index is rebuilt on the GPU at the
+        next query).  Cosine files hold normalised rows that a rebuild would
+        normalise again, so the cosine space keeps them read-only."""
+        from . import pickling
+        if self.space == "cosine" or getattr(self, "_source", None) is None:
+            raise NotImplementedError("add_items / delete_vector after load_index: not supported for the cosine "
+                                      "space (its file holds normalised rows)")
+        with open(self._source, "rb") as f:
+            self._maxel, self._rows, self._row_labels = pickling.bf_file_to_rows(f.read(), self.dim)
 
     def _sync(self):
         if self._rows is not None and (self._dirty or not self._h):
@@ -586,9 +595,26 @@ class BFIndex(_GpuIndex):
                                                 self.device, C.byref(h)))
         self._h = h
         self.cur_l = self._info().count
+        self._source = os.path.abspath(str(path_to_index))
 
-    def save_index(self, *args, **kwargs):
-        raise NotImplementedError("save_index is not part of the GPU query path")
+    def save_index(self, path_to_index: str) -> None:
+        """BruteforceSearch::saveIndex (bruteforce.h:128-139).  A loaded,
+        unchanged index is written back as loaded; rows added here are written
+        as given (l2 / ip; the cosine space normalises them on the GPU, so an
+        in-memory cosine index cannot be written)."""
+        from . import pickling
+        if self._rows is None:
+            if getattr(self, "_source", None) is None:
+                raise RuntimeError("nothing to save: call init_index / add_items or load_index first")
+            with open(self._source, "rb") as f:
+                buf = f.read()
+        else:
+            if self.space == "cosine":
+                raise NotImplementedError("save_index of a cosine BFIndex built in memory is not supported")
+            buf = pickling.bf_rows_to_file(self._rows, self._row_labels, max(self._maxel, self._rows.shape[0]),
+                                           self.dim)
+        with open(path_to_index, "wb") as f:
+            f.write(buf)
 
     def get_current_count(self) -> int:
         if self._rows is not None:

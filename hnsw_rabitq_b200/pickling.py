@@ -137,3 +137,33 @@ def with_max_elements(buf: bytes, max_elements: int) -> bytes:
     out = bytearray(buf)
     struct.pack_into("<Q", out, 8, int(max_elements))
     return bytes(out)
+
+
+# BruteforceSearch::saveIndex / loadIndex (hnswlib/bruteforce.h:128-161):
+# maxelements_, size_per_element_, cur_element_count (size_t), then
+# maxelements_ records of (vector, label).
+_BF_HEADER = struct.Struct("<QQQ")
+
+
+def bf_file_to_rows(buf: bytes, dim: int):
+    """(max_elements, rows [cur, dim] float32, labels [cur] uint64) of a
+    brute-force index file."""
+    maxel, size_per, cur = _BF_HEADER.unpack_from(buf, 0)
+    if size_per != dim * 4 + 8 or len(buf) < _BF_HEADER.size + maxel * size_per or cur > maxel:
+        raise RuntimeError("Index seems to be corrupted or unsupported")
+    rec = np.frombuffer(buf, np.uint8, cur * size_per, _BF_HEADER.size).reshape(cur, size_per)
+    rows = rec[:, :dim * 4].copy().view(np.float32).reshape(cur, dim)
+    labels = rec[:, dim * 4:].copy().view(np.uint64).reshape(cur)
+    return int(maxel), rows, labels
+
+
+def bf_rows_to_file(rows: np.ndarray, labels: np.ndarray, max_elements: int, dim: int) -> bytes:
+    """The brute-force index file of these rows (records beyond the current
+    count are zero; the reference writes whatever its buffer holds there)."""
+    cur = rows.shape[0]
+    size_per = dim * 4 + 8
+    rec = np.zeros((max(int(max_elements), cur), size_per), np.uint8)
+    if cur:
+        rec[:cur, :dim * 4] = np.ascontiguousarray(rows, np.float32).view(np.uint8).reshape(cur, dim * 4)
+        rec[:cur, dim * 4:] = np.ascontiguousarray(labels, np.uint64).view(np.uint8).reshape(cur, 8)
+    return _BF_HEADER.pack(rec.shape[0], size_per, cur) + rec.tobytes()

@@ -66,3 +66,25 @@ def test_bf_add_items_and_ties():
         g.knn_query(q, k=3000)
     g.delete_vector(int(labels[0]))
     assert g.get_current_count() == 1999
+
+
+def test_bf_loaded_then_changed_and_saved(tmp_path):
+    """A file-loaded BFIndex: delete_vector pulls its rows from the file, the
+    next query runs on the changed set (the recorded top-25 minus the deleted
+    label), and save_index / load_index keep it."""
+    g = golden()
+    b = H.BFIndex("l2", 7)
+    b.load_index(f"{GOLDEN}/bf_l2_d7.bin")
+    q = g["bf_l2_d7/queries"]
+    top = g["bf_l2_d7/k25/labels"]
+    gone = int(top[0, 0])
+    b.delete_vector(gone)
+    want = np.stack([row[row != gone][:10] for row in top])
+    l, _ = b.knn_query(q, k=10)
+    assert np.array_equal(l, want)
+    b.save_index(str(tmp_path / "c.bin"))
+    c = H.BFIndex("l2", 7)
+    c.load_index(str(tmp_path / "c.bin"))
+    l2, _ = c.knn_query(q, k=10)
+    assert np.array_equal(l2, want)
+    assert c.get_current_count() == b.get_current_count()

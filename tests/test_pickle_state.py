@@ -111,3 +111,33 @@ def test_constructor_overloads_unloaded():
     assert (j.space, j.dim, j.ef) == ("ip", 9, 21)
     with pytest.raises(ValueError, match="return_type"):
         H.Index("l2", 4).get_items([1], return_type="tuple")
+
+
+@pytest.mark.parametrize("space", ["l2", "ip"])
+def test_bf_save_index_matches_the_reference(tmp_path, space):
+    """BFIndex built in memory (init_index / add_items / delete_vector, no GPU
+    needed) saves the reference's file: header and every current record
+    byte-equal (slots past the count hold leftovers in the reference)."""
+    hnswlib = ref_or_skip()
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((330, 12)).astype(np.float32)
+    ops = [("add", x[:300], np.arange(300) * 2 + 3), ("del", 5), ("del", 17), ("del", 12345),
+           ("add", x[300:330], np.arange(30) * 2 + 1000), ("add", x[:2], [3, 5])]
+    ref = hnswlib.BFIndex(space, 12)
+    ref.init_index(400)
+    ours = H.BFIndex(space, 12)
+    ours.init_index(400)
+    for op in ops:
+        for idx in (ref, ours):
+            if op[0] == "add":
+                idx.add_items(op[1], op[2])
+            else:
+                idx.delete_vector(op[1])
+    ref.save_index(str(tmp_path / "r.bin"))
+    ours.save_index(str(tmp_path / "o.bin"))
+    a, b = (tmp_path / "r.bin").read_bytes(), (tmp_path / "o.bin").read_bytes()
+    cur = int(np.frombuffer(a[16:24], np.uint64)[0])
+    assert len(a) == len(b) and a[:24] == b[:24]
+    assert a[24:24 + cur * (12 * 4 + 8)] == b[24:24 + cur * (12 * 4 + 8)]
+    maxel, rows, labels = PK.bf_file_to_rows(a, 12)
+    assert maxel == 400 and np.array_equal(rows, ours._rows) and np.array_equal(labels, ours._row_labels)
