@@ -774,6 +774,120 @@ int orc_hnsw_search(void* p, const float* q, uint64_t nq, uint64_t k, uint64_t e
     return 0;
 }
 
+// searchStopConditionClosest with a MultiVectorSearchStopCondition
+// (stop_condition.h:146-216) over a multi-vector index, whose elements carry
+// a uint32 document id right after the vector.  The loop is the non-bare-bone
+// one of base_layer_reference, but its size tests count distinct documents
+// among top_candidates (curr_num_docs against ef_collection =
+// max(ef_collection, num_docs)), and the condition keeps its own max-heap of
+// (distance, document) pairs, popped on every eviction and by
+// filter_results, which trims the result until num_docs documents remain.
+void search_multivector(const Hnsw& h, const float* q, size_t num_docs, size_t ef_coll_in,
+                        std::vector<uint32_t>& vis, uint32_t& tag, SearchOut& out) {
+    out.res.clear();
+    if (h.cur == 0) return;
+    Trace tr;
+    uint32_t ep = descend(h, q, tr);
+    tag++;
+    if (tag == 0) { std::fill(vis.begin(), vis.end(), 0u); tag = 1; }
+    const size_t ef_coll = std::max(ef_coll_in, num_docs);
+    auto doc = [&](uint32_t id) {
+        uint32_t d;
+        memcpy(&d, (const char*)h.vec(id) + h.dim * sizeof(float), 4);
+        return d;
+    };
+    using P = std::pair<float, uint32_t>;
+    CompareByFirst cmp;
+    std::vector<P> top, cand;
+    std::unordered_map<uint32_t, size_t> doc_counter;
+    size_t cur_docs = 0;
+    std::priority_queue<std::pair<float, uint32_t>> results;  // (distance, document)
+    auto add_point = [&](uint32_t id, float d) {
+        const uint32_t dc = doc(id);
+        if (doc_counter[dc] == 0) cur_docs++;
+        results.emplace(d, dc);
+        doc_counter[dc]++;
+    };
+    auto remove_point = [&](uint32_t id) {
+        const uint32_t dc = doc(id);
+        if (--doc_counter[dc] == 0) cur_docs--;
+        results.pop();
+    };
+    const float d0 = dist(h.space, q, h.vec(ep), h.dim);
+    float lb = d0;
+    top.push_back({d0, ep});
+    std::push_heap(top.begin(), top.end(), cmp);
+    add_point(ep, d0);
+    cand.push_back({-d0, ep});
+    std::push_heap(cand.begin(), cand.end(), cmp);
+    vis[ep] = tag;
+    while (!cand.empty()) {
+        const P cp = cand.front();
+        const float cd = -cp.first;
+        if (cd > lb && cur_docs == ef_coll) break;
+        std::pop_heap(cand.begin(), cand.end(), cmp);
+        cand.pop_back();
+        const uint32_t* ll = h.links0(cp.second);
+        const size_t size = Hnsw::count(ll);
+        for (size_t j = 1; j <= size; j++) {
+            const uint32_t c = ll[j];
+            if (vis[c] == tag) continue;
+            vis[c] = tag;
+            const float d = dist(h.space, q, h.vec(c), h.dim);
+            if (cur_docs < ef_coll || lb > d) {
+                cand.push_back({-d, c});
+                std::push_heap(cand.begin(), cand.end(), cmp);
+                top.push_back({d, c});
+                std::push_heap(top.begin(), top.end(), cmp);
+                add_point(c, d);
+                while (cur_docs > ef_coll) {
+                    const uint32_t gone = top.front().second;
+                    std::pop_heap(top.begin(), top.end(), cmp);
+                    top.pop_back();
+                    remove_point(gone);
+                }
+                if (!top.empty()) lb = top.front().first;
+            }
+        }
+    }
+    std::vector<std::pair<float, uint64_t>> res(top.size());
+    size_t sz = top.size();
+    while (!top.empty()) {
+        res[--sz] = {top.front().first, (uint64_t)top.front().second};
+        std::pop_heap(top.begin(), top.end(), cmp);
+        top.pop_back();
+    }
+    while (cur_docs > num_docs && !res.empty()) {
+        const uint32_t dc = results.top().second;
+        if (--doc_counter[dc] == 0) cur_docs--;
+        results.pop();
+        res.pop_back();
+    }
+    out.res = std::move(res);
+}
+
+// Batched multi-vector search; up to `cap` results per query (internal ids,
+// as the reference returns them), counts[i] = result size or -1 beyond cap.
+int orc_hnsw_search_multivector(void* p, const float* q, uint64_t nq, uint64_t num_docs, uint64_t ef_coll,
+                                uint64_t cap, uint64_t* ids, float* dists, int32_t* counts, int nthreads) {
+    auto* h = (Hnsw*)p;
+    if (nthreads <= 0) nthreads = (int)std::thread::hardware_concurrency();
+    std::vector<std::vector<uint32_t>> vis(nthreads, std::vector<uint32_t>());
+    std::vector<uint32_t> tags(nthreads, 0);
+    std::vector<SearchOut> outs(nthreads);
+    parallel_for(nq, nthreads, [&](size_t i, int t) {
+        if (vis[t].size() != h->cur) vis[t].assign(h->cur + 1, 0);
+        search_multivector(*h, q + i * h->dim, num_docs, ef_coll, vis[t], tags[t], outs[t]);
+        auto& r = outs[t].res;
+        counts[i] = r.size() <= cap ? (int32_t)r.size() : -1;
+        for (size_t j = 0; j < cap; j++) {
+            ids[i * cap + j] = j < r.size() ? r[j].second : ~0ull;
+            dists[i * cap + j] = j < r.size() ? r[j].first : std::numeric_limits<float>::infinity();
+        }
+    });
+    return 0;
+}
+
 // Batched epsilon search (searchStopConditionClosest with
 // EpsilonSearchStopCondition).  Outputs max_c slots per query in the
 // reference's result order; counts[i] = results kept.

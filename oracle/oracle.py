@@ -65,6 +65,8 @@ def lib():
         L.orc_hnsw_set_deleted.argtypes = [P, U64, C.c_int]
         L.orc_hnsw_search.restype = C.c_int
         L.orc_hnsw_search.argtypes = [P, P, U64, U64, U64, C.c_int, P, P, P, P, P, C.c_int]
+        L.orc_hnsw_search_multivector.restype = C.c_int
+        L.orc_hnsw_search_multivector.argtypes = [P, P, U64, U64, U64, U64, P, P, P, C.c_int]
         L.orc_hnsw_search_epsilon.restype = C.c_int
         L.orc_hnsw_search_epsilon.argtypes = [P, P, U64, F32, U64, U64, P, P, P, P, C.c_int]
         L.orc_bf_load.restype = P
@@ -146,6 +148,22 @@ class Hnsw:
         if rc != 0:
             raise RuntimeError(lib().orc_last_error().decode())
         return (labels, dists, counts, tr) if trace else (labels, dists, counts)
+
+    def search_multivector(self, q, num_docs, ef_collection, cap, nthreads=0):
+        """searchStopConditionClosest with MultiVectorSearchStopCondition on a
+        multi-vector index (a uint32 document id after each vector): (ids,
+        dists) of `cap` slots in the reference's result order (internal ids),
+        counts (-1 where the result is longer than cap)."""
+        q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+        nq = q.shape[0]
+        ids = np.empty((nq, cap), np.uint64)
+        dists = np.empty((nq, cap), np.float32)
+        counts = np.empty(nq, np.int32)
+        rc = lib().orc_hnsw_search_multivector(self._h, _ptr(q), nq, int(num_docs), int(ef_collection), int(cap),
+                                               _ptr(ids), _ptr(dists), _ptr(counts), nthreads)
+        if rc != 0:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return ids, dists, counts
 
     def search_epsilon(self, q, epsilon, min_candidates, max_candidates, allow=None, nthreads=0):
         """searchStopConditionClosest with EpsilonSearchStopCondition(epsilon,
@@ -234,6 +252,42 @@ def ref_epsilon_search(path, space, q, epsilon, min_candidates, max_candidates, 
     if rc != 0:
         raise RuntimeError("reference epsilon search failed")
     return labels, dists, counts
+
+
+def ref_multivec():
+    """ctypes handle of oracle/_ref/libref_multivec.so (the reference's
+    multi-vector search), or None where it was not built."""
+    path = os.path.join(HERE, "_ref", "libref_multivec.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    P, U64 = C.c_void_p, C.c_uint64
+    L.ref_mv_build.restype = C.c_int
+    L.ref_mv_build.argtypes = [C.c_char_p, C.c_int, P, P, P, U64, U64, U64, U64, U64]
+    L.ref_mv_search.restype = C.c_int
+    L.ref_mv_search.argtypes = [C.c_char_p, C.c_int, U64, P, U64, U64, U64, U64, P, P, P]
+    return L
+
+
+def ref_mv_build(path, space, x, docs, labels, M=16, efc=100, seed=100):
+    x = np.ascontiguousarray(x, np.float32)
+    d = np.ascontiguousarray(docs, np.uint32)
+    lab = np.ascontiguousarray(labels, np.uint64)
+    if ref_multivec().ref_mv_build(str(path).encode(), SPACES[space], _ptr(x), _ptr(d), _ptr(lab), x.shape[0],
+                                   x.shape[1], M, efc, seed) != 0:
+        raise RuntimeError("reference multi-vector build failed")
+
+
+def ref_mv_search(path, space, q, num_docs, ef_collection, cap):
+    q = np.ascontiguousarray(np.atleast_2d(q), np.float32)
+    nq, dim = q.shape
+    ids = np.empty((nq, cap), np.uint64)
+    dists = np.empty((nq, cap), np.float32)
+    counts = np.empty(nq, np.int32)
+    if ref_multivec().ref_mv_search(str(path).encode(), SPACES[space], dim, _ptr(q), nq, int(num_docs),
+                                    int(ef_collection), int(cap), _ptr(ids), _ptr(dists), _ptr(counts)) != 0:
+        raise RuntimeError("reference multi-vector search failed")
+    return ids, dists, counts
 
 
 def ref_l2u8():

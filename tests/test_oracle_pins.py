@@ -292,3 +292,39 @@ def test_oracle_l2_uint8_vs_reference_fresh(tmp_path):
             ol, od, oc = o.search(q.astype(np.float32), k, ef, mode=O.REFERENCE)
             assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
             assert np.array_equal(od, rd.astype(np.float32))
+
+
+def test_oracle_multivector_matches_reference_golden():
+    """searchStopConditionClosest with MultiVectorSearchStopCondition over a
+    multi-vector L2 index (a document id after each vector): the oracle's
+    restatement against the reference's recorded results (ids in result
+    order, distances, counts) for four (num_docs, ef_collection) pairs."""
+    e = np.load(f"{GOLDEN}/multivec.npz")
+    o = O.Hnsw(f"{GOLDEN}/hnsw_mv_l2_d16.bin", "l2", 16)
+    for nd, efc in ((10, 15), (5, 5), (3, 20), (20, 10)):
+        key = f"docs{nd}_efc{efc}"
+        ids, d, c = o.search_multivector(e["queries"], nd, efc, 400)
+        assert np.array_equal(c, e[key + "/counts"]), key
+        assert np.array_equal(ids, e[key + "/ids"]), key
+        assert np.array_equal(d.view(np.uint32), e[key + "/dists"].view(np.uint32)), key
+        # every result row holds exactly num_docs documents
+        for i in range(e["queries"].shape[0]):
+            assert len(set(e["docs"][ids[i, :c[i]].astype(np.int64)].tolist())) == nd
+
+
+def test_oracle_multivector_vs_reference_fresh(tmp_path):
+    if O.ref_multivec() is None:
+        pytest.skip("oracle/_ref/libref_multivec.so not built")
+    rng = np.random.default_rng(77)
+    for n_docs_total, dim in ((30, 8), (200, 24)):
+        x = rng.standard_normal((1500, dim)).astype(np.float32)
+        docs = rng.integers(0, n_docs_total, 1500)
+        q = rng.standard_normal((40, dim)).astype(np.float32)
+        path = tmp_path / f"mv{dim}.bin"
+        O.ref_mv_build(path, "l2", x, docs, np.arange(1500), M=12, efc=80)
+        o = O.Hnsw(str(path), "l2", dim)
+        for nd, efc in ((4, 8), (12, 12), (2, 30)):
+            rl, rd, rc = O.ref_mv_search(path, "l2", q, nd, efc, 600)
+            ol, od, oc = o.search_multivector(q, nd, efc, 600)
+            assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
+            assert np.array_equal(od.view(np.uint32), rd.view(np.uint32))
