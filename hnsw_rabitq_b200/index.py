@@ -259,13 +259,28 @@ class Index(_GpuIndex):
         ids = [] if ids is None else np.asarray(ids)
         if isinstance(ids, np.ndarray) and ids.ndim == 0:
             raise ValueError("get_items accepts a list of indices and returns a list of vectors")
+        self._require()
         elem = np.uint8 if self.space == "l2_uint8" else np.float32
-        rows = pickling.items_from_file(self._file_bytes(), list(ids), self.dim, elem)
+        where = {int(v): i for i, v in enumerate(self.labels_by_internal_id().tolist())}
+        rows = np.empty((len(ids), self.dim), np.float32)
+        with pickling.RecordReader(self._source if self._source is not None else self._state_bytes) as rd:
+            for r, lab in enumerate(np.asarray(ids).reshape(-1).tolist()):
+                i = where.get(int(lab))
+                if i is None:
+                    raise RuntimeError("Label not found")
+                # a mark changed in this session overrides the file's
+                dead = self._marks[int(lab)] if int(lab) in self._marks else rd.deleted(i)
+                if dead:
+                    raise RuntimeError("Label not found")
+                rows[r] = rd.vector(i, self.dim, elem)
         return rows.tolist() if return_type == "list" else rows
 
     def index_file_size(self) -> int:
         """HierarchicalNSW::indexFileSize (hnswalg.h:658-683): bytes save_index writes."""
-        return len(self._file_bytes())
+        self._require()
+        if self._source is not None:
+            return os.path.getsize(self._source)
+        return len(self._state_bytes)
 
     def resize_index(self, new_size: int) -> None:
         """resizeIndex (hnswalg.h:633-656): the capacity recorded with the

@@ -167,3 +167,43 @@ def bf_rows_to_file(rows: np.ndarray, labels: np.ndarray, max_elements: int, dim
         rec[:cur, :dim * 4] = np.ascontiguousarray(rows, np.float32).view(np.uint8).reshape(cur, dim * 4)
         rec[:cur, dim * 4:] = np.ascontiguousarray(labels, np.uint64).view(np.uint8).reshape(cur, 8)
     return _BF_HEADER.pack(rec.shape[0], size_per, cur) + rec.tobytes()
+
+
+class RecordReader:
+    """Reads single elements of a saveIndex file (a path, read by seeking, or
+    the file's bytes) without loading the whole level-0 block."""
+
+    def __init__(self, src):
+        self._bytes = src if isinstance(src, (bytes, bytearray)) else None
+        self._f = None if self._bytes is not None else open(src, "rb")
+        head = self._read(0, _HEADER.size)
+        (self.off0, _, self.cur, self.size_data, self.label_off, self.data_off, *_rest) = _HEADER.unpack(head)
+
+    def _read(self, pos: int, n: int) -> bytes:
+        if self._bytes is not None:
+            return bytes(self._bytes[pos:pos + n])
+        self._f.seek(pos)
+        return self._f.read(n)
+
+    def _rec(self, i: int) -> int:
+        if not 0 <= i < self.cur:
+            raise IndexError(i)
+        return _HEADER.size + i * self.size_data
+
+    def deleted(self, i: int) -> bool:
+        return (self._read(self._rec(i) + self.off0 + 2, 1)[0] & 1) != 0
+
+    def vector(self, i: int, dim: int, elem_dtype=np.float32) -> np.ndarray:
+        w = dim * np.dtype(elem_dtype).itemsize
+        return np.frombuffer(self._read(self._rec(i) + self.data_off, w), elem_dtype).astype(np.float32)
+
+    def close(self):
+        if self._f is not None:
+            self._f.close()
+            self._f = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -141,3 +141,48 @@ def test_bf_save_index_matches_the_reference(tmp_path, space):
     assert a[24:24 + cur * (12 * 4 + 8)] == b[24:24 + cur * (12 * 4 + 8)]
     maxel, rows, labels = PK.bf_file_to_rows(a, 12)
     assert maxel == 400 and np.array_equal(rows, ours._rows) and np.array_equal(labels, ours._row_labels)
+
+
+def test_record_reader_matches_whole_file_reads(tmp_path):
+    hnswlib = ref_or_skip()
+    p, _ = _ref_index(hnswlib, "l2", 16, 300, 0, 8, seed=4)
+    p.mark_deleted(21)
+    path = tmp_path / "r.bin"
+    p.save_index(str(path))
+    buf = path.read_bytes()
+    st = PK.file_bytes_to_state(buf, "l2", 16, ef=10)
+    for src in (str(path), buf):
+        with PK.RecordReader(src) as rd:
+            assert rd.cur == 300
+            for i, lab in enumerate(st["label_lookup_external"].tolist()):
+                assert rd.deleted(i) == (lab == 21)
+                if lab != 21:
+                    assert np.array_equal(rd.vector(i, 16), PK.items_from_file(buf, [lab], 16)[0])
+
+
+def test_get_items_uses_labels_and_marks_without_gpu(tmp_path, monkeypatch):
+    """Index.get_items over a recorder in place of the GPU handle: labels
+    from the index, delete marks from the file and from this session."""
+    hnswlib = ref_or_skip()
+    p, _ = _ref_index(hnswlib, "l2", 16, 200, 0, 8, seed=6)
+    p.mark_deleted(11)
+    path = tmp_path / "g.bin"
+    p.save_index(str(path))
+    buf = path.read_bytes()
+    idx = H.Index("l2", 16)
+    idx._h = object()  # never passed to the library here
+    idx._source = str(path)
+    idx._labels = PK.file_bytes_to_state(buf, "l2", 16, ef=10)["label_lookup_external"]
+    try:
+        assert np.array_equal(idx.get_items([1, 6, 16]), np.asarray(p.get_items([1, 6, 16])))
+        assert idx.get_items([1], return_type="list") == np.asarray(p.get_items([1])).tolist()
+        with pytest.raises(RuntimeError, match="Label not found"):
+            idx.get_items([11])
+        idx._marks[11] = False  # unmarked in this session
+        assert np.array_equal(idx.get_items([11]), PK.items_from_file(PK.set_delete_marks(buf, set(), {11}), [11], 16))
+        idx._marks[6] = True
+        with pytest.raises(RuntimeError, match="Label not found"):
+            idx.get_items([6])
+        assert idx.index_file_size() == len(buf)
+    finally:
+        idx._h = None
