@@ -58,7 +58,14 @@ extern "C" {
                                      pointers; the call is asynchronous on
                                      `stream` and does not synchronise.  Without
                                      it they are host pointers and the call
-                                     copies, launches and synchronises.         */
+                                     copies, launches and synchronises.
+                                     Tie-exact searches (HNSWGPU_EXACT_TIES,
+                                     hnswgpu_search_epsilon) of one index share
+                                     its scratch (candidate-heap tails, the tie
+                                     list): asynchronous ones must not overlap
+                                     on the GPU, so issue them on one stream or
+                                     order their streams (the serving loop runs
+                                     one at a time).                            */
 #define HNSWGPU_TRACE 0x2u        /* write per-query work counters to `trace`   */
 #define HNSWGPU_EXACT_TIES 0x4u   /* HNSW: replay the reference's heap order so
                                      that exact distance ties resolve as in
