@@ -288,3 +288,26 @@ def test_full_size_parity_1m():
         assert np.array_equal(gl, cl) and np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
         same, bad = compare_rows(gl, rl, rt[:, 4])
         assert same >= 0.995 and not bad, (ef, same, bad[:5])
+
+
+def test_config1_uniform_10k():
+    """The CPU-runnable configuration on the GPU: 10,000 x 128 U[0,1)
+    vectors, M=16, ef_construction=200, random_seed=100, 1,000 queries, k=10,
+    ef=50: the default (reference) tie order returns the reference's results
+    for every query, the id order the canonical oracle's; the brute force
+    returns the reference's exact top-10."""
+    import os
+    import tempfile
+
+    from hnsw_rabitq_b200.datasets import uniform_10k
+    x, q = uniform_10k()
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "c1.bin")
+        build_hnsw(path, x, "l2", M=16, efc=200, seed=100, num_threads=8)
+        check_parity(path, "l2", q, 10, 50)
+    b = H.BFIndex("l2", 128)
+    b.init_index(x.shape[0])
+    b.add_items(x)
+    gl, gd = b.knn_query(q, k=10)
+    ml, md = O.bf_matrix("l2", x, q, 10)
+    assert np.array_equal(gl, ml) and np.array_equal(gd.view(np.uint32), md.view(np.uint32))

@@ -328,3 +328,29 @@ def test_oracle_multivector_vs_reference_fresh(tmp_path):
             ol, od, oc = o.search_multivector(q, nd, efc, 600)
             assert np.array_equal(oc, rc) and np.array_equal(ol, rl)
             assert np.array_equal(od.view(np.uint32), rd.view(np.uint32))
+
+
+def test_config1_uniform_10k_oracle_vs_reference(tmp_path):
+    """The CPU-runnable configuration: 10,000 x 128 U[0,1) vectors
+    (default_rng(0)), M=16, ef_construction=200, random_seed=100, 1,000 queries
+    from the same stream, k=10, ef=50, with BFIndex exact top-10 as ground
+    truth.  The oracle's reference mode returns the reference's knn_query
+    results for every query, and its brute force the reference's BFIndex."""
+    from hnsw_rabitq_b200.datasets import uniform_10k
+    hnswlib = ref_or_skip()
+    x, q = uniform_10k()
+    p = build_hnsw(tmp_path / "c1.bin", x, "l2", M=16, efc=200, seed=100, num_threads=8)
+    p.set_ef(50)
+    rl, rd = p.knn_query(q, k=10, num_threads=8)
+    o = O.Hnsw(str(tmp_path / "c1.bin"), "l2", 128)
+    ol, od, _ = o.search(q, 10, 50, mode=O.REFERENCE)
+    assert np.array_equal(ol, rl) and np.array_equal(od.view(np.uint32), rd.view(np.uint32))
+    bf = hnswlib.BFIndex("l2", 128)
+    bf.init_index(x.shape[0])
+    bf.add_items(x)
+    gl, gd = bf.knn_query(q, k=10)
+    ml, md = O.bf_matrix("l2", x, q, 10)
+    assert np.array_equal(ml, gl) and np.array_equal(md.view(np.uint32), gd.view(np.uint32))
+    # i.i.d. uniform 128-d data is hard for a graph: recall@10 at ef 50 is ~0.65
+    recall = np.mean([len(np.intersect1d(rl[i], gl[i])) / 10 for i in range(q.shape[0])])
+    assert 0.5 < recall < 0.8
