@@ -267,7 +267,8 @@ def recall(found, gt):
 # -------------------------------------------------------------- our GPU arm
 class DeviceLoop:
     """Device-resident batch search through the C ABI (HNSWGPU_DEVICE_PTRS):
-    queries and outputs stay in HBM, one kernel launch per step."""
+    queries and outputs stay in HBM; one kernel launch per step (two for the
+    reference tie order, whose two-pass search lists then replays)."""
 
     def __init__(self, idx, q, dev, k=10):
         import torch
