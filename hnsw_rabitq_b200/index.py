@@ -615,8 +615,8 @@ class BFIndex(_GpuIndex):
     def save_index(self, path_to_index: str) -> None:
         """BruteforceSearch::saveIndex (bruteforce.h:128-139).  A loaded,
         unchanged index is written back as loaded; rows added here are written
-        as given (l2 / ip; the cosine space normalises them on the GPU, so an
-        in-memory cosine index cannot be written)."""
+        as the reference stores them (cosine: normalised with the reference's
+        arithmetic)."""
         from . import pickling
         if self._rows is None:
             if getattr(self, "_source", None) is None:
@@ -624,10 +624,8 @@ class BFIndex(_GpuIndex):
             with open(self._source, "rb") as f:
                 buf = f.read()
         else:
-            if self.space == "cosine":
-                raise NotImplementedError("save_index of a cosine BFIndex built in memory is not supported")
-            buf = pickling.bf_rows_to_file(self._rows, self._row_labels, max(self._maxel, self._rows.shape[0]),
-                                           self.dim)
+            rows = pickling.normalize_rows(self._rows) if self.space == "cosine" else self._rows
+            buf = pickling.bf_rows_to_file(rows, self._row_labels, max(self._maxel, self._rows.shape[0]), self.dim)
         with open(path_to_index, "wb") as f:
             f.write(buf)
 

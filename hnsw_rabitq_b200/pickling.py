@@ -207,3 +207,40 @@ class RecordReader:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def _fma32(a: np.ndarray, b: np.ndarray, c: np.ndarray) -> np.ndarray:
+    """float32 fused multiply-add, correctly rounded: the float64 product of
+    two float32 values is exact, TwoSum gives the exact error of adding c, and
+    that error decides the one case float64 rounding can get wrong (a sum
+    exactly halfway between two float32 values)."""
+    p = a.astype(np.float64) * b.astype(np.float64)
+    c64 = c.astype(np.float64)
+    t = p + c64
+    bb = t - p
+    err = (p - (t - bb)) + (c64 - bb)
+    r = t.astype(np.float32)
+    up = np.nextafter(r, np.float32(np.inf))
+    dn = np.nextafter(r, np.float32(-np.inf))
+    r64 = r.astype(np.float64)
+    r = np.where((t == (r64 + up.astype(np.float64)) / 2) & (err > 0), up, r)
+    r = np.where((t == (r64 + dn.astype(np.float64)) / 2) & (err < 0), dn, r)
+    return r.astype(np.float32)
+
+
+def normalize_rows(x: np.ndarray) -> np.ndarray:
+    """The reference's normalize_vector (bindings.cpp:241-248) over rows, in
+    the arithmetic of its optimised build (the one the GPU's norm_scale
+    reproduces): the squares of the first dim - dim % 4 elements are rounded
+    and added in order, the last dim % 4 are fused multiply-adds, then
+    x * (1 / (sqrt(norm) + 1e-30)), all in float32."""
+    x = np.ascontiguousarray(x, np.float32)
+    n, dim = x.shape
+    n4 = dim & ~3
+    s = np.zeros(n, np.float32)
+    for i in range(n4):
+        s = (s + (x[:, i] * x[:, i]).astype(np.float32)).astype(np.float32)
+    for i in range(n4, dim):
+        s = _fma32(x[:, i], x[:, i], s)
+    sc = (np.float32(1.0) / (np.sqrt(s) + np.float32(1e-30))).astype(np.float32)
+    return (x * sc[:, None]).astype(np.float32)

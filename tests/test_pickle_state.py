@@ -113,7 +113,7 @@ def test_constructor_overloads_unloaded():
         H.Index("l2", 4).get_items([1], return_type="tuple")
 
 
-@pytest.mark.parametrize("space", ["l2", "ip"])
+@pytest.mark.parametrize("space", ["l2", "ip", "cosine"])
 def test_bf_save_index_matches_the_reference(tmp_path, space):
     """BFIndex built in memory (init_index / add_items / delete_vector, no GPU
     needed) saves the reference's file: header and every current record
@@ -140,7 +140,23 @@ def test_bf_save_index_matches_the_reference(tmp_path, space):
     assert len(a) == len(b) and a[:24] == b[:24]
     assert a[24:24 + cur * (12 * 4 + 8)] == b[24:24 + cur * (12 * 4 + 8)]
     maxel, rows, labels = PK.bf_file_to_rows(a, 12)
-    assert maxel == 400 and np.array_equal(rows, ours._rows) and np.array_equal(labels, ours._row_labels)
+    want = PK.normalize_rows(ours._rows) if space == "cosine" else ours._rows
+    assert maxel == 400 and np.array_equal(rows, want) and np.array_equal(labels, ours._row_labels)
+
+
+def test_normalize_rows_is_the_references(tmp_path):
+    """normalize_rows against the rows the reference's cosine BFIndex
+    stores, bit for bit, for dims with and without a remainder mod 4."""
+    hnswlib = ref_or_skip()
+    rng = np.random.default_rng(8)
+    for dim in (1, 3, 7, 16, 33, 100, 768):
+        x = (rng.standard_normal((300, dim)) * rng.uniform(0.01, 100, (300, 1))).astype(np.float32)
+        b = hnswlib.BFIndex("cosine", dim)
+        b.init_index(300)
+        b.add_items(x)
+        b.save_index(str(tmp_path / "n.bin"))
+        _, rows, _ = PK.bf_file_to_rows((tmp_path / "n.bin").read_bytes(), dim)
+        assert np.array_equal(PK.normalize_rows(x).view(np.uint32), rows.view(np.uint32)), dim
 
 
 def test_record_reader_matches_whole_file_reads(tmp_path):
