@@ -27,6 +27,14 @@
 //                   (distance, internal id) and a sorted candidate pool, which
 //                   is what the GPU kernel computes (see canonical_search()).
 //   * brute force -- BruteforceSearch::searchKnn (bruteforce.h:106-125).
+//   * stop conditions -- searchStopConditionClosest (hnswalg.h:1326-1377) with
+//                   EpsilonSearchStopCondition and MultiVectorSearchStopCondition
+//                   (stop_condition.h), pinned to the reference by the harnesses
+//                   oracle/ref_stopcond.cpp and oracle/ref_multivec.cpp.
+//   * L2SpaceI   -- space 3: uint8 elements, integer squared L2
+//                   (space_l2.h:255-323), pinned by oracle/ref_l2u8.cpp.
+//   * listing    -- mode 1 also marks the runs the GPU's two-pass tie-exact
+//                   search lists for the heap replay (Trace::listed).
 #include <algorithm>
 #include <atomic>
 #include <cmath>

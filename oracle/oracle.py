@@ -6,7 +6,10 @@ module, always as the checker.  The product package never imports it.
 ``Hnsw.search(mode=REFERENCE)`` reproduces hnswlib 0.9.0's ``searchKnn``
 bit-for-bit (heap tie order included); ``mode=CANONICAL`` is the tie-broken
 form the CUDA kernel implements.  ``ref_module()`` imports the reference's own
-compiled extension from ``oracle/_ref`` when it has been built.
+compiled extension from ``oracle/_ref`` when it has been built;
+``ref_stopcond()``, ``ref_l2u8()`` and ``ref_multivec()`` load the harnesses
+compiled from the reference's headers there (epsilon search, L2SpaceI
+indexes, multi-vector search), which the Python bindings cannot reach.
 """
 from __future__ import annotations
 
