@@ -221,7 +221,7 @@ def ref_module():
     from oracle import oracle as O
     mod = O.ref_module()
     if mod is None:
-        raise SystemExit("the reference extension (oracle/_ref) is not built: run `make -C oracle ref`")
+        raise SystemExit("the reference extension (oracle/_ref) is not built: run `make -C oracle ref REF=<hnswlib source tree>`")
     return mod
 
 

@@ -78,6 +78,8 @@ SIGNATURES = {
     "hnswgpu_search": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_get_status": (C.c_int, [P, C.POINTER(U32)]),
     "hnswgpu_search_noalloc": (C.c_int, [P, P, U64, U64, U64, U32, P, P, P, P, P]),
+    "hnswgpu_noalloc_get_status": (C.c_int, [C.c_int, P, C.POINTER(U32)]),
+    "hnswgpu_selftest_wait_timeout": (C.c_int, [C.c_int, C.POINTER(U32)]),
     "hnswgpu_search_epsilon": (C.c_int, [P, P, U64, C.c_float, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_set_termination_model": (C.c_int, [P, P, U32, C.c_float]),
     "hnswgpu_search_checkpoints": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), U32, U32, P, P, P, P, P, P]),

@@ -55,13 +55,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs = []
+    headers = [f for f in deps() if not f.endswith(".cu")]
+    newest_header = max((os.path.getmtime(f) for f in headers), default=0.0)
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        # an object is reused when it is newer than its source and every header
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) > max(os.path.getmtime(src), newest_header):
+            continue
         cmd = [nvcc()] + ARCH + FLAGS + ["-I", INCLUDE, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
-        objs.append(obj)
     tmp = LIB + ".tmp"
     cmd = [nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lpthread"]
     subprocess.check_call(cmd)

@@ -37,6 +37,11 @@ __device__ __forceinline__ uint64_t mkkey(float d, uint32_t id) { return ((uint6
 __device__ __forceinline__ uint32_t khi(uint64_t k) { return (uint32_t)(k >> 32); }
 __device__ __forceinline__ uint32_t kid(uint64_t k) { return (uint32_t)k & ~EXP_BIT; }
 
+// Slot of node `id` in a direct-mapped visited cache of 2^log2v entries.
+__device__ __forceinline__ uint32_t vis_slot(uint32_t id, uint32_t log2v) {
+    return (id * 0x9E3779B1u) >> (32 - log2v);
+}
+
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
     uint32_t lo = __shfl_sync(FULL, (uint32_t)v, src);
     uint32_t hi = __shfl_sync(FULL, (uint32_t)(v >> 32), src);
@@ -65,10 +70,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
-// Bounded wait for the completion of the phase with parity `parity`.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the completion of the phase with parity `parity`: at most
+// `limit` tries (each may suspend up to MBAR_SUSPEND_NS); false when it gave up.
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, uint32_t parity, uint32_t limit) {
     uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < MBAR_SPIN_LIMIT; it++) {
+    for (uint32_t it = 0; it < limit; it++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -80,6 +86,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         if (done) return true;
     }
     return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    return mbar_wait_limit(bar, parity, MBAR_SPIN_LIMIT);
 }
 // One TMA bulk copy global -> shared (no multicast); `bytes` and both
 // addresses are multiples of 16.

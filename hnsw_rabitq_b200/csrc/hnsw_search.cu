@@ -37,6 +37,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -109,10 +110,6 @@ __device__ __forceinline__ bool is_allowed(const SearchParams& p, uint32_t id) {
     if (p.deleted_bits && ((p.deleted_bits[id >> 5] >> (id & 31)) & 1u)) return false;
     if (p.allow && !p.allow[id]) return false;
     return true;
-}
-
-__device__ __forceinline__ uint32_t vis_slot(uint32_t id, uint32_t log2v) {
-    return (id * 0x9E3779B1u) >> (32 - log2v);
 }
 
 // Count of entries of the sorted array with (key & KEY_MASK) < key.
@@ -1538,17 +1535,44 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocScratchWords
 
 cudaError_t noalloc_scratch_address(int device, uint32_t** out) {
     // Resolved once per device, with that device current: in host code the
-    // symbol's name is only a host-side stand-in, not a device address.
-    static uint32_t* addr[kMaxDevices] = {nullptr};
+    // symbol's name is only a host-side stand-in, not a device address.  Two
+    // threads making their first call at once both resolve it and store the
+    // same value; the slots are atomics, so that is well defined.  The cached
+    // address belongs to the device's current context: after a
+    // cudaDeviceReset on that device the library must be unloaded and loaded
+    // again before this entry point is used.
+    static std::atomic<uint32_t*> addr[kMaxDevices];
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!addr[device]) {
+    uint32_t* a = addr[device].load(std::memory_order_acquire);
+    if (!a) {
         void* ptr = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        addr[device] = static_cast<uint32_t*>(ptr);
+        a = static_cast<uint32_t*>(ptr);
+        addr[device].store(a, std::memory_order_release);
     }
-    *out = addr[device];
+    *out = a;
     return cudaSuccess;
+}
+
+// Self-test of the bounded wait and of the status path that reports it: the
+// thread arms an mbarrier phase for 16 bytes that no copy will ever deliver
+// (no copy is issued, so nothing is in flight when it gives up), waits at most
+// `limit` tries, and records HNSWGPU_STATUS_TIMEOUT_BIT as a search would.
+__global__ void wait_timeout_selftest_kernel(uint32_t limit, uint32_t* status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    fence_mbar_init();
+    __syncwarp();
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16);
+    __syncwarp();
+    const bool ok = mbar_wait_limit(&bar, 0, limit);
+    if (threadIdx.x == 0 && !ok) atomicOr(status, HNSWGPU_STATUS_TIMEOUT_BIT);
+}
+
+cudaError_t launch_wait_timeout_selftest(uint32_t limit, uint32_t* status, cudaStream_t stream) {
+    wait_timeout_selftest_kernel<<<1, 32, 0, stream>>>(limit, status);
+    return cudaGetLastError();
 }
 
 // Pipelined beam over an index with deletions and / or a filter (id order,

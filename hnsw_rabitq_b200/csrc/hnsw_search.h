@@ -136,6 +136,11 @@ constexpr int kMaxDevices = 64;
 // Device address of the fixed scratch on `device`, which must be current.
 cudaError_t noalloc_scratch_address(int device, uint32_t** out);
 
+// Bounded-wait self-test: one warp waits (at most `limit` tries) on an
+// mbarrier phase that never completes and ORs HNSWGPU_STATUS_TIMEOUT_BIT into
+// *status (device memory).
+cudaError_t launch_wait_timeout_selftest(uint32_t limit, uint32_t* status, cudaStream_t stream);
+
 // Fills the off_* fields and warp_smem from the sizes; returns warp_smem.
 size_t warp_smem_layout(SearchParams& p);
 

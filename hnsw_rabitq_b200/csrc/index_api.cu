@@ -943,6 +943,7 @@ int hnswgpu_get_info(const hnswgpu_index* h, hnswgpu_info* o) {
 
 int hnswgpu_set_ef(hnswgpu_index* h, uint64_t ef) {
     if (!h) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+    std::lock_guard<std::mutex> g(h->mu);
     h->ef = ef;
     return HNSWGPU_OK;
 }
@@ -1134,11 +1135,15 @@ int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint6
         if (k == 0 || (nq && (!d_queries || !d_labels || !d_dists || !d_counts)))
             return fail(HNSWGPU_ERR_ARG, "invalid argument");
         // The fixed scratch holds one 32-bit work counter: it hands out query
-        // indices, so a call may carry at most 2^31 queries.
-        if (nq > 0x7fffffffull || k > 0xffffffffull)
+        // indices, so a call may carry at most 2^31 - 1 queries.
+        if (nq > 0x7fffffffull)
             return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc: nq must be < 2^31 (fixed 256-byte scratch)");
+        if (k > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc: k must be < 2^32");
         if (flags & ~(uint32_t)HNSWGPU_EXACT_TIES)
             return fail(HNSWGPU_ERR_ARG, "hnswgpu_search_noalloc: only HNSWGPU_EXACT_TIES may be set");
+        // the index must not change (set_ef, mark_deleted, ...) while the
+        // launch parameters are read from it
+        std::lock_guard<std::mutex> g(h->mu);
         cuda_check(cudaSetDevice(h->device), "cudaSetDevice");
         if (nq == 0) return HNSWGPU_OK;
         cudaStream_t st = (cudaStream_t)stream;
@@ -1155,11 +1160,48 @@ int hnswgpu_search_noalloc(const hnswgpu_index* h, const float* d_queries, uint6
         p.work_counter = scratch + 0;
         p.done_counter = scratch + 1;
         p.status = scratch + 2;
-        // counters and status must start at zero: clear what a previous call
-        // (or an interrupted one) may have left
-        cuda_check(cudaMemsetAsync(scratch, 0, 3 * sizeof(uint32_t), st), "cudaMemsetAsync");
+        // the two counters must start at zero: clear what a previous call (or
+        // an interrupted one) may have left; the status word is left alone, so
+        // that its bits accumulate until hnswgpu_noalloc_get_status reads them
+        cuda_check(cudaMemsetAsync(scratch, 0, 2 * sizeof(uint32_t), st), "cudaMemsetAsync");
         cuda_check(hnswgpu::launch_hnsw_search(p, kspace(h), h->num_sms, st, nullptr),
                    "hnsw_search launch");
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_noalloc_get_status(int device, void* stream, uint32_t* out_bits) {
+    return guarded([&] {
+        if (!out_bits) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        uint32_t* scratch = nullptr;
+        cuda_check(hnswgpu::noalloc_scratch_address(device, &scratch), "cudaGetSymbolAddress");
+        cudaStream_t st = (cudaStream_t)stream;
+        uint32_t v = 0;
+        // ordered after the searches queued on `stream`; the copy into
+        // pageable host memory allocates nothing
+        cuda_check(cudaMemcpyAsync(&v, scratch + 2, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
+                   "cudaMemcpyAsync");
+        cuda_check(cudaMemsetAsync(scratch + 2, 0, sizeof(uint32_t), st), "cudaMemsetAsync");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        *out_bits = v;
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_selftest_wait_timeout(int device, uint32_t* out_bits) {
+    return guarded([&] {
+        if (!out_bits) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        cuda_check(cudaSetDevice(device), "cudaSetDevice");
+        DevBuf<uint32_t> st;
+        st.alloc(1);
+        cuda_check(cudaMemset(st.p, 0, 4), "cudaMemset");
+        // 64 tries of at most 50 us each: the wait gives up within ~3 ms
+        cuda_check(hnswgpu::launch_wait_timeout_selftest(64, st.p, nullptr), "selftest launch");
+        cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+        uint32_t v = 0;
+        cuda_check(cudaMemcpy(&v, st.p, 4, cudaMemcpyDeviceToHost), "cudaMemcpy");
+        *out_bits = v;
         return HNSWGPU_OK;
     });
 }

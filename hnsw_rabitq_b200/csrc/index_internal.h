@@ -108,7 +108,9 @@ struct hnswgpu_index {
     DevBuf<uint8_t> scan_mask;         // exact scan over an index with deletions
     uint32_t term_period = 0;
     float term_logit = 0.f;
-    std::mutex mu;
+    // guards the index state; mutable so that the const allocation-free
+    // search can hold it while it reads that state
+    mutable std::mutex mu;
     ~hnswgpu_index() {
         if (tie_host) cudaFreeHost(tie_host);
         if (tie_ev) cudaEventDestroy(tie_ev);

@@ -91,9 +91,11 @@ extern "C" {
 
 /* kernel status bits (hnswgpu_search_opts.status / hnswgpu_get_status) */
 #define HNSWGPU_STATUS_TIMEOUT 0x1u   /* a bounded wait gave up; results invalid   */
-#define HNSWGPU_STATUS_OVERFLOW 0x2u  /* a filtered search overflowed its
-                                         candidate list; results may differ from
-                                         the reference for the flagged queries   */
+#define HNSWGPU_STATUS_OVERFLOW 0x2u  /* a search overflowed a candidate list
+                                         (filtered search, or the shared-memory
+                                         heap of hnswgpu_search_noalloc); results
+                                         may differ from the reference for the
+                                         flagged queries                        */
 
 typedef struct hnswgpu_index hnswgpu_index;
 
@@ -246,19 +248,42 @@ HNSWGPU_API int hnswgpu_search_epsilon(hnswgpu_index* index, const float* querie
  * the optional allow mask are device pointers, `ef` 0 means the index's ef,
  * flags may only hold HNSWGPU_EXACT_TIES (which here always runs the one-pass
  * heap replay: the two-pass form needs a per-query list); the call is
- * asynchronous on `stream`.
+ * asynchronous on `stream`.  It holds the index's lock while it reads the
+ * index, so it may run beside set_ef / mark_deleted in other threads.
  * The kernel's scratch (work counter, finished-CTA counter, status word) is a
  * fixed 256-byte array in the library's device image instead of per-index
  * memory; nq >= 2^31 is rejected.  Every GPU that loads the library holds that
  * array until the process exits.  The first call on a device resolves the
  * array's device address (cudaGetSymbolAddress with that device current): make
- * it before any stream capture.  All calls on a device share the array, so
- * calls that overlap on the GPU (other streams, or a graph replay while
- * another call runs) race and must not be issued; each call clears the
- * counters before its launch.  Status bits are not reported by this call. */
+ * it before any stream capture; after a cudaDeviceReset the library must be
+ * loaded again.  All calls on a device share the array, so calls that overlap
+ * on the GPU (other streams, or a graph replay while another call runs) race
+ * and must not be issued; each call clears the two counters before its launch.
+ *
+ * With HNSWGPU_EXACT_TIES the reference's candidate heap has no global tail
+ * here: it lives in shared memory only, max(512, 12 * ef) entries, fewer (down
+ * to 4 * ef) where the per-query shared memory runs short, against 28 * ef in
+ * hnswgpu_search.  A query whose heap outgrows it drops pushes and raises
+ * HNSWGPU_STATUS_OVERFLOW; its results may then differ from the reference.
+ * The status bits of these calls (overflow; a bounded wait that timed out,
+ * which invalidates the results) accumulate in the array's status word until
+ * hnswgpu_noalloc_get_status reads them. */
 HNSWGPU_API int hnswgpu_search_noalloc(const hnswgpu_index* index, const float* d_queries, uint64_t nq, uint64_t k,
                                        uint64_t ef, uint32_t flags, const uint8_t* d_allow, uint64_t* d_labels,
                                        float* d_dists, int32_t* d_counts, void* stream);
+
+/* OR of the status bits (HNSWGPU_STATUS_*) raised by hnswgpu_search_noalloc
+ * calls on `device` since the last read; clears them.  Ordered after the work
+ * queued on `stream` and synchronises it; allocates nothing.  No counterpart in
+ * the reference. */
+HNSWGPU_API int hnswgpu_noalloc_get_status(int device, void* stream, uint32_t* out_bits);
+
+/* Self-test of the kernels' bounded waits: launches one warp that waits on a
+ * copy that never arrives, gives up after a few milliseconds and reports
+ * HNSWGPU_STATUS_TIMEOUT in *out_bits, the way a search whose copy stalled
+ * reports it; the device stays usable afterwards.  No counterpart in the
+ * reference (its searches never wait on a device). */
+HNSWGPU_API int hnswgpu_selftest_wait_timeout(int device, uint32_t* out_bits);
 
 /* Ground-truth oracle: float64 distances between each query and m rows
  * given by label (labels: nq x m; out: nq x m doubles, NaN for an unknown

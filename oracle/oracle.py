@@ -31,13 +31,18 @@ SPACES = {"l2": 0, "ip": 1, "cosine": 1, "l2_uint8": 3}
 _lib = None
 
 
-def build(force: bool = False) -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference sources exist)."""
+def build(force: bool = False, ref_dir: str | None = None) -> None:
+    """Compile liboracle.so; with `ref_dir` (or the environment variable
+    HNSW_REFERENCE_DIR), the hnswlib source tree, also the reference's own
+    extension and harnesses into oracle/_ref."""
+    ref_dir = ref_dir or os.environ.get("HNSW_REFERENCE_DIR")
     targets = ["oracle"]
-    if os.path.isdir("/root/reference"):
+    extra = []
+    if ref_dir and os.path.isdir(ref_dir):
         targets.append("ref")
+        extra = [f"REF={ref_dir}"]
     if force or not os.path.exists(LIB_PATH) or targets != ["oracle"]:
-        subprocess.check_call(["make", "-s", "-C", HERE] + targets)
+        subprocess.check_call(["make", "-s", "-C", HERE] + targets + extra)
 
 
 def lib():

@@ -1,7 +1,7 @@
 """Generate tests/golden/epsilon.npz from the reference itself.
 
 Run where the reference's stop-condition harness has been built into
-oracle/_ref (``make -C oracle ref``):
+oracle/_ref (``make -C oracle ref REF=<hnswlib source tree>``):
 
     python tests/golden/make_epsilon_golden.py
 
@@ -37,7 +37,7 @@ SETTINGS = [("q02_min20_max64", 0.02, 20, 64), ("q10_min50_max128", 0.10, 50, 12
 
 def main():
     if O.ref_stopcond() is None:
-        raise SystemExit("oracle/_ref/libref_stopcond.so not built: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref/libref_stopcond.so not built: run `make -C oracle ref REF=<hnswlib source tree>` first")
     g = np.load(os.path.join(HERE, "golden.npz"))
     out = {}
     for name, space, dim in CASES:

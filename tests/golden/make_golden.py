@@ -1,7 +1,7 @@
 """Generate the golden fixtures in this directory from the reference itself.
 
 Run in a container where the reference's own extension has been built into
-oracle/_ref (``make -C oracle ref``):
+oracle/_ref (``make -C oracle ref REF=<hnswlib source tree>``):
 
     python tests/golden/make_golden.py
 
@@ -51,7 +51,7 @@ def data_for(kind, n, dim, seed):
 def main():
     hnswlib = O.ref_module()
     if hnswlib is None:
-        raise SystemExit("oracle/_ref not built: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref not built: run `make -C oracle ref REF=<hnswlib source tree>` first")
     out = {}
     for ci, (name, kind, space, dim, n, M, efc, dk) in enumerate(CASES):
         x = data_for(dk, n, dim, 100 + ci)

@@ -1,6 +1,6 @@
 """Generate the uint8 L2SpaceI fixtures from the reference itself.
 
-Run where oracle/_ref/libref_l2u8.so has been built (``make -C oracle ref``):
+Run where oracle/_ref/libref_l2u8.so has been built (``make -C oracle ref REF=<hnswlib source tree>``):
 
     python tests/golden/make_l2u8_golden.py
 
@@ -36,7 +36,7 @@ def data(n, seed):
 
 def main():
     if O.ref_l2u8() is None:
-        raise SystemExit("oracle/_ref/libref_l2u8.so not built: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref/libref_l2u8.so not built: run `make -C oracle ref REF=<hnswlib source tree>` first")
     x = data(N, 300)
     q = data(NQ, 301)
     labels = np.arange(N, dtype=np.uint64) * 3 + 7

@@ -1,6 +1,6 @@
 """Generate the multi-vector fixtures from the reference itself.
 
-Run where oracle/_ref/libref_multivec.so has been built (``make -C oracle ref``):
+Run where oracle/_ref/libref_multivec.so has been built (``make -C oracle ref REF=<hnswlib source tree>``):
 
     python tests/golden/make_multivec_golden.py
 
@@ -34,7 +34,7 @@ CAP = 400
 
 def main():
     if O.ref_multivec() is None:
-        raise SystemExit("oracle/_ref/libref_multivec.so not built: run `make -C oracle ref` first")
+        raise SystemExit("oracle/_ref/libref_multivec.so not built: run `make -C oracle ref REF=<hnswlib source tree>` first")
     rng = np.random.default_rng(500)
     x = rng.random((1000, 16), dtype=np.float32)
     docs = rng.integers(0, 50, 1000).astype(np.uint32)
