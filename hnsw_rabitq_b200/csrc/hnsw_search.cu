@@ -1427,6 +1427,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP 
 }  // namespace
 
 size_t warp_smem_layout(SearchParams& p) {
+    if (p.lean) return lean_smem_layout(p);
     size_t off = 16;  // mbarrier (8 bytes) + pad
     p.off_query = (uint32_t)off;
     off += (size_t)p.row_floats * 4;
@@ -1590,6 +1591,7 @@ cudaError_t launch_filter(const SearchParams& p, int num_sms, cudaStream_t strea
 }
 
 cudaError_t launch_hnsw_search(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out) {
+    if (p.lean) return lean_eligible(p) ? launch_hnsw_lean(p, space, num_sms, stream, blocks_out) : cudaErrorInvalidValue;
     if (!p.bare && !p.exact && p.fast16 && p.maxM0 <= 32 && p.term_mode != 1 && !p.tie_list)
         return space == 0 ? launch_filter<0>(p, num_sms, stream, blocks_out)
                           : launch_filter<1>(p, num_sms, stream, blocks_out);

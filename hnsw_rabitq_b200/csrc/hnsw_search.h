@@ -124,6 +124,10 @@ struct SearchParams {
     uint32_t tslots;             // traversal rows per staging batch
     uint32_t rerank;             // best candidates re-ranked with fp32 distances
     uint32_t rr_slots;           // fp32 rows per re-rank staging batch
+    // lean fp8 beam (hnsw_lean.cu): id tie order, no filter or deletions;
+    // `lean_w` link rows expanded per iteration (64 link slots per pass)
+    uint32_t lean, lean_w;
+    uint32_t off_q8, off_cid, off_lacc;
     // per-warp shared memory layout
     uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
     uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;
@@ -143,11 +147,20 @@ cudaError_t launch_wait_timeout_selftest(uint32_t limit, uint32_t* status, cudaS
 
 // Fills the off_* fields and warp_smem from the sizes; returns warp_smem.
 size_t warp_smem_layout(SearchParams& p);
+// The lean fp8 beam's per-warp layout (called by warp_smem_layout when p.lean).
+size_t lean_smem_layout(SearchParams& p);
+// Whether the lean fp8 beam can run these parameters: fp8 copy, id tie order,
+// no filter / deletions / checkpoint listing, maxM0 <= 64, fp8 data bytes per
+// row a multiple of 32 and either <= 128 or a multiple of 128.
+bool lean_eligible(const SearchParams& p);
+cudaError_t launch_hnsw_lean(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out);
+constexpr int kLeanWarpsPerBlock = 2;
 
 // Low-precision traversal copies (quantize.cu).  Row layouts:
 //   bf16: dim x bf16, zero padded to a 16-byte multiple;
 //   fp8 : dim x e4m3 (value / scale, scale = max|x| / 448), zero padded to a
-//         16-byte multiple, then 16 bytes holding the float scale.
+//         16-byte multiple, then 16 bytes holding the float scale and the
+//         float squared norm of the dequantized row.
 uint32_t traversal_row_bytes(uint32_t prec, uint32_t dim);
 cudaError_t launch_quantize_rows(const float* src, uint32_t count, uint32_t dim, uint32_t src_stride, uint32_t prec,
                                  unsigned char* dst, cudaStream_t stream);

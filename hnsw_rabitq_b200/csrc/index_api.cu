@@ -425,13 +425,15 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     }
     p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
     if (prec) {
-        if (!p.fast16 || p.maxM0 > 32 || exact)
-            throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
-                           "low-precision traversal needs dim % 16 == 0, maxM0 <= 32 and the id tie order");
+        const char* need =
+            "low-precision traversal needs dim % 16 == 0, maxM0 <= 32 (fp8 without deletions or a filter: "
+            "maxM0 <= 64) and the id tie order";
+        if (!p.fast16 || exact) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, need);
         if (!h->tcopy[prec].p) throw ApiError(HNSWGPU_ERR_ARG, "traversal copy not built");
         p.prec = prec;
         p.tvecs = h->tcopy[prec].p;
         p.trow_bytes = hnswgpu::traversal_row_bytes(prec, (uint32_t)h->dim);
+        if (p.maxM0 > 32 && !hnswgpu::lean_eligible(p)) throw ApiError(HNSWGPU_ERR_UNSUPPORTED, need);
         // staging stride: a multiple of 64 bytes with an odd count of 64-byte
         // units, so the two rows a quarter warp reads hit disjoint bank halves
         uint32_t st = (p.trow_bytes + 63) / 64;
@@ -444,18 +446,23 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
         if (getenv("HNSWGPU_DEBUG_NO_RERANK")) p.rerank = 0;
 #endif
     }
+    // the lean fp8 beam (no row staging, tensor-core distances, two link rows
+    // per iteration where maxM0 <= 32) serves unfiltered id-order fp8 searches
+    p.lean = hnswgpu::lean_eligible(p) ? 1u : 0u;
+    p.lean_w = p.maxM0 <= 32 ? 2u : 1u;
+    const size_t wpb = p.lean ? hnswgpu::kLeanWarpsPerBlock : hnswgpu::kWarpsPerBlock;
     size_t ws = hnswgpu::warp_smem_layout(p);
     int max_optin = 0;
     cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
-    while (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin && p.log2_vis > 8) {
+    while (!p.lean && ws * wpb > (size_t)max_optin && p.log2_vis > 8) {
         p.log2_vis--;
         ws = hnswgpu::warp_smem_layout(p);
     }
-    while (exact && ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin && p.cand_cap > 4u * p.ef) {
+    while (exact && ws * wpb > (size_t)max_optin && p.cand_cap > 4u * p.ef) {
         p.cand_cap -= p.ef;
         ws = hnswgpu::warp_smem_layout(p);
     }
-    if (ws * hnswgpu::kWarpsPerBlock > (size_t)max_optin)
+    if (ws * wpb > (size_t)max_optin)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
     return p;
 }

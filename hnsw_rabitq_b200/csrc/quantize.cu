@@ -4,10 +4,13 @@
 //   bf16: round-to-nearest bf16 per element (exact for integers up to 256,
 //         i.e. for 8-bit image / SIFT-style data);
 //   fp8 : e4m3 per element of x / s with s = max|x| / 448 (the largest finite
-//         e4m3), saturating, plus s stored in the row's 16-byte tail.
+//         e4m3), saturating; the row's 16-byte tail holds s and the squared
+//         norm of the dequantized row (s * e4m3 value per element), for the
+//         |q|^2 - 2 q.x + |x|^2 form of the tensor-core distances.
 // The search kernel accumulates distances from these copies in fp32 and then
 // re-ranks its best candidates with the exact float32 rows.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
@@ -44,12 +47,18 @@ __global__ void quantize_rows_kernel(const float* __restrict__ src, uint32_t cou
     const float scale = amax > 0.f ? amax / 448.0f : 1.0f;
     const float inv = 1.0f / scale;
     const uint32_t data_bytes = row_bytes - 16;
+    float sq = 0.f;  // squared norm of the dequantized row (scale * e4m3 value)
     for (uint32_t i = 2 * lane; i < data_bytes; i += 64) {
         float2 v = make_float2(i < dim ? x[i] * inv : 0.f, i + 1 < dim ? x[i + 1] * inv : 0.f);
         __nv_fp8x2_storage_t q = __nv_cvt_float2_to_fp8x2(v, __NV_SATFINITE, __NV_E4M3);
         *reinterpret_cast<__nv_fp8x2_storage_t*>(out + i) = q;
+        const float2 back = __half22float2(__half2(__nv_cvt_fp8x2_to_halfraw2(q, __NV_E4M3)));
+        const float a = scale * back.x, b = scale * back.y;
+        sq = fmaf(a, a, fmaf(b, b, sq));
     }
-    if (lane < 4) reinterpret_cast<float*>(out + data_bytes)[lane] = lane == 0 ? scale : 0.f;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    if (lane < 4) reinterpret_cast<float*>(out + data_bytes)[lane] = lane == 0 ? scale : (lane == 1 ? sq : 0.f);
 }
 
 }  // namespace
