@@ -12,23 +12,30 @@ search, with the plain FP32 beam (both tie orders) measured beside it in the
 same run.  Recall is measured against exact top-10 from the GPU brute force
 (bit-identical to the reference's BruteforceSearch).
 
-* plain FP32: the smallest ef of the sweep 10..400 whose recall@10 meets the
-  target, device-resident timed loop.
+* plain FP32: every ef of the sweep 10..400 timed (QPS and recall@10 per
+  ef, both tie orders); the operating point is the smallest ef whose recall
+  meets the target, timed over the full K steps.  The reference tie order
+  returns hnswlib's own results (the parity contract); the id order breaks
+  exact distance ties by internal id, and the share of its rows identical to
+  the reference order is reported.
+* fp8 at fixed ef: the same sweep over the fp8 beam (the learned stop's
+  fallback and cap).
 * learned + FP8 (``value``): the termination network is trained on the GPU
   from checkpoint traces of 20,000 training queries (a query stream disjoint
   from the 10,000 evaluation queries), its cap and logit threshold
-  calibrated on a held-out third of them at the target recall (as the plain
-  arm's ef is chosen at the target); K launches over the 10,000 resident
-  queries, timed with CUDA events on the launch stream.  If the evaluation
-  recall falls short of the target, the calibration target is raised (no
-  retraining) until it does not.
+  calibrated on a held-out third of them at the target recall; a second
+  held-out stream of 5,000 queries checks the calibrated recall and, if it
+  falls short, the calibration target is raised (no retraining).  The
+  evaluation queries never inform a choice.  K launches over the 10,000
+  resident queries, timed with CUDA events on the launch stream.
 * ``e2e``    -- the learned + FP8 search through the C ABI (hnswgpu_search)
   with pinned host buffers: host->device copy of the queries, search,
   device->host copy of the labels/distances/counts every step, wall clock.
 * ``roofline`` -- HBM bound: algorithmic bytes per query of the headline
   kernel from its own work counters (link lists x their size, fp8 rows of
-  144 B, float32 upper-layer and re-rank rows of 512 B), divided by the
-  kernel time; the plain beam's fraction (bytes from the oracle's trace at
+  136 B -- 128 e4m3 bytes, scale and squared norm -- for upper-layer and
+  level-0 distances, float32 re-rank rows of 512 B), divided by the kernel
+  time; the plain beam's fraction (bytes from the oracle's trace at
   the same ef) sits under ``plain_fp32``.
 * ``cpu_baseline`` -- the reference's own knn_query (oracle/_ref) on the
   host cores of this machine, all threads, same index / queries, at the
@@ -356,18 +363,22 @@ def e2e_qps(idx, q, o_flags, ef, precision, rerank, steps, warmup, dist, expect,
     return dist.world * nq * steps / dt, int(q.nbytes), int(nq * k * 8 + nq * k * 4 + nq * 4)
 
 
-def plain_sweep(idx, loop, q, gt, target, tie_order, fixed_ef=0):
-    """Smallest ef of the sweep whose recall@10 meets the target."""
+def plain_sweep(idx, loop, q, gt, target, tie_order, fixed_ef=0, precision=0, dist=None):
+    """Every ef of the sweep, timed (5 steps after 2 warm-up steps, device
+    events): recall@10 and QPS per ef.  Returns the smallest ef whose
+    recall meets the target, the flags and the curve."""
     from hnsw_rabitq_b200 import _capi
     flags = _capi.EXACT_TIES if tie_order == "reference" else 0
     sweep, ef_star = [], fixed_ef
     for ef in ([fixed_ef] if fixed_ef else EFS):
-        loop.step(loop.opts(ef, flags))
+        o = loop.opts(ef, flags, precision)
+        loop.step(o)
         r = recall(loop.labels(), gt) if gt is not None else None
-        sweep.append({"ef": ef, "recall": None if r is None else round(r, 5)})
+        ms, _ = loop.time(o, 5, 2, dist or _Solo())
+        sweep.append({"ef": ef, "recall": None if r is None else round(r, 5),
+                      "qps": round(loop.nq / (ms / 1e3), 1)})
         if r is not None and r >= target and not ef_star:
             ef_star = ef
-            break
     return (ef_star or EFS[-1]), flags, sweep
 
 
@@ -425,11 +436,13 @@ def run_ours(args, dist: Dist):
 
     # ---- plain FP32 beam (the comparison), both tie orders
     plain = {}
+    rows = {}
     for order in ("id", "reference"):
-        ef_p, fl_p, sw = plain_sweep(idx, loop, q, gt, args.target_recall, order, args.ef)
+        ef_p, fl_p, sw = plain_sweep(idx, loop, q, gt, args.target_recall, order, args.ef, dist=dist)
         o = loop.opts(ef_p, fl_p)
         loop.step(o)
         lab_p = loop.labels()
+        rows[order] = lab_p
         ms_p, _ = loop.time(o, args.steps, args.warmup, dist)
         plain[order] = {"ef": ef_p, "recall@10": round(recall(lab_p, gt), 5), "ms_per_step": round(ms_p, 4),
                         "qps": round(dist.world * nq / (ms_p / 1e3), 1), "sweep": sw}
@@ -443,25 +456,43 @@ def run_ours(args, dist: Dist):
             plain[order]["replay_all"] = {"ms_per_step": round(ms_r, 4), "qps": round(dist.world * nq / (ms_r / 1e3), 1),
                                           "same_labels": same}
 
-    # ---- learned termination + FP8 traversal + FP32 re-rank (the headline)
+    # the parity contract: the reference tie order returns hnswlib's own
+    # results; the id order differs only where distances tie exactly
+    same_rows = float(np.mean(np.all(rows["id"] == rows["reference"], axis=1))) \
+        if plain["id"]["ef"] == plain["reference"]["ef"] else None
+    plain["id"]["rows_identical_to_reference_order"] = None if same_rows is None else round(same_rows, 5)
+
+    # ---- fp8 traversal at fixed ef (the learned stop's fallback), swept
+    ef_f, _, sw_f = plain_sweep(idx, loop, q, gt, args.target_recall, "id", 0, precision=_capi.PREC_FP8,
+                                dist=dist)
+
+    # ---- learned termination + FP8 traversal + FP32 re-rank (the headline).
+    # Trained and calibrated on training-stream queries; a second held-out
+    # stream (never the evaluation queries) checks the calibrated recall and,
+    # if it falls short, tightens the calibration target (no retraining).
     model, rep, tq, fit_s = train_termination(idx, args)
     flags = _capi.LEARNED_STOP
+    from hnsw_rabitq_b200.datasets import gmm_1m_128_queries
+    vq = gmm_1m_128_queries(5000, stream_seed=2000)
+    vgt = idx.knn_query_exact(vq, 10)[0]
+    hold = tq[: max(1, len(tq) // 3)]
+    hgt = idx.knn_query_exact(hold, 10)[0]
     tgt = args.target_recall
+    val_rec = None
     for _ in range(6):
-        o = loop.opts(model.ef_cap, flags, _capi.PREC_FP8, args.rerank)
-        loop.step(o)
-        lab = loop.labels()
-        rec = recall(lab, gt)
-        if rec >= args.target_recall:
+        vl, _, _, _ = idx.knn_query_traced(vq, 10, ef=model.ef_cap, tie_order="id", precision="fp8",
+                                           rerank=args.rerank, learned=np.isfinite(model.threshold))
+        val_rec = recall(vl, vgt)
+        if val_rec >= args.target_recall:
             break
-        # the held-out calibration fell short on the evaluation queries:
-        # tighten its target (no retraining) and recalibrate
         tgt += 0.005
-        hold = tq[: max(1, len(tq) // 3)]
-        hgt = idx.knn_query_exact(hold, 10)[0]
         cap, thr, _ = learned.calibrate(idx, hold, hgt, 10, model, tgt, caps=sorted({c for c, *_ in rep["curve"]}))
         model.ef_cap, model.threshold = cap, thr
         idx.set_termination_model(model)
+    o = loop.opts(model.ef_cap, flags, _capi.PREC_FP8, args.rerank)
+    loop.step(o)
+    lab = loop.labels()
+    rec = recall(lab, gt)
     ms_step, clk = loop.time(o, args.steps, args.warmup, dist, clocks=True)
     value = dist.world * nq * args.steps / (ms_step * args.steps / 1e3)
     _, _, _, trace = idx.knn_query_traced(q, 10, ef=model.ef_cap, tie_order="id", precision="fp8",
@@ -477,9 +508,9 @@ def run_ours(args, dist: Dist):
         # upper-layer link lists (4 + 4 maxM) and float32 rows; level-0 link
         # lists (4 + 4 maxM0) and fp8 rows (128 B + 16 B scale block); the
         # float32 re-rank of the pool (at most ef_cap rows of 512 B)
-        fp8_row = 128 + 16
+        fp8_row = 128 + 8  # e4m3 data, scale and squared norm of the dequantized row
         rr = args.rerank or model.ef_cap
-        bq = (trace[:, 0] * (4 + 4 * info.maxM) + trace[:, 1] * 512 + trace[:, 2] * (4 + 4 * info.maxM0)
+        bq = (trace[:, 0] * (4 + 4 * info.maxM) + trace[:, 1] * fp8_row + trace[:, 2] * (4 + 4 * info.maxM0)
               + trace[:, 3] * fp8_row).mean() + min(rr, model.ef_cap) * 512
         achieved = bq * nq / (ms_step / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
@@ -487,10 +518,11 @@ def run_ours(args, dist: Dist):
                 # with threshold +inf the calibrated search is the plain fp8 beam
                 "traffic": committed_traffic("learned_fp8" if np.isfinite(model.threshold) else "fp8",
                                              model.ef_cap),
+                "traffic_source": "committed ncu capture (profiles/), not measured in this run",
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "algorithmic_bytes_per_query": round(float(bq), 1),
-                "kernel": "hnsw_search_kernel<L2, fp8 traversal, " +
+                "kernel": "hnsw_lean_kernel<L2, fp8 traversal, " +
                           ("learned stop>" if np.isfinite(model.threshold) else "fixed ef (calibrated: no stop)>")}
         cpu, bytes_q = (cpu_baseline(args, path, q, plain["id"]["ef"], info) if not args.no_cpu_baseline
                         else (None, None))
@@ -506,10 +538,15 @@ def run_ours(args, dist: Dist):
             "vs_baseline": None, "dtype": "fp8 traversal, f32 accumulation and re-rank", "data": "synthetic",
             "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
                                    "HNSW M=16 efc=200, 10,000 queries, k=10",
-                       "method": "learned early termination (6-64-64-1 fp16 MLP every "
-                                 f"{model.period} expansions) over an fp8 e4m3 per-row-scaled beam, fp32 re-rank",
+                       "method": ("learned early termination (6-64-64-1 fp16 MLP every "
+                                  f"{model.period} expansions) over an fp8 e4m3 per-row-scaled beam, fp32 re-rank")
+                       if np.isfinite(model.threshold) else
+                       ("fixed ef: the calibrated logit threshold is +inf (the network never stops a query "
+                        "earlier than the cap), fp8 e4m3 per-row-scaled beam, fp32 re-rank"),
                        "ef_cap": model.ef_cap, "logit_threshold": model.threshold,
-                       "recall@10": round(rec, 5), "mean_l0_expansions": round(float(trace[:, 2].mean()), 2),
+                       "recall@10": round(rec, 5), "validation_recall@10": round(val_rec, 5),
+                       "calibration_target": round(tgt, 4),
+                       "mean_l0_expansions": round(float(trace[:, 2].mean()), 2),
                        "global_batch": nq, "parallelism": f"replicas x{dist.world}",
                        "l2_flush": "not needed: index data 640 MB + fp8 copy 144 MB > 126 MB L2",
                        "index_device_bytes": int(idx._info().device_bytes),
@@ -518,6 +555,9 @@ def run_ours(args, dist: Dist):
                                     "loss_first_last": [round(rep["loss"][0], 4), round(rep["loss"][-1], 4)],
                                     "trained_cap": rep["trained_cap"], "fit_seconds": round(fit_s, 1)}},
             "plain_fp32": plain,
+            "parity_contract_arm": "plain_fp32.reference (results identical to hnswlib's searchKnn, "
+                                   "including exact ties)",
+            "fp8_fixed_ef": {"ef": ef_f, "sweep": sw_f},
             "speedup_vs_plain_fp32": {o2: round(value / plain[o2]["qps"], 3) for o2 in plain},
             "roofline": roof,
             "cpu_baseline": cpu,

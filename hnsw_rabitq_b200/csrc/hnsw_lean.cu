@@ -246,7 +246,7 @@ struct LeanTerm {
 };
 
 // Checkpoint of the learned termination (trace mode 1 records it, mode 2
-// asks the network whether to stop), as the general beam takes it.
+// asks the network whether to stop), with the general beam's features.
 template <int TERM>
 __device__ __forceinline__ bool lean_checkpoint(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
                                                 uint32_t e, int psize, uint32_t next_dk, float d_entry, float qn,
@@ -500,7 +500,12 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         }
         __syncwarp();
         if (sel == 0) break;
-        if (TERM && ct.l0_exp >= ts.next) {
+        // a checkpoint falls due every term_period expansions; it is taken
+        // (trace mode records it, learned mode consults the network) at the
+        // first iteration from then on where no unexpanded candidate is
+        // closer than the current k-th result, the only states in which
+        // stopping can keep the top-k
+        if (TERM && ct.l0_exp >= ts.next && psize >= kq && next_dk > khi(s.pool[kq - 1])) {
             const bool stop = lean_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d_entry, lq.qn, ts);
             while (ts.next <= ct.l0_exp) ts.next += p.term_period;
             if (stop) break;

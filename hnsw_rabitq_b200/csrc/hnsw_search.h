@@ -36,14 +36,21 @@ constexpr int kTermOffB2 = kTermOffW2 + kTermHidden * kTermHidden;
 constexpr int kTermOffW3 = kTermOffB2 + kTermHidden;
 constexpr int kTermOffB3 = kTermOffW3 + kTermHidden;
 constexpr int kTermParams = kTermOffB3 + 1;
-// Inference form (device), laid out for coalesced warp reads: float mu[6],
-// inv_sigma[6], b1[64], b2[64], b3, pad[3] (kTermPackedFloats floats); then
-// half W1[64][8] (rows padded to 16 bytes), W2 as half2 [32][64] holding
-// (W2[u][2p], W2[u][2p+1]) at [p][u], and w3[64].
-constexpr int kTermPackedFloats = 2 * kTermFeatures + 2 * kTermHidden + 4;
-constexpr int kTermW1Stride = 8;
-constexpr int kTermPackedHalves = kTermHidden * kTermW1Stride + kTermHidden * kTermHidden + kTermHidden;
-constexpr size_t kTermPackedBytes = (size_t)kTermPackedFloats * 4 + (size_t)kTermPackedHalves * 2;
+// Inference form (device): both layers run on the tensor cores (mma.sync
+// m16n8k16, fp16 operands, fp32 accumulation), weights pre-arranged in the B
+// fragments each lane reads.  With g = lane / 4 and t = lane % 4, tile v of a
+// layer covers units 8v .. 8v + 7 and lane (g, t) accumulates units 8v + 2t
+// and 8v + 2t + 1 of every tile.  In order:
+//   float mu[6], inv_sigma[6], b3, pad[3]                      (16 floats)
+//   float2 b1f[4][8], b2f[4][8]: (b[8v + 2t], b[8v + 2t + 1]) at [t][v]
+//   half2 w3f[4][8]:             (w3[8v + 2t], w3[8v + 2t + 1]) at [t][v]
+//   half2 W1f[32][8]:            (W1[8v + g][2t], W1[8v + g][2t + 1]) at
+//                                [lane][v] (features 6, 7 are zero)
+//   half2 W2f[32][4][8][2]:      (W2[8v + g][16s + 2t + 8h],
+//                                 W2[8v + g][16s + 2t + 8h + 1]) at [lane][s][v][h]
+constexpr int kTermPackedFloats = 16 + 2 * 4 * 8 * 2;
+constexpr int kTermPackedHalf2 = 4 * 8 + 32 * 8 + 32 * 4 * 8 * 2;
+constexpr size_t kTermPackedBytes = (size_t)kTermPackedFloats * 4 + (size_t)kTermPackedHalf2 * 4;
 // Convert the float32 parameter vector (kTermParams) into the inference form.
 void pack_term_model(const float* params, unsigned char* out);
 // Training side (term_train.cu), host pointers, current device:

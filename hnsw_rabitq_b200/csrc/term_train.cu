@@ -34,28 +34,49 @@ namespace hnswgpu {
 
 void pack_term_model(const float* params, unsigned char* out) {
     float* f = reinterpret_cast<float*>(out);
+    for (int i = 0; i < kTermPackedFloats; i++) f[i] = 0.f;
     for (int i = 0; i < kTermFeatures; i++) {
         f[i] = params[kTermOffMu + i];
         f[kTermFeatures + i] = params[kTermOffInvSigma + i];
     }
-    for (int u = 0; u < kTermHidden; u++) {
-        f[2 * kTermFeatures + u] = params[kTermOffB1 + u];
-        f[2 * kTermFeatures + kTermHidden + u] = params[kTermOffB2 + u];
-    }
-    f[2 * kTermFeatures + 2 * kTermHidden] = params[kTermOffB3];
-    for (int i = 2 * kTermFeatures + 2 * kTermHidden + 1; i < kTermPackedFloats; i++) f[i] = 0.f;
+    f[2 * kTermFeatures] = params[kTermOffB3];
+    float* b1f = f + 16;
+    float* b2f = b1f + 4 * 8 * 2;
+    for (int t = 0; t < 4; t++)
+        for (int v = 0; v < 8; v++)
+            for (int e = 0; e < 2; e++) {
+                b1f[(t * 8 + v) * 2 + e] = params[kTermOffB1 + 8 * v + 2 * t + e];
+                b2f[(t * 8 + v) * 2 + e] = params[kTermOffB2 + 8 * v + 2 * t + e];
+            }
     __half* h = reinterpret_cast<__half*>(out + (size_t)kTermPackedFloats * 4);
-    for (int u = 0; u < kTermHidden; u++)
-        for (int i = 0; i < kTermW1Stride; i++)
-            h[u * kTermW1Stride + i] = __float2half_rn(i < kTermFeatures ? params[kTermOffW1 + u * kTermFeatures + i] : 0.f);
-    h += kTermHidden * kTermW1Stride;
-    for (int pr = 0; pr < kTermHidden / 2; pr++)
-        for (int u = 0; u < kTermHidden; u++) {
-            h[(pr * kTermHidden + u) * 2] = __float2half_rn(params[kTermOffW2 + u * kTermHidden + 2 * pr]);
-            h[(pr * kTermHidden + u) * 2 + 1] = __float2half_rn(params[kTermOffW2 + u * kTermHidden + 2 * pr + 1]);
-        }
-    h += kTermHidden * kTermHidden;
-    for (int i = 0; i < kTermHidden; i++) h[i] = __float2half_rn(params[kTermOffW3 + i]);
+    // w3f[t][v]
+    for (int t = 0; t < 4; t++)
+        for (int v = 0; v < 8; v++)
+            for (int e = 0; e < 2; e++) h[(t * 8 + v) * 2 + e] = __float2half_rn(params[kTermOffW3 + 8 * v + 2 * t + e]);
+    h += 4 * 8 * 2;
+    // W1f[lane][v]
+    for (int lane = 0; lane < 32; lane++) {
+        const int g = lane >> 2, t = lane & 3;
+        for (int v = 0; v < 8; v++)
+            for (int e = 0; e < 2; e++) {
+                const int feat = 2 * t + e;
+                h[(lane * 8 + v) * 2 + e] =
+                    __float2half_rn(feat < kTermFeatures ? params[kTermOffW1 + (8 * v + g) * kTermFeatures + feat] : 0.f);
+            }
+    }
+    h += 32 * 8 * 2;
+    // W2f[lane][s][v][hh]
+    for (int lane = 0; lane < 32; lane++) {
+        const int g = lane >> 2, t = lane & 3;
+        for (int st = 0; st < 4; st++)
+            for (int v = 0; v < 8; v++)
+                for (int hh = 0; hh < 2; hh++)
+                    for (int e = 0; e < 2; e++) {
+                        const int j = 16 * st + 2 * t + 8 * hh + e;
+                        h[(((lane * 4 + st) * 8 + v) * 2 + hh) * 2 + e] =
+                            __float2half_rn(params[kTermOffW2 + (8 * v + g) * kTermHidden + j]);
+                    }
+    }
 }
 
 namespace {

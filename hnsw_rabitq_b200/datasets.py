@@ -104,12 +104,14 @@ def gmm_unit_ip(n: int = 1_000_000, nq: int = 10_000, dim: int = 768, n_comp: in
 
 
 def gmm_lognormal_sigma(n: int = 10_000_000, nq: int = 10_000, dim: int = 96, n_comp: int = 4096,
-                        seed: int = 0, chunk: int = 1 << 18, query_seed=None):
-    """N(0,1) centres with per-component sigma log-uniform in [0.05, 0.5]
-    (queries: ``default_rng(seed + 1)`` or ``default_rng(query_seed)``)."""
+                        seed: int = 0, chunk: int = 1 << 18, query_seed=None, sigma_range=(0.05, 0.5)):
+    """N(0,1) centres with per-component sigma log-uniform in `sigma_range`
+    (default [0.05, 0.5]; queries: ``default_rng(seed + 1)`` or
+    ``default_rng(query_seed)``)."""
     crng = np.random.default_rng(seed + 7)
     centres = crng.standard_normal((n_comp, dim), dtype=np.float32)
-    sig = np.exp(crng.uniform(np.log(0.05), np.log(0.5), n_comp)).astype(np.float32)
+    lo, hi = sigma_range
+    sig = np.exp(crng.uniform(np.log(lo), np.log(hi), n_comp)).astype(np.float32)
 
     def draw(rng, m):
         out = np.empty((m, dim), np.float32)

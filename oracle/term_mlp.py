@@ -39,15 +39,27 @@ def _softplus(x):
     return np.maximum(x, 0.0) + np.log1p(np.exp(-np.abs(x)))
 
 
-def forward(params, feats, fp16_weights: bool = False):
+def _f16(a):
+    return np.asarray(a, np.float64).astype(np.float16).astype(np.float64)
+
+
+def forward(params, feats, fp16_weights: bool = False, fp16_activations: bool = False):
     """Logits (float64) of feature rows [n, 6].  fp16_weights: round W1, W2,
-    w3 to fp16 first, as the search's inference form does."""
+    w3 to fp16 first; fp16_activations: also round the standardised features
+    (in float32 arithmetic) and the first hidden layer to fp16 -- the
+    operands of the search's tensor-core inference form."""
     q = unpack(params)
     W1, W2, w3 = q["W1"], q["W2"], q["w3"]
     if fp16_weights:
-        W1, W2, w3 = (a.astype(np.float16).astype(np.float64) for a in (W1, W2, w3))
-    x = (np.asarray(feats, np.float64) - q["mu"]) * q["inv_sigma"]
+        W1, W2, w3 = (_f16(a) for a in (W1, W2, w3))
+    if fp16_activations:
+        f32 = np.asarray(feats, np.float32)
+        x = _f16((f32 - q["mu"].astype(np.float32)) * q["inv_sigma"].astype(np.float32))
+    else:
+        x = (np.asarray(feats, np.float64) - q["mu"]) * q["inv_sigma"]
     h1 = np.maximum(x @ W1.T + q["b1"], 0.0)
+    if fp16_activations:
+        h1 = _f16(h1)
     h2 = np.maximum(h1 @ W2.T + q["b2"], 0.0)
     return h2 @ w3 + q["b3"]
 

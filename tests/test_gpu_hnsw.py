@@ -287,7 +287,10 @@ def test_full_size_parity_1m():
         cl, cd, _ = o.search(qs, 10, ef, mode=O.CANONICAL)
         assert np.array_equal(gl, cl) and np.array_equal(gd.view(np.uint32), cd.view(np.uint32))
         same, bad = compare_rows(gl, rl, rt[:, 4])
-        assert same >= 0.995 and not bad, (ef, same, bad[:5])
+        # every differing row has a tie decision; at the operating points
+        # around recall 0.95 (ef >= 48) at least 99.9 % of the rows are the
+        # reference's (ties are denser among the few candidates of ef 16-24)
+        assert same >= (0.999 if ef >= 48 else 0.995) and not bad, (ef, same, bad[:5])
 
 
 def test_config1_uniform_10k():

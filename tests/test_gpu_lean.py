@@ -78,8 +78,8 @@ def test_lean_gmm_8bit_matches_fp32_recall(tmp_path):
 
 def test_lean_learned_stop_bounds(tmp_path):
     """Threshold +inf (and 1e30, which evaluates the network) gives the plain
-    lean beam; -inf stops at the first checkpoint; recording checkpoints does
-    not change the search."""
+    lean beam; -inf stops at the first checkpoint taken; recording
+    checkpoints does not change the search."""
     rng = np.random.default_rng(3)
     x = rng.standard_normal((10000, 64)).astype(np.float32)
     q = rng.standard_normal((300, 64)).astype(np.float32)
@@ -95,9 +95,13 @@ def test_lean_learned_stop_bounds(tmp_path):
         g.set_termination_model(learned.TerminationModel(p, period, never, ef, "fp8"))
         ll, ld, _, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", precision="fp8", learned=True)
         assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
+    # -inf stops at the first checkpoint taken: the first one due (every
+    # `period` expansions) at which no unexpanded candidate is closer than
+    # the current k-th result
     g.set_termination_model(learned.TerminationModel(p, period, -float("inf"), ef, "fp8"))
     ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", precision="fp8", learned=True)
-    assert np.all(lt[:, 2] <= period) and np.all(lc == k)
+    assert np.all(lt[:, 2] <= pt[:, 2]) and lt[:, 2].mean() < 0.8 * pt[:, 2].mean() and np.all(lc == k)
+    assert np.all(lt[:, 2] >= period)
     assert np.all(np.diff(ld, axis=1) >= 0)
     ck = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=64, precision="fp8")
     assert np.array_equal(ck["labels"], pl)

@@ -41,13 +41,15 @@ def test_gradient_matches_oracle(n, pw):
 
 
 def test_inference_matches_oracle_with_fp16_weights():
-    """The search's in-warp inference (fp16 weights, fp32 accumulation)
-    against the oracle with the same fp16-rounded weights: within 1e-4
-    relative to the logit scale."""
+    """The search's in-warp tensor-core inference (fp16 weights and
+    activations, fp32 accumulation) against the oracle with the same fp16
+    rounding: within 1e-3 relative to the logit scale (a hidden unit whose
+    float32 value sits on an fp16 rounding boundary may round the other
+    way)."""
     p, f, _ = _random_problem(3000, seed=5)
     z = learned.logits(p, f)
-    ref = T.forward(p, f, fp16_weights=True)
-    assert np.abs(z - ref).max() <= 1e-4 * max(1.0, np.abs(ref).max())
+    ref = T.forward(p, f, fp16_weights=True, fp16_activations=True)
+    assert np.abs(z - ref).max() <= 1e-3 * max(1.0, np.abs(ref).max())
     # and close to the float32 network
     assert np.abs(z - T.forward(p, f)).max() <= 2e-2 * max(1.0, np.abs(ref).max())
 
@@ -130,27 +132,46 @@ def test_stop_rule_bounds(gmm_index):
         g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
 
 
-def test_fit_meets_target_with_less_work(gmm_index):
-    """Trained and calibrated on 1000 queries, evaluated on 500 others: the
-    learned search reaches the target recall@10 (less a small
-    generalisation margin) with fewer level-0 expansions than the cap."""
-    g, x, q = gmm_index
-    tr, te = q[:1000], q[1000:]
-    model, rep = learned.fit(g, tr, k=10, ef_cap=96, period=4, target_recall=0.95, epochs=15, seed=0, caps=[96],
-                             cost="expansions")
+@pytest.fixture(scope="module")
+def hetero_index(tmp_path_factory):
+    """Queries of very different difficulty: 32 Gaussian components with
+    per-component sigma log-uniform in [0.05, 1.0] (40,000 x 64 rows,
+    reference-built graph, M = 12)."""
+    from hnsw_rabitq_b200.datasets import gmm_lognormal_sigma
+    x, q = gmm_lognormal_sigma(n=40000, nq=3000, dim=64, n_comp=32, sigma_range=(0.05, 1.0))
+    path = tmp_path_factory.mktemp("hetero") / "g.bin"
+    build_hnsw(path, x, "l2", M=12, efc=100, num_threads=8)
+    g = H.Index("l2", 64)
+    g.load_index(str(path))
+    return g, x, q
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp8"])
+def test_learned_beats_fixed_ef_at_equal_recall(hetero_index, precision):
+    """Trained and calibrated on 2,000 queries, evaluated on 1,000 others:
+    the learned stop needs at least 10 % fewer level-0 expansions than the
+    smallest fixed ef whose recall@10 on the same evaluation queries is at
+    least the learned search's (the method without the network, at equal
+    recall), and its recall stays near the calibration target."""
+    g, x, q = hetero_index
+    tr, te = q[:2000], q[2000:]
+    cap = 96
+    model, rep = learned.fit(g, tr, k=10, ef_cap=cap, period=4, target_recall=0.97, precision=precision, epochs=20,
+                             seed=0, caps=[cap], cost="expansions")
     assert rep["samples"] > 10000 and 0.05 < rep["positive"] < 0.95
-    assert rep["loss"][-1] < rep["loss"][0]
-    assert model.ef_cap == 96 and np.isfinite(model.threshold)
+    assert np.isfinite(model.threshold), rep["curve"]
     gt = g.knn_query_exact(te, 10)[0]
-    g.learned_stop = True
-    g.tie_order = "id"
-    g.set_ef(model.ef_cap)
-    lab, _ = g.knn_query(te, 10)
-    r = learned.recall(lab, gt)
-    _, _, _, tl = g.knn_query_traced(te, 10, ef=model.ef_cap, learned=True)
-    _, _, _, tp = g.knn_query_traced(te, 10, ef=model.ef_cap, learned=False)
-    assert r >= 0.94, (r, rep["curve"])
-    assert tl[:, 2].mean() < 0.9 * tp[:, 2].mean(), (tl[:, 2].mean(), tp[:, 2].mean())
+    ll, _, _, lt = g.knn_query_traced(te, 10, ef=cap, tie_order="id", precision=precision, learned=True)
+    r_l, e_l = learned.recall(ll, gt), float(lt[:, 2].mean())
+    assert r_l >= 0.95, (r_l, rep["curve"])
+    sweep = []
+    for ef in range(12, cap + 1, 4):
+        fl, _, _, ft = g.knn_query_traced(te, 10, ef=ef, tie_order="id", precision=precision)
+        sweep.append((ef, learned.recall(fl, gt), float(ft[:, 2].mean())))
+    ok = [s for s in sweep if s[1] >= r_l]
+    assert ok, (r_l, sweep)
+    ef_f, r_f, e_f = ok[0]
+    assert e_l <= 0.9 * e_f, (precision, r_l, e_l, ef_f, r_f, e_f)
 
 
 def test_fit_fp8_labels_use_the_beam_state(gmm_index):
