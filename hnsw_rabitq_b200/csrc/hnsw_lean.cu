@@ -213,9 +213,7 @@ __device__ __forceinline__ int lean_merge(uint64_t* pool, int& size, int cap, un
         const uint64_t k2 = shfl64(key, __ffs(m) - 1);
         rank += k2 < key;
     }
-    int mpos = mine ? pos : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) mpos = min(mpos, __shfl_xor_sync(FULL, mpos, o));
+    const int mpos = (int)__reduce_min_sync(FULL, mine ? (unsigned)pos : 0x7fffffffu);
     if (size > mpos) {
         // move the entries [mpos, size) right, last chunk first
         const int nmove = size - mpos;

@@ -51,6 +51,7 @@ namespace {
 
 struct WarpSmem {
     uint64_t* bar;
+    uint32_t* cbuf;      // 32 ids: compaction of one expansion's fresh neighbours
     float* q;
     float* stage;
     uint64_t* pool;
@@ -221,9 +222,7 @@ __device__ __forceinline__ int merge_sorted(uint64_t* a, int& size, int cap, uns
         uint64_t k2 = shfl64(kc, src);
         rank += (k2 < kc);
     }
-    int mpos = mine ? pos : 0x7fffffff;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) mpos = min(mpos, __shfl_xor_sync(FULL, mpos, o));
+    const int mpos = (int)__reduce_min_sync(FULL, mine ? (unsigned)pos : 0x7fffffffu);
     if (size > mpos) {
         // Move the entries [mpos, size) right, last chunk first.
         int nmove = size - mpos;
@@ -407,8 +406,11 @@ __device__ __forceinline__ void fetch_links(const SearchParams& p, WarpSmem& s, 
     f.allowed = !FILTER || !fresh || is_allowed(p, id);
     f.nmask = __ballot_sync(FULL, fresh);
     f.nnew = __popc(f.nmask);
-    const int src = (int)__fns(f.nmask, 0, lane + 1);
-    f.cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
+    // compact the fresh ids (link order kept) through shared memory: lane i
+    // then holds the i-th fresh id (lanes >= nnew hold stale values)
+    if (fresh) s.cbuf[__popc(f.nmask & lanemask_lt())] = id;
+    __syncwarp();
+    f.cid2 = s.cbuf[lane];
     f.n0 = min((int)rs.slots, f.nnew);
     if (f.n0 > 0) {
         fence_proxy_async_smem();
@@ -701,12 +703,11 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < kq)) ts.last_change = ct.l0_exp;
         PT_MARK(6);
         // ---- the next candidate
-        uint64_t kmin = accept ? key : ~0ull;  // smallest accepted key
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            uint64_t other = shfl64(kmin, lane ^ o);
-            kmin = other < kmin ? other : kmin;
-        }
+        // smallest accepted key: the smallest distance key, then the smallest
+        // id among the lanes holding it (two warp reductions)
+        const uint32_t kmin_hi = __reduce_min_sync(FULL, accept ? dk : 0xffffffffu);
+        const uint32_t kmin_lo = __reduce_min_sync(FULL, accept && dk == kmin_hi ? f.id : 0xffffffffu);
+        const uint64_t kmin = ((uint64_t)kmin_hi << 32) | kmin_lo;
         bool have_next = false, spec = false, next_extra = false;
         uint32_t next = INVALID_ID, next_dk = 0xffffffffu;
         if (!EXACT) {
@@ -1173,8 +1174,10 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             ct.l0_dists += nnew;
             // compact the fresh ids to lanes [0, nnew), evaluate, route back
             int ci = __popc(nmask & lanemask_lt());
-            int src = __fns(nmask, 0, lane + 1);  // lane holding the (lane)-th fresh id
-            uint32_t cid2 = __shfl_sync(FULL, id, src < 0 ? 0 : src);
+            if (fresh) s.cbuf[ci] = id;  // lane i then holds the i-th fresh id
+            __syncwarp();
+            uint32_t cid2 = s.cbuf[lane];
+            __syncwarp();
             float dc;
             if (!lane_distances<SPACE, FAST16>(p, s, phase, cid2, nnew, lane, dc, pc)) return false;
             float d = __shfl_sync(FULL, dc, ci & 31);
@@ -1361,6 +1364,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP 
     unsigned char* base = smem + (size_t)warp * p.warp_smem;
     WarpSmem s;
     s.bar = reinterpret_cast<uint64_t*>(base);
+    s.cbuf = reinterpret_cast<uint32_t*>(base + 16);
     s.q = reinterpret_cast<float*>(base + p.off_query);
     s.stage = reinterpret_cast<float*>(base + p.off_stage);
     s.pool = reinterpret_cast<uint64_t*>(base + p.off_pool);
@@ -1428,7 +1432,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, PREC ? HNSWGPU_MINB_LOWP 
 
 size_t warp_smem_layout(SearchParams& p) {
     if (p.lean) return lean_smem_layout(p);
-    size_t off = 16;  // mbarrier (8 bytes) + pad
+    size_t off = 16 + 128;  // mbarrier (8 bytes) + pad, then the 32-entry id compaction buffer
     p.off_query = (uint32_t)off;
     off += (size_t)p.row_floats * 4;
     off = (off + 15) & ~(size_t)15;
