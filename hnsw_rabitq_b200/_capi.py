@@ -41,7 +41,7 @@ class Info(C.Structure):
 
 class SearchOpts(C.Structure):
     _fields_ = [("flags", U32), ("precision", U32), ("ef", U64), ("allow", P), ("trace", P), ("stream", P),
-                ("rerank", U32), ("reserved1", U32)]
+                ("rerank", U32), ("filter", U32)]
 
 
 class TermTrainOpts(C.Structure):
@@ -79,6 +79,9 @@ SIGNATURES = {
     "hnswgpu_get_status": (C.c_int, [P, C.POINTER(U32)]),
     "hnswgpu_search_noalloc": (C.c_int, [P, P, U64, U64, U64, U32, P, P, P, P, P]),
     "hnswgpu_noalloc_get_status": (C.c_int, [C.c_int, P, C.POINTER(U32)]),
+    "hnswgpu_filter_create": (C.c_int, [P, P, C.POINTER(U32)]),
+    "hnswgpu_filter_destroy": (C.c_int, [P, U32]),
+    "hnswgpu_save_hnsw": (C.c_int, [P, C.c_char_p]),
     "hnswgpu_selftest_wait_timeout": (C.c_int, [C.c_int, C.POINTER(U32)]),
     "hnswgpu_search_epsilon": (C.c_int, [P, P, U64, C.c_float, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_set_termination_model": (C.c_int, [P, P, U32, C.c_float]),

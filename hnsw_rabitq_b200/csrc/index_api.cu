@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iterator>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -871,6 +872,7 @@ int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_el
         std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
         init_common(h.get(), device);
         load_hnsw_file(h.get(), path, space, dim, max_elements);
+        h->source_path = path;
         *out = h.release();
         return HNSWGPU_OK;
     });
@@ -1006,6 +1008,13 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
         std::lock_guard<std::mutex> g(h->mu);
         set_device(h);
+        const uint8_t* dfilter = nullptr;  // a registered filter's device mask
+        if (o.filter) {
+            if (o.allow) return fail(HNSWGPU_ERR_ARG, "give either an allow mask or a registered filter, not both");
+            if (o.filter > h->filters.size() || !h->filters[o.filter - 1])
+                return fail(HNSWGPU_ERR_ARG, "unknown filter id");
+            dfilter = h->filters[o.filter - 1]->p;
+        }
         if (nq == 0) return HNSWGPU_OK;
         if (h->count == 0) {
             // empty index: searchKnn returns nothing (hnswalg.h:1272)
@@ -1023,7 +1032,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
             return HNSWGPU_OK;
         }
         if (dev) {
-            run_search(h, queries, nq, k, ef, o.allow, out_labels, out_dists, out_counts,
+            run_search(h, queries, nq, k, ef, dfilter ? dfilter : o.allow, out_labels, out_dists, out_counts,
                        want_trace ? o.trace : nullptr, st, exact, o.precision, o.rerank, &term, scan, replay_all);
             return HNSWGPU_OK;
         }
@@ -1038,7 +1047,7 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
         float* dd = (float*)(base + al(qb) + al(lb));
         int32_t* dc = (int32_t*)(base + al(qb) + al(lb) + al(db));
         uint32_t* dt = want_trace ? (uint32_t*)(base + al(qb) + al(lb) + al(db) + al(cb)) : nullptr;
-        const uint8_t* dallow = nullptr;
+        const uint8_t* dallow = dfilter;
         if (o.allow) {
             h->allow.ensure(h->count);
             cuda_check(cudaMemcpyAsync(h->allow.p, o.allow, h->count, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
@@ -1063,6 +1072,69 @@ int hnswgpu_search(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t
     });
 }
 
+int hnswgpu_filter_create(hnswgpu_index* h, const uint8_t* allow, uint32_t* out_id) {
+    return guarded([&] {
+        if (!h || !out_id || (h->count && !allow)) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        std::unique_ptr<DevBuf<uint8_t>> buf(new DevBuf<uint8_t>());
+        buf->alloc(std::max<uint64_t>(h->count, 1));
+        if (h->count) {
+            cuda_check(cudaMemcpyAsync(buf->p, allow, h->count, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+            cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        }
+        size_t slot = 0;
+        while (slot < h->filters.size() && h->filters[slot]) slot++;
+        if (slot == h->filters.size()) h->filters.emplace_back();
+        h->filters[slot] = std::move(buf);
+        *out_id = (uint32_t)slot + 1;
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_filter_destroy(hnswgpu_index* h, uint32_t id) {
+    return guarded([&] {
+        if (!h) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        std::lock_guard<std::mutex> g(h->mu);
+        if (id == 0 || id > h->filters.size() || !h->filters[id - 1]) return fail(HNSWGPU_ERR_ARG, "unknown filter id");
+        set_device(h);
+        // searches queued on the index's stream may still read it
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        h->filters[id - 1].reset();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_save_hnsw(hnswgpu_index* h, const char* path) {
+    return guarded([&] {
+        if (!h || !path || h->is_bf) return fail(HNSWGPU_ERR_ARG, "hnswgpu_save_hnsw needs an HNSW index");
+        std::lock_guard<std::mutex> g(h->mu);
+        if (h->source_path.empty()) return fail(HNSWGPU_ERR_STATE, "the index was not loaded from a file");
+        std::ifstream in(h->source_path, std::ios::binary);
+        if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+        std::vector<char> bytes((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+        // header (hnswalg.h:685-712), then the level-0 block: rewrite the
+        // delete mark of every element (bit 0 of byte 2 of its record,
+        // hnswalg.h:872-885) from the current marks
+        const size_t header = 8 * 6 + 4 + 4 + 8 * 3 + 8 + 8;
+        uint64_t size_data = 0;
+        if (bytes.size() < header) throw ApiError(HNSWGPU_ERR_FORMAT, "Index seems to be corrupted or unsupported");
+        memcpy(&size_data, bytes.data() + 24, 8);
+        if (bytes.size() < header + h->count * size_data)
+            throw ApiError(HNSWGPU_ERR_FORMAT, "Index seems to be corrupted or unsupported");
+        for (uint64_t i = 0; i < h->count; i++) {
+            char& flags = bytes[header + i * size_data + 2];
+            const bool del = (h->deleted[i >> 5] >> (i & 31)) & 1u;
+            flags = del ? (char)(flags | 1) : (char)(flags & ~1);
+        }
+        std::ofstream out(path, std::ios::binary);
+        if (!out.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+        out.write(bytes.data(), (std::streamsize)bytes.size());
+        if (!out) throw ApiError(HNSWGPU_ERR_IO, "write failed");
+        return HNSWGPU_OK;
+    });
+}
+
 int hnswgpu_search_epsilon(hnswgpu_index* h, const float* queries, uint64_t nq, float epsilon,
                            uint64_t min_candidates, uint64_t max_candidates, const hnswgpu_search_opts* opts,
                            uint64_t* out_ids, float* out_dists, int32_t* out_counts) {
@@ -1075,10 +1147,10 @@ int hnswgpu_search_epsilon(hnswgpu_index* h, const float* queries, uint64_t nq, 
         if (nq > 0xffffffffull || max_candidates > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "batch too large");
         hnswgpu_search_opts o{};
         if (opts) o = *opts;
-        if ((o.flags & ~(uint32_t)HNSWGPU_DEVICE_PTRS) || o.precision)
+        if ((o.flags & ~(uint32_t)HNSWGPU_DEVICE_PTRS) || o.precision || o.filter)
             return fail(HNSWGPU_ERR_UNSUPPORTED,
-                        "epsilon search: only HNSWGPU_DEVICE_PTRS may be set, float32 only (it always replays the "
-                        "reference's heaps)");
+                        "epsilon search: only HNSWGPU_DEVICE_PTRS may be set, float32 only, an allow mask rather "
+                        "than a registered filter (it always replays the reference's heaps)");
         const bool dev = (o.flags & HNSWGPU_DEVICE_PTRS) != 0;
         const uint64_t m = max_candidates;
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;

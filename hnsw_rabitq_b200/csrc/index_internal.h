@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <stdexcept>
 #include <string>
@@ -108,6 +109,9 @@ struct hnswgpu_index {
     DevBuf<uint8_t> scan_mask;         // exact scan over an index with deletions
     uint32_t term_period = 0;
     float term_logit = 0.f;
+    // registered filters (hnswgpu_filter_create): id - 1 -> device mask
+    std::vector<std::unique_ptr<DevBuf<uint8_t>>> filters;
+    std::string source_path;  // HNSW index file this index was loaded from (saveIndex)
     // guards the index state; mutable so that the const allocation-free
     // search can hold it while it reads that state
     mutable std::mutex mu;

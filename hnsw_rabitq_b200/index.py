@@ -45,6 +45,19 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+class RegisteredFilter:
+    """A filter evaluated once and kept on the GPU (Index.register_filter);
+    ``release()`` frees it."""
+
+    def __init__(self, index, fid: int):
+        self.index, self.id = index, fid
+
+    def release(self) -> None:
+        if self.id and self.index._h:
+            _capi.check(_capi.lib().hnswgpu_filter_destroy(self.index._h, self.id))
+        self.id = 0
+
+
 class _GpuIndex:
     _extra_spaces: dict = {}
 
@@ -57,7 +70,6 @@ class _GpuIndex:
         self.device = 0
         self._h = None
         self._labels = None
-        self._filter_cache = None
 
     # -- lifecycle
     def _free(self):
@@ -65,7 +77,6 @@ class _GpuIndex:
             _capi.lib().hnswgpu_free(self._h)
             self._h = None
         self._labels = None
-        self._filter_cache = None
 
     def __del__(self):
         try:
@@ -96,17 +107,33 @@ class _GpuIndex:
         return self._labels
 
     def _allow_mask(self, filter: Optional[Callable[[int], bool]]) -> Optional[np.ndarray]:
-        """Evaluate the filter functor once per label (it is called per
-        candidate in the reference, bindings.cpp:83-94); cached per callable."""
-        if filter is None:
+        """Evaluate the filter functor for every label, at every call (the
+        reference calls it per candidate during the search,
+        bindings.cpp:83-94, so a callable whose answers change is honoured);
+        a filter registered with ``register_filter`` is not re-evaluated."""
+        if filter is None or isinstance(filter, RegisteredFilter):
             return None
-        c = self._filter_cache
-        if c is not None and c[0] is filter:
-            return c[1]
+        labels = self.labels_by_internal_id()
+        return np.fromiter((1 if filter(int(l)) else 0 for l in labels), dtype=np.uint8, count=labels.shape[0])
+
+    def register_filter(self, filter: Callable[[int], bool]) -> "RegisteredFilter":
+        """Evaluate `filter` once over the index's labels and keep the answers
+        on the GPU: pass the returned object as ``filter=`` to search without
+        re-evaluating the callable or copying a mask (an extension; the
+        reference has no such form)."""
+        self._require()
         labels = self.labels_by_internal_id()
         mask = np.fromiter((1 if filter(int(l)) else 0 for l in labels), dtype=np.uint8, count=labels.shape[0])
-        self._filter_cache = (filter, mask)
-        return mask
+        fid = _capi.U32(0)
+        _capi.check(_capi.lib().hnswgpu_filter_create(self._h, _ptr(mask), C.byref(fid)))
+        return RegisteredFilter(self, fid.value)
+
+    def _filter_id(self, filter) -> int:
+        if not isinstance(filter, RegisteredFilter):
+            return 0
+        if filter.index is not self or not filter.id:
+            raise RuntimeError("the registered filter belongs to another index or was released")
+        return filter.id
 
     def _queries(self, data, k: int):
         self._require()
@@ -136,6 +163,7 @@ class _GpuIndex:
                 opts.flags |= _capi.REPLAY_ALL
         mask = self._allow_mask(filter)
         opts.allow = mask.ctypes.data if mask is not None else None
+        opts.filter = self._filter_id(filter)
         tr = None
         if trace:
             tr = np.zeros((nq, 4), np.uint32)
@@ -592,7 +620,6 @@ class BFIndex(_GpuIndex):
                 _capi.lib().hnswgpu_free(self._h)
                 self._h = None
             self._labels = None
-            self._filter_cache = None
             h = C.c_void_p()
             r = np.ascontiguousarray(self._rows, np.float32)
             lab = np.ascontiguousarray(self._row_labels, np.uint64)

@@ -140,7 +140,9 @@ typedef struct hnswgpu_search_opts {
     uint32_t rerank;           /* low precision: candidates re-ranked; HNSW:
                                   0 = ef; brute force: the over-fetch of the
                                   tensor-core scan, 0 = 4 k, at most 1024     */
-    uint32_t reserved1;
+    uint32_t filter;           /* 0, or a filter id from hnswgpu_filter_create
+                                  (its device-resident mask is used instead of
+                                  `allow`, which must then be NULL)           */
 } hnswgpu_search_opts;
 
 /* traversal precisions (hnswgpu_search_opts.precision) */
@@ -218,6 +220,21 @@ HNSWGPU_API int hnswgpu_unmark_deleted(hnswgpu_index* index, uint64_t label);
 HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint64_t nq, uint64_t k,
                    const hnswgpu_search_opts* opts, uint64_t* out_labels, float* out_dists,
                    int32_t* out_counts);
+
+/* A filter functor evaluated once over the index's labels and kept on the
+ * device: `allow` holds a byte per internal id (hnswgpu_get_labels order),
+ * nonzero = the functor accepts that label (hnswlib/hnswlib.h:128-132 calls
+ * the functor per candidate instead).  Searches name it by the returned id in
+ * hnswgpu_search_opts.filter, so repeated filtered searches copy no mask.
+ * hnswgpu_filter_destroy waits for the index's stream, then frees it. */
+HNSWGPU_API int hnswgpu_filter_create(hnswgpu_index* index, const uint8_t* allow, uint32_t* out_id);
+HNSWGPU_API int hnswgpu_filter_destroy(hnswgpu_index* index, uint32_t filter_id);
+
+/* HierarchicalNSW::saveIndex (hnswlib/hnswalg.h:685-712) of an index loaded
+ * from a file: the file it was loaded from, re-read, with every element's
+ * delete mark set as it is now (mark_deleted / unmark_deleted since the
+ * load), written to `path`. */
+HNSWGPU_API int hnswgpu_save_hnsw(hnswgpu_index* index, const char* path);
 
 /* Replaces HierarchicalNSW::searchStopConditionClosest with an
  * EpsilonSearchStopCondition(epsilon, min_candidates, max_candidates)

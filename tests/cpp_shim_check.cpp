@@ -8,11 +8,63 @@
 // EpsilonSearchStopCondition(eps, min, max) (tests/cpp/epsilon_search_test.cpp
 // drives the reference the same way).
 // Usage: cpp_shim_check index.bin queries.f32 dim nq k ef [eps min max]
+//        cpp_shim_check --timed index.bin queries.f32 dim nq k ef out.bin
+// The second form runs nq single-query searchKnn calls with a filter functor
+// of a type unrelated to hnswgpu::BaseFilterFunctor (the shape of
+// hnswlib::BaseFilterFunctor: even labels only), prints each result and, last,
+// the seconds the calls took; it also checks the ef_ proxy and writes the
+// index with one delete mark through saveIndex to out.bin.
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "hnswgpu.hpp"
+
+// A filter functor as hnswlib declares one (hnswlib/hnswlib.h:128-132),
+// not derived from hnswgpu::BaseFilterFunctor.
+namespace hnswlib_like {
+class BaseFilterFunctor {
+ public:
+    virtual bool operator()(size_t) { return true; }
+    virtual ~BaseFilterFunctor() {}
+};
+}  // namespace hnswlib_like
+struct PickEven : public hnswlib_like::BaseFilterFunctor {
+    bool operator()(size_t l) override { return l % 2 == 0; }
+};
+
+static int timed(int argc, char** argv) {
+    if (argc != 9) return 2;
+    const char* path = argv[2];
+    size_t dim = atoi(argv[4]), nq = atoi(argv[5]), k = atoi(argv[6]), ef = atoi(argv[7]);
+    std::vector<float> q(nq * dim);
+    FILE* f = fopen(argv[3], "rb");
+    if (!f || fread(q.data(), 4, q.size(), f) != q.size()) return 3;
+    fclose(f);
+    hnswgpu::L2Space space(dim);
+    hnswgpu::HierarchicalNSW<float> alg(&space, path);
+    alg.ef_ = ef;
+    if ((size_t)alg.ef_ != ef) return 20;
+    PickEven even;
+    hnswlib_like::BaseFilterFunctor* filter = &even;
+    std::vector<std::vector<std::pair<float, size_t>>> res(nq);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (size_t i = 0; i < nq; i++) res[i] = alg.searchKnnCloserFirst(q.data() + i * dim, k, filter);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    for (auto& r : res) {
+        for (auto& e : r) {
+            if (e.second % 2) return 21;
+            printf("%llu %.9g ", (unsigned long long)e.second, e.first);
+        }
+        printf("\n");
+    }
+    alg.markDelete(res[0][0].second);
+    alg.saveIndex(argv[8]);
+    printf("SECONDS %.6f\n", secs);
+    return 0;
+}
 
 struct PickNothing : public hnswgpu::BaseFilterFunctor {
     bool operator()(hnswgpu::labeltype) override { return false; }
@@ -24,6 +76,7 @@ struct PickDivisible : public hnswgpu::BaseFilterFunctor {
 };
 
 int main(int argc, char** argv) {
+    if (argc > 1 && strcmp(argv[1], "--timed") == 0) return timed(argc, argv);
     if (argc != 7 && argc != 10) return 2;
     const char* path = argv[1];
     size_t dim = atoi(argv[3]), nq = atoi(argv[4]), k = atoi(argv[5]), ef = atoi(argv[6]);

@@ -314,3 +314,27 @@ def test_config1_uniform_10k():
     gl, gd = b.knn_query(q, k=10)
     ml, md = O.bf_matrix("l2", x, q, 10)
     assert np.array_equal(gl, ml) and np.array_equal(gd.view(np.uint32), md.view(np.uint32))
+
+
+def test_filters_evaluated_per_call_and_registered():
+    """A plain callable is evaluated at every call, as the reference calls it
+    during every search (a stateful filter changed between calls is
+    honoured); a registered filter keeps its mask on the GPU and returns the
+    same results as the callable it was made from."""
+    g = golden()
+    q = g["hnsw_l2_d16/queries"]
+    idx = gpu_index(f"{GOLDEN}/hnsw_l2_d16.bin", "l2", 16)
+    idx.set_ef(32)
+    state = {"mod": 2}
+    flt = lambda l: l % state["mod"] == 0
+    l2, d2 = idx.knn_query(q, k=10, filter=flt)
+    state["mod"] = 3
+    l3, d3 = idx.knn_query(q, k=10, filter=flt)
+    assert np.all(l2 % 2 == 0) and np.all(l3 % 3 == 0)
+    assert np.array_equal(l2, g["hnsw_l2_d16/ef32_k10_even/labels"])
+    reg = idx.register_filter(lambda l: l % 2 == 0)
+    lr, dr = idx.knn_query(q, k=10, filter=reg)
+    assert np.array_equal(lr, l2) and np.array_equal(dr.view(np.uint32), d2.view(np.uint32))
+    reg.release()
+    with pytest.raises(RuntimeError):
+        idx.knn_query(q, k=10, filter=reg)
