@@ -32,12 +32,18 @@ def served(tmp_path_factory):
 
 
 def _mix(n, rng, parity_id):
+    """The serving mix of the 1M x 768 workload in miniature: k over {1, 10,
+    100}, ef over {32 .. 512}, 30 % filtered, 20 % tie-exact, 25 % fp8
+    traversal (id order), ~30 % of the id-order requests with the learned
+    stop."""
     reqs = []
     for i in range(n):
-        reqs.append(Server.request(k=int(rng.choice([1, 10, 100])), ef=int(rng.choice([32, 64, 128, 256])),
+        exact = rng.random() < 0.2
+        fp8 = not exact and rng.random() < 0.3
+        reqs.append(Server.request(k=int(rng.choice([1, 10, 100])), ef=int(rng.choice([32, 64, 128, 256, 512])),
                                    filter=parity_id if rng.random() < 0.3 else -1,
-                                   tie_order="reference" if rng.random() < 0.2 else "id",
-                                   learned=False, precision="fp32"))
+                                   tie_order="reference" if exact else "id",
+                                   learned=False, precision="fp8" if fp8 else "fp32"))
         if reqs[-1].flags == 0 and rng.random() < 0.3:
             reqs[-1].flags = H._capi.LEARNED_STOP
     return reqs
@@ -59,23 +65,26 @@ def test_same_alone_and_in_mix(served):
             r = reqs[i]
             t = srv.submit(q[i], k=r.k, ef=r.ef, filter=r.filter,
                            tie_order="reference" if r.flags & H._capi.EXACT_TIES else "id",
-                           learned=bool(r.flags & H._capi.LEARNED_STOP))
+                           learned=bool(r.flags & H._capi.LEARNED_STOP),
+                           precision="fp8" if r.precision == H._capi.PREC_FP8 else "fp32")
             al, ad, _ = srv.wait(t)
             assert mc[i] == len(al)
             assert np.array_equal(al, ml[i, :mc[i]]), i
             assert np.array_equal(ad.view(np.uint32), md[i, :mc[i]].view(np.uint32)), i
 
 
-def test_matches_batch_search(served):
+@pytest.mark.parametrize("precision", ["fp32", "fp8"])
+def test_matches_batch_search(served, precision):
     """A served request equals the batched C-ABI search with the same settings."""
     g, x, q = served
     with Server(g) as srv:
         parity = srv.add_filter(lambda l: l % 2 == 0)
         n = 300
-        reqs = [Server.request(k=10, ef=64, filter=parity if i % 2 else -1) for i in range(n)]
+        reqs = [Server.request(k=10, ef=64, filter=parity if i % 2 else -1, precision=precision) for i in range(n)]
         ml, md, mc, _ = srv.replay(q[:n], reqs, np.zeros(n))
-    fl, fd, fc, _ = g.knn_query_traced(q[:n], 10, filter=lambda l: l % 2 == 0, ef=64, tie_order="id")
-    ul, ud, uc, _ = g.knn_query_traced(q[:n], 10, ef=64, tie_order="id")
+    fl, fd, fc, _ = g.knn_query_traced(q[:n], 10, filter=lambda l: l % 2 == 0, ef=64, tie_order="id",
+                                       precision=precision)
+    ul, ud, uc, _ = g.knn_query_traced(q[:n], 10, ef=64, tie_order="id", precision=precision)
     for i in range(n):
         want = (fl, fc) if i % 2 else (ul, uc)
         assert mc[i] == want[1][i] and np.array_equal(ml[i, :mc[i]], want[0][i, :mc[i]])
