@@ -80,6 +80,8 @@ SIGNATURES = {
     "hnswgpu_search_noalloc": (C.c_int, [P, P, U64, U64, U64, U32, P, P, P, P, P]),
     "hnswgpu_noalloc_get_status": (C.c_int, [C.c_int, P, C.POINTER(U32)]),
     "hnswgpu_filter_create": (C.c_int, [P, P, C.POINTER(U32)]),
+    "hnswgpu_load_hnsw_multivector": (C.c_int, [C.c_char_p, U64, U64, C.c_int, C.POINTER(P)]),
+    "hnswgpu_search_multivector": (C.c_int, [P, P, U64, U64, U64, U64, P, P, P]),
     "hnswgpu_filter_destroy": (C.c_int, [P, U32]),
     "hnswgpu_save_hnsw": (C.c_int, [P, C.c_char_p]),
     "hnswgpu_selftest_wait_timeout": (C.c_int, [C.c_int, C.POINTER(U32)]),

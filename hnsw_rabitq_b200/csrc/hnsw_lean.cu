@@ -47,6 +47,32 @@
 
 namespace hnswgpu {
 
+// Optional self-checks (compile with -DHNSWGPU_BOUNDS_CHECK; the shipped
+// library is built without them): each global and shared-memory index of the
+// lean beam is checked against its buffer; the first violation is recorded in
+// g_lean_dbg (code, two values, block) and the access is skipped.
+#ifdef HNSWGPU_BOUNDS_CHECK
+__device__ unsigned long long g_lean_dbg[8];
+__device__ __forceinline__ bool lean_ok(bool cond, unsigned code, unsigned long long a, unsigned long long b) {
+    if (cond) return true;
+    if (atomicCAS(&g_lean_dbg[0], 0ull, (unsigned long long)code) == 0ull) {
+        g_lean_dbg[1] = a;
+        g_lean_dbg[2] = b;
+        g_lean_dbg[3] = blockIdx.x;
+    }
+    return false;
+}
+#define LCHK(cond, code, a, b) lean_ok((cond), (code), (unsigned long long)(a), (unsigned long long)(b))
+cudaError_t read_lean_debug_record(unsigned long long* out) {
+    cudaError_t e = cudaMemcpyFromSymbol(out, g_lean_dbg, sizeof(unsigned long long) * 8);
+    if (e != cudaSuccess) return e;
+    unsigned long long z[8] = {0};
+    return cudaMemcpyToSymbol(g_lean_dbg, z, sizeof(z));
+}
+#else
+#define LCHK(cond, code, a, b) true
+#endif
+
 namespace {
 
 struct LeanSmem {
@@ -159,11 +185,12 @@ __device__ __forceinline__ float lean_pass(const SearchParams& p, const LeanSmem
     const unsigned char* rows[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-        valid[r] = base + 4 * g + r < nnew;
+        valid[r] = base + 4 * g + r < nnew && LCHK(base + 4 * g + r < 64, 199, base, nnew);
+        if (valid[r] && !LCHK(ids[r] < p.count, 200, ids[r], p.count)) valid[r] = false;
         rows[r] = p.tvecs + (size_t)(valid[r] ? ids[r] : 0u) * p.trow_bytes;
     }
     my_id = t == 0 ? ids[0] : t == 1 ? ids[1] : t == 2 ? ids[2] : ids[3];
-    const bool mine = base + lane < nnew;
+    const bool mine = base + lane < nnew && LCHK(my_id < p.count, 201, my_id, base + lane);
     float2 tail = make_float2(0.f, 0.f);
     if (mine) tail = __ldg(reinterpret_cast<const float2*>(p.tvecs + (size_t)my_id * p.trow_bytes + D));
     float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
@@ -225,12 +252,12 @@ __device__ __forceinline__ int lean_merge(uint64_t* pool, int& size, int cap, un
             int sh = 0;
             for (unsigned m = amask; m; m &= m - 1) sh += shfl64(key, __ffs(m) - 1) < em;
             __syncwarp();
-            if (have && i + sh < cap) pool[i + sh] = e;
+            if (have && i + sh < cap && LCHK(i + sh >= 0, 231, i, sh)) pool[i + sh] = e;
             __syncwarp();
         }
     }
     const int np = pos + rank;
-    if (mine && np < cap) pool[np] = key;
+    if (mine && np < cap && LCHK(np >= 0 && pos <= size, 232, np, pos)) pool[np] = key;
     __syncwarp();
     top = __any_sync(FULL, mine && np < kq);
     size = min(size + na, cap);
@@ -300,7 +327,8 @@ __device__ void lean_rerank(const SearchParams& p, const LeanSmem& s, int lane, 
     for (int b = 0; b < R; b += 8) {
         const int v = b + (lane >> 2);
         const bool valid = v < R;
-        const uint32_t id = kid(s.pool[valid ? v : b]);
+        uint32_t id = kid(s.pool[valid ? v : b]);
+        if (!LCHK(id < p.count && R <= (int)p.ef, 250, id, R)) id = 0;
         const float4* x4 = reinterpret_cast<const float4*>(p.vecs + (size_t)id * p.row_floats);
         float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f;
         for (int cb = 0; cb < n16; cb += 4) {
@@ -338,7 +366,7 @@ __device__ void lean_rerank(const SearchParams& p, const LeanSmem& s, int lane, 
         const uint64_t kr = s.pool[r];
         int rank = 0;
         for (int t = 0; t < R; t++) rank += s.pool[t] < kr;
-        tmp[rank] = kr;
+        if (LCHK((size_t)(rank + 1) * 8 <= ((size_t)4 << p.log2_vis), 252, rank, R)) tmp[rank] = kr;
     }
     __syncwarp();
     for (int r = lane; r < R; r += 32) s.pool[r] = tmp[r];
@@ -418,8 +446,9 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     const uint32_t up_stride = p.maxM + 1;
     for (int level = p.maxlevel; level > 0; level--) {
         while (true) {
+            if (!LCHK(cur < p.count && p.upper_off[cur] != 0xffffffffu, 270, cur, level)) break;
             const uint32_t* row = p.upper_links + (size_t)(p.upper_off[cur] + (uint32_t)(level - 1)) * up_stride;
-            const int cnt = (int)(__ldg(row) & 0xffffu);
+            const int cnt = LCHK((__ldg(row) & 0xffffu) <= p.maxM, 271, __ldg(row), cur) ? (int)(__ldg(row) & 0xffffu) : 0;
             ct.upper_hops += 1;
             ct.upper_dists += cnt;
             float best = curd;
@@ -480,7 +509,8 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
                 continue;
             }
             const int take = min(__popc(m), W - sel);
-            if (u && __popc(m & lanemask_lt()) < take) s.pool[i] = e | EXP_BIT;
+            if (u && __popc(m & lanemask_lt()) < take && LCHK(i < ef && psize <= ef, 230, i, psize))
+                s.pool[i] = e | EXP_BIT;
             const int src0 = __ffs(m) - 1;
             const uint32_t id0 = __shfl_sync(FULL, kid(e), src0);
             const uint32_t dk0 = __shfl_sync(FULL, khi(e), src0);
@@ -515,9 +545,13 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         uint32_t id0 = INVALID_ID, id1 = INVALID_ID;
         {
             const int j0 = lane, ci0 = j0 >= maxM0 ? 1 : 0;
-            if (ci0 < sel) id0 = __ldg(p.links0 + (size_t)(ci0 ? cand1 : cand0) * maxM0 + (j0 - ci0 * maxM0));
+            if (ci0 < sel && LCHK((ci0 ? cand1 : cand0) < p.count, 210, ci0 ? cand1 : cand0, sel) &&
+                LCHK(j0 - ci0 * maxM0 < maxM0, 211, j0, ci0))
+                id0 = __ldg(p.links0 + (size_t)(ci0 ? cand1 : cand0) * maxM0 + (j0 - ci0 * maxM0));
             const int j1 = lane + 32, ci1 = j1 >= maxM0 ? (j1 >= 2 * maxM0 ? 2 : 1) : 0;
-            if (ci1 < sel) id1 = __ldg(p.links0 + (size_t)(ci1 ? cand1 : cand0) * maxM0 + (j1 - ci1 * maxM0));
+            if (ci1 < sel && LCHK((ci1 ? cand1 : cand0) < p.count, 212, ci1 ? cand1 : cand0, sel) &&
+                LCHK(j1 - ci1 * maxM0 < maxM0 && j1 - ci1 * maxM0 >= 0, 213, j1, ci1))
+                id1 = __ldg(p.links0 + (size_t)(ci1 ? cand1 : cand0) * maxM0 + (j1 - ci1 * maxM0));
         }
         bool f0 = id0 != INVALID_ID, f1 = id1 != INVALID_ID;
         if (!p.links_unique) {
@@ -540,8 +574,8 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         const unsigned m0 = __ballot_sync(FULL, f0), m1 = __ballot_sync(FULL, f1);
         const int n0 = __popc(m0);
         const int nnew = n0 + __popc(m1);
-        if (f0) s.cid[__popc(m0 & lanemask_lt())] = id0;
-        if (f1) s.cid[n0 + __popc(m1 & lanemask_lt())] = id1;
+        if (f0 && LCHK(id0 < p.count, 214, id0, lane)) s.cid[__popc(m0 & lanemask_lt())] = id0;
+        if (f1 && LCHK(id1 < p.count, 215, id1, lane)) s.cid[n0 + __popc(m1 & lanemask_lt())] = id1;
         __syncwarp();
         if (nnew == 0) continue;
         ct.l0_dists += (uint32_t)nnew;
@@ -599,18 +633,21 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     uint64_t* olab = p.out_labels + (size_t)qi * kq;
     float* odist = p.out_dists + (size_t)qi * kq;
     for (int r = lane; r < kk; r += 32) {
-        const uint64_t e = s.pool[r];
+        uint64_t e = s.pool[r];
+        if (!LCHK(kid(e) < p.count, 260, kid(e), r)) e = 0;
         const uint32_t dk = khi(e);
         const uint64_t lab = p.labels[kid(e)];
         int st = r;
         while (st > 0 && khi(s.pool[st - 1]) == dk) st--;
         int below = 0;
         for (int t = st; t < kk && khi(s.pool[t]) == dk; t++) {
-            const uint64_t lt = p.labels[kid(s.pool[t])];
+            const uint64_t lt = LCHK(kid(s.pool[t]) < p.count, 261, kid(s.pool[t]), t) ? p.labels[kid(s.pool[t])] : 0;
             if (t != r && (lt < lab || (lt == lab && t < r))) below++;
         }
-        olab[st + below] = lab;
-        odist[st + below] = funkey(dk);
+        if (LCHK(st + below < kk, 262, st + below, kk)) {
+            olab[st + below] = lab;
+            odist[st + below] = funkey(dk);
+        }
     }
     for (int r = kk + lane; r < kq; r += 32) {
         olab[r] = ~0ull;
@@ -631,6 +668,9 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
     s.lacc = reinterpret_cast<uint64_t*>(base + p.off_lacc);
     s.pool = reinterpret_cast<uint64_t*>(base + p.off_pool);
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
+    if (!LCHK(p.off_vis + ((size_t)4 << p.log2_vis) <= p.warp_smem && p.off_pool + (size_t)8 * p.ef <= p.off_vis,
+              280, p.off_vis, p.warp_smem))
+        return;
     while (true) {
         uint32_t qi = 0;
         if (lane == 0) {

@@ -36,6 +36,7 @@
 #include "bf_tc.h"
 #include "device_common.cuh"
 #include "hnsw_search.h"
+#include "hnsw_multivec.h"
 
 static_assert(HNSWGPU_TERM_PARAMS == hnswgpu::kTermParams, "termination parameter count");
 static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feature count");
@@ -85,7 +86,8 @@ void init_common(hnswgpu_index* h, int device) {
 // HierarchicalNSW::loadIndex (hnswlib/hnswalg.h:715-821) plus the structural
 // checks a GPU kernel needs before it may follow the links (ids in range,
 // upper-level lists present where the descent reads them).
-void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim, uint64_t max_elements_i) {
+void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim, uint64_t max_elements_i,
+                    bool multivector) {
     std::ifstream in(path, std::ios::binary);
     if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
     in.seekg(0, in.end);
@@ -136,7 +138,10 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
     if (space == HNSWGPU_SPACE_L2_UINT8 && dim * 65025ull >= (1ull << 24))
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED,
                        "uint8 L2 needs dim <= 258 (integer distances exact in float32)");
-    if (offsetLevel0 != 0 || offsetData != size_links0 || label_offset != offsetData + dim * elem ||
+    // a multi-vector index (MultiVectorL2Space, hnswlib/stop_condition.h:7-76)
+    // stores a 32-bit document id right after each vector
+    const uint64_t doc_bytes = multivector ? 4 : 0;
+    if (offsetLevel0 != 0 || offsetData != size_links0 || label_offset != offsetData + dim * elem + doc_bytes ||
         size_data != label_offset + 8)
         throw ApiError(HNSWGPU_ERR_FORMAT,
                        "index layout does not match dim=" + std::to_string(dim) + " (" + corrupt + ")");
@@ -164,6 +169,7 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
     std::vector<float> hv(cur * h->row_floats, 0.f);
     std::vector<uint32_t> hl(cur * maxM0, 0xffffffffu);
     h->labels.resize(cur);
+    std::vector<uint32_t> hdocs(multivector ? cur : 0);
     h->deleted.assign((cur + 31) / 32 + 1, 0u);
     h->num_deleted = 0;
     for (uint64_t r0 = 0; r0 < cur; r0 += chunk_rows) {
@@ -193,6 +199,7 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
             } else {
                 memcpy(&hv[i * h->row_floats], rec + offsetData, dim * 4);
             }
+            if (multivector) memcpy(&hdocs[i], rec + offsetData + dim * 4, 4);
             uint64_t lab;
             memcpy(&lab, rec + label_offset, 8);
             h->labels[i] = lab;
@@ -262,6 +269,10 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
     up(h->upper_links.p, hup.data(), hup.size() * 4);
     up(h->dlabels.p, h->labels.data(), cur * 8);
     up(h->deleted_bits.p, h->deleted.data(), h->deleted.size() * 4);
+    if (multivector) {
+        h->docs.alloc(std::max<size_t>(cur, 1));
+        up(h->docs.p, hdocs.data(), cur * 4);
+    }
 }
 
 // BruteforceSearch::loadIndex (hnswlib/bruteforce.h:142-161).
@@ -854,6 +865,7 @@ void run_search(hnswgpu_index* h, const float* dq, uint64_t nq, uint64_t k, uint
 #ifdef HNSWGPU_BOUNDS_CHECK
 namespace hnswgpu {
 cudaError_t read_debug_record(unsigned long long* out);
+cudaError_t read_lean_debug_record(unsigned long long* out);
 }
 #endif
 
@@ -871,9 +883,99 @@ int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_el
         *out = nullptr;
         std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
         init_common(h.get(), device);
-        load_hnsw_file(h.get(), path, space, dim, max_elements);
+        load_hnsw_file(h.get(), path, space, dim, max_elements, false);
         h->source_path = path;
         *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_load_hnsw_multivector(const char* path, uint64_t dim, uint64_t max_elements, int device,
+                                  hnswgpu_index** out) {
+    return guarded([&] {
+        if (!path || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        *out = nullptr;
+        std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
+        init_common(h.get(), device);
+        load_hnsw_file(h.get(), path, HNSWGPU_SPACE_L2, dim, max_elements, true);
+        h->source_path = path;
+        *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_search_multivector(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t num_docs,
+                               uint64_t ef_collection, uint64_t cap, uint64_t* out_ids, float* out_dists,
+                               int32_t* out_counts) {
+    return guarded([&] {
+        if (!h || h->is_bf || (nq && (!queries || !out_ids || !out_dists || !out_counts)) || cap == 0)
+            return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (!h->docs.p) return fail(HNSWGPU_ERR_STATE, "not a multi-vector index (hnswgpu_load_hnsw_multivector)");
+        if (num_docs == 0) return fail(HNSWGPU_ERR_ARG, "num_docs must be > 0");
+        if (nq > 0x7fffffffull || cap > 0xffffffffull || num_docs > 0xffffffffull || ef_collection > 0xffffffffull)
+            return fail(HNSWGPU_ERR_ARG, "batch too large");
+        if (h->num_deleted)
+            return fail(HNSWGPU_ERR_UNSUPPORTED, "multi-vector search over an index with deleted elements");
+        if (h->maxM0 > 64) return fail(HNSWGPU_ERR_UNSUPPORTED, "multi-vector search needs maxM0 <= 64");
+        std::lock_guard<std::mutex> g(h->mu);
+        set_device(h);
+        if (nq == 0) return HNSWGPU_OK;
+        if (h->count == 0) {
+            memset(out_counts, 0, nq * 4);
+            for (uint64_t i = 0; i < nq * cap; i++) {
+                out_ids[i] = ~0ull;
+                out_dists[i] = __builtin_inff();
+            }
+            return HNSWGPU_OK;
+        }
+        hnswgpu::MvParams p{};
+        p.vecs = h->vecs.p;
+        p.links0 = h->links0.p;
+        p.upper_off = h->upper_off.p;
+        p.upper_links = h->upper_links.p;
+        p.docs = h->docs.p;
+        p.count = (uint32_t)h->count;
+        p.dim = (uint32_t)h->dim;
+        p.row_floats = h->row_floats;
+        p.maxM = (uint32_t)h->maxM;
+        p.maxM0 = (uint32_t)h->maxM0;
+        p.ep = h->ep;
+        p.maxlevel = h->maxlevel;
+        p.nq = (uint32_t)nq;
+        p.num_docs = (uint32_t)num_docs;
+        p.ef_coll = (uint32_t)ef_collection;
+        p.cap = (uint32_t)cap;
+        p.max_expansions = (uint32_t)std::min<uint64_t>(0xffffff00ull, 2 * h->count + 1024);
+        // the largest layout that fits: top_candidates up to 2048 entries,
+        // the document table and the visited set sized from the index
+        int max_optin = 0;
+        cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+        p.top_cap = 2048;
+        p.doc_log2 = 12;
+        p.vis_log2 = (uint32_t)std::min<uint64_t>(14, std::max<uint64_t>(10, next_pow2_log2(2 * h->count)));
+        while (hnswgpu::multivec_smem(p) > (size_t)max_optin && p.top_cap > 256) p.top_cap /= 2;
+        while (hnswgpu::multivec_smem(p) > (size_t)max_optin && p.vis_log2 > 10) p.vis_log2--;
+        if (hnswgpu::multivec_smem(p) > (size_t)max_optin)
+            return fail(HNSWGPU_ERR_UNSUPPORTED, "multi-vector search: dim too large for the shared-memory layout");
+        DevBuf<float> dq;
+        DevBuf<uint64_t> di;
+        DevBuf<float> dd;
+        DevBuf<int32_t> dc;
+        dq.alloc(nq * h->dim);
+        di.alloc(nq * cap);
+        dd.alloc(nq * cap);
+        dc.alloc(nq);
+        cuda_check(cudaMemcpyAsync(dq.p, queries, nq * h->dim * 4, cudaMemcpyHostToDevice, h->stream), "cudaMemcpyAsync");
+        p.queries = dq.p;
+        p.out_ids = di.p;
+        p.out_dists = dd.p;
+        p.out_counts = dc.p;
+        p.status = h->status.p;
+        cuda_check(hnswgpu::launch_hnsw_multivec(p, h->num_sms, h->stream), "multivector launch");
+        cuda_check(cudaMemcpyAsync(out_ids, di.p, nq * cap * 8, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_dists, dd.p, nq * cap * 4, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaMemcpyAsync(out_counts, dc.p, nq * 4, cudaMemcpyDeviceToHost, h->stream), "cudaMemcpyAsync");
+        cuda_check(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
         return HNSWGPU_OK;
     });
 }
@@ -1457,6 +1559,8 @@ int hnswgpu_get_status(hnswgpu_index* h, uint32_t* out_bits) {
 // Self-checking builds only: first recorded violation (code, a, b, block).
 HNSWGPU_API int hnswgpu_debug_record(unsigned long long* out) {
     cudaDeviceSynchronize();
+    if (hnswgpu::read_lean_debug_record(out) != cudaSuccess) return HNSWGPU_ERR_CUDA;
+    if (out[0]) return HNSWGPU_OK;
     return hnswgpu::read_debug_record(out) == cudaSuccess ? HNSWGPU_OK : HNSWGPU_ERR_CUDA;
 }
 #endif

@@ -77,6 +77,7 @@ struct hnswgpu_index {
     DevBuf<float> vecs;
     DevBuf<uint32_t> links0, upper_off, upper_links, deleted_bits;
     DevBuf<uint64_t> dlabels;
+    DevBuf<uint32_t> docs;  // multi-vector index: document id per element (else empty)
     // per-call workspace
     DevBuf<uint32_t> counters;  // ring of work counters
     uint32_t next_counter = 0;

@@ -475,6 +475,40 @@ class Index(_GpuIndex):
                                                        C.byref(opts), _ptr(ids), _ptr(dists), _ptr(counts)))
         return ids, dists, counts
 
+    def load_multivector_index(self, path_to_index: str, max_elements: int = 0) -> None:
+        """Load a multi-vector index: a HierarchicalNSW that the C++ API built
+        over a MultiVectorL2Space (hnswlib/stop_condition.h:7-76), whose
+        elements carry a 32-bit document id after the vector (L2 only)."""
+        if self.space != "l2":
+            raise RuntimeError("multi-vector indexes use the l2 space")
+        self._free()
+        h = C.c_void_p()
+        _capi.check(_capi.lib().hnswgpu_load_hnsw_multivector(str(path_to_index).encode(), self.dim,
+                                                              int(max_elements), self.device, C.byref(h)))
+        self._h = h
+        self._default_ef = 10
+        self._source = os.path.abspath(str(path_to_index))
+        self._marks = {}
+        self._max_elements = None
+
+    def search_multivector(self, data, num_docs: int, ef_collection: int, cap: int = 1024):
+        """The C++ API's searchStopConditionClosest with a
+        MultiVectorSearchStopCondition(space, num_docs, ef_collection)
+        (hnswalg.h:1326-1377, stop_condition.h:146-216) on an index loaded by
+        load_multivector_index: per query, the elements of the num_docs
+        nearest documents in the reference's result order, (ids uint64 [N,
+        cap], distances float32 [N, cap], counts int32 [N]); as in the
+        reference the ids are internal ids; a count of -1 means the result
+        has more than `cap` elements (or outgrew the kernel's heaps)."""
+        q, _ = self._queries(data, 1)
+        nq, cap = q.shape[0], int(cap)
+        ids = np.empty((nq, cap), np.uint64)
+        dists = np.empty((nq, cap), np.float32)
+        counts = np.empty(nq, np.int32)
+        _capi.check(_capi.lib().hnswgpu_search_multivector(self._h, _ptr(q), nq, int(num_docs), int(ef_collection),
+                                                           cap, _ptr(ids), _ptr(dists), _ptr(counts)))
+        return ids, dists, counts
+
     def knn_query_exact(self, data, k: int = 1, filter: Optional[Callable[[int], bool]] = None):
         """Exact k-NN by an exhaustive GPU scan of the index's vectors (the
         ground truth of recall measurements): (labels, distances)."""

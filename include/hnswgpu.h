@@ -221,6 +221,26 @@ HNSWGPU_API int hnswgpu_search(hnswgpu_index* index, const float* queries, uint6
                    const hnswgpu_search_opts* opts, uint64_t* out_labels, float* out_dists,
                    int32_t* out_counts);
 
+/* Multi-vector indexes: a HierarchicalNSW over a MultiVectorL2Space
+ * (hnswlib/stop_condition.h:7-76), whose elements carry a 32-bit document id
+ * right after the vector.  The loader is hnswgpu_load_hnsw's with that
+ * element layout (L2 space). */
+HNSWGPU_API int hnswgpu_load_hnsw_multivector(const char* path, uint64_t dim, uint64_t max_elements, int device,
+                                              hnswgpu_index** out);
+
+/* searchStopConditionClosest with a MultiVectorSearchStopCondition(space,
+ * num_docs, ef_collection) (hnswlib/hnswalg.h:1326-1377,
+ * hnswlib/stop_condition.h:146-216): per query, the elements of the num_docs
+ * nearest documents as the reference returns them -- closest first, equal
+ * distances in its heap's pop order, INTERNAL ids (the reference copies
+ * top_candidates' ids unchanged).  Host buffers: out_ids / out_dists nq x cap,
+ * out_counts[i] = the result's size, or -1 when it has more than cap entries
+ * or the query outgrew the kernel's fixed heaps (HNSWGPU_STATUS_OVERFLOW is
+ * then raised too).  Indexes with deleted elements are not supported. */
+HNSWGPU_API int hnswgpu_search_multivector(hnswgpu_index* index, const float* queries, uint64_t nq,
+                                           uint64_t num_docs, uint64_t ef_collection, uint64_t cap,
+                                           uint64_t* out_ids, float* out_dists, int32_t* out_counts);
+
 /* A filter functor evaluated once over the index's labels and kept on the
  * device: `allow` holds a byte per internal id (hnswgpu_get_labels order),
  * nonzero = the functor accepts that label (hnswlib/hnswlib.h:128-132 calls
