@@ -82,6 +82,8 @@ struct LeanSmem {
     uint64_t* lacc;      // accepted keys of one iteration, compacted (64)
     uint64_t* pool;      // sorted (distance key, id | EXP_BIT), at most ef
     uint32_t* vis;       // direct-mapped visited cache; re-rank scratch after the beam
+    unsigned char* stage;  // 32 row slots (lean_stage bytes apart): one distance pass's gathered rows
+    float2* tails;       // 32 (scale, squared norm) of the pass's candidates
 };
 
 struct LeanQuery {
@@ -114,6 +116,19 @@ __device__ __forceinline__ uint2 ldg_stream8(const void* p) {
     return v;
 }
 
+// Per-lane asynchronous copies global -> shared (no registers held while
+// they are in flight); each lane later reads back only what it copied, so
+// waiting for its own copies is enough.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 // Byte layout of one 128-byte block of a row (or of the whole row when it is
 // shorter) over the four lanes t of a quad: lane t reads load units of U
 // bytes (U = 16 when NS is even, else 8) at offsets (4 j + t) U, j = 0, 1, ...
@@ -125,8 +140,22 @@ __device__ __forceinline__ int lane_step_offset(int st, int t) {
     return NS % 2 == 0 ? ((st >> 1) * 4 + t) * 16 + (st & 1) * 8 : (st * 4 + t) * 8;
 }
 
+// Copy this lane's quarter of a row block (its load units) into its stage
+// slot, same offsets.
 template <int NS>
-__device__ __forceinline__ void load_quarter(const unsigned char* row, int t, bool valid, uint32_t (&r)[2 * NS]) {
+__device__ __forceinline__ void stage_quarter(uint32_t slot, const unsigned char* row, int t) {
+    if (NS % 2 == 0) {
+#pragma unroll
+        for (int j = 0; j < NS / 2; j++) cp_async16(slot + (j * 4 + t) * 16, row + (j * 4 + t) * 16);
+    } else {
+#pragma unroll
+        for (int j = 0; j < NS; j++) cp_async8(slot + (j * 4 + t) * 8, row + (j * 4 + t) * 8);
+    }
+}
+
+// Read the quarter back (zero for an empty row) as the mma A operand bytes.
+template <int NS>
+__device__ __forceinline__ void read_quarter(const unsigned char* slot, int t, bool valid, uint32_t (&r)[2 * NS]) {
     if (!valid) {
 #pragma unroll
         for (int i = 0; i < 2 * NS; i++) r[i] = 0u;
@@ -135,7 +164,7 @@ __device__ __forceinline__ void load_quarter(const unsigned char* row, int t, bo
     if (NS % 2 == 0) {
 #pragma unroll
         for (int j = 0; j < NS / 2; j++) {
-            const uint4 v = ldg_stream16(row + (j * 4 + t) * 16);
+            const uint4 v = *reinterpret_cast<const uint4*>(slot + (j * 4 + t) * 16);
             r[4 * j] = v.x;
             r[4 * j + 1] = v.y;
             r[4 * j + 2] = v.z;
@@ -144,7 +173,7 @@ __device__ __forceinline__ void load_quarter(const unsigned char* row, int t, bo
     } else {
 #pragma unroll
         for (int j = 0; j < NS; j++) {
-            const uint2 v = ldg_stream8(row + (j * 4 + t) * 8);
+            const uint2 v = *reinterpret_cast<const uint2*>(slot + (j * 4 + t) * 8);
             r[2 * j] = v.x;
             r[2 * j + 1] = v.y;
         }
@@ -172,48 +201,63 @@ __device__ __forceinline__ void load_bfrag(const LeanSmem& s, uint32_t D, int bl
 // + 2 in row g + 8, tile 1 holds base + 4g + 1 and base + 4g + 3.  With the
 // hi / lo query in the even / odd columns of B, lane (g, t) receives both
 // products of candidate base + 4g + t in its accumulator pair (c0, c1) or
-// (c2, c3).
+// (c2, c3).  Each lane gathers its quarter of the quad's four rows (and the
+// scale / norm tail of its own candidate) into its stage slots with
+// asynchronous copies, then reads them back tile by tile.
 template <int SPACE, int NS, bool MULTI>
-__device__ __forceinline__ float lean_pass(const SearchParams& p, const LeanSmem& s, const LeanQuery& lq,
-                                           const uint32_t (&bq)[2 * NS], int base, int nnew, int lane,
-                                           uint32_t& my_id) {
+__device__ __forceinline__ float lean_pass(const SearchParams& p, const LeanSmem& s, const LeanQuery& lq, int base,
+                                           int nnew, int lane, uint32_t& my_id) {
     const int g = lane >> 2, t = lane & 3;
     const uint4 ids4 = *reinterpret_cast<const uint4*>(s.cid + base + 4 * g);
     const uint32_t ids[4] = {ids4.x, ids4.y, ids4.z, ids4.w};
     const uint32_t D = p.trow_bytes - 16;
+    const uint32_t SS = p.lean_stage;  // stage slot stride (bytes)
     bool valid[4];
-    const unsigned char* rows[4];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         valid[r] = base + 4 * g + r < nnew && LCHK(base + 4 * g + r < 64, 199, base, nnew);
         if (valid[r] && !LCHK(ids[r] < p.count, 200, ids[r], p.count)) valid[r] = false;
-        rows[r] = p.tvecs + (size_t)(valid[r] ? ids[r] : 0u) * p.trow_bytes;
     }
     my_id = t == 0 ? ids[0] : t == 1 ? ids[1] : t == 2 ? ids[2] : ids[3];
     const bool mine = base + lane < nnew && LCHK(my_id < p.count, 201, my_id, base + lane);
-    float2 tail = make_float2(0.f, 0.f);
-    if (mine) tail = __ldg(reinterpret_cast<const float2*>(p.tvecs + (size_t)my_id * p.trow_bytes + D));
+    const uint32_t stage = smem_u32(s.stage);
     float c0[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    float2 tail = make_float2(0.f, 0.f);
     const int nblk = MULTI ? (int)(D >> 7) : 1;
     for (int blk = 0; blk < nblk; blk++) {
-        uint32_t a[4][2 * NS];
 #pragma unroll
-        for (int r = 0; r < 4; r++) load_quarter<NS>(rows[r] + blk * 128, t, valid[r], a[r]);
-        uint32_t bm[2 * NS];
-        if (MULTI) load_bfrag<NS>(s, D, blk, lane, bm);
+        for (int r = 0; r < 4; r++)
+            if (valid[r])
+                stage_quarter<NS>(stage + (uint32_t)(4 * g + r) * SS,
+                                  p.tvecs + (size_t)ids[r] * p.trow_bytes + blk * 128, t);
+        if (blk == 0 && mine)
+            cp_async8(smem_u32(s.tails + lane), p.tvecs + (size_t)my_id * p.trow_bytes + D);
+        cp_async_wait_all();
+        uint32_t b[2 * NS];
+        load_bfrag<NS>(s, D, blk, lane, b);
         __syncwarp();  // mma.sync needs the whole warp converged
+        // tile 0: rows (g, g + 8) = candidates 4g, 4g + 2; tile 1: 4g + 1, 4g + 3
 #pragma unroll
-        for (int st = 0; st < NS; st++) {
-            const uint32_t b0 = MULTI ? bm[2 * st] : bq[2 * st], b1 = MULTI ? bm[2 * st + 1] : bq[2 * st + 1];
-            mma_e4m3(c0, a[0][2 * st], a[2][2 * st], a[0][2 * st + 1], a[2][2 * st + 1], b0, b1);
-            mma_e4m3(c1, a[1][2 * st], a[3][2 * st], a[1][2 * st + 1], a[3][2 * st + 1], b0, b1);
+        for (int tile = 0; tile < 2; tile++) {
+            uint32_t a0[2 * NS], a1[2 * NS];
+            read_quarter<NS>(s.stage + (4 * g + tile) * SS, t, valid[tile], a0);
+            read_quarter<NS>(s.stage + (4 * g + tile + 2) * SS, t, valid[tile + 2], a1);
+#pragma unroll
+            for (int st = 0; st < NS; st++) {
+                if (tile == 0) mma_e4m3(c0, a0[2 * st], a1[2 * st], a0[2 * st + 1], a1[2 * st + 1], b[2 * st], b[2 * st + 1]);
+                else mma_e4m3(c1, a0[2 * st], a1[2 * st], a0[2 * st + 1], a1[2 * st + 1], b[2 * st], b[2 * st + 1]);
+            }
         }
+        if (blk == 0 && mine) tail = s.tails[lane];
+        if (MULTI) __syncwarp();
     }
     const float hi = t == 0 ? c0[0] : t == 1 ? c1[0] : t == 2 ? c0[2] : c1[2];
     const float lo = t == 0 ? c0[1] : t == 1 ? c1[1] : t == 2 ? c0[3] : c1[3];
-    const float dot = tail.x * fmaf(lq.s_hi, hi, lq.s_lo * lo);
-    if (SPACE == 0) return fmaf(-2.0f, dot, lq.qn + tail.y);
-    return 1.0f - dot;
+    // explicit rounding: every call site must give a node the same key (the
+    // pool recognises a node evaluated again by its exact key)
+    const float dot = __fmul_rn(tail.x, __fmaf_rn(lq.s_hi, hi, __fmul_rn(lq.s_lo, lo)));
+    if (SPACE == 0) return __fmaf_rn(-2.0f, dot, __fadd_rn(lq.qn, tail.y));
+    return __fsub_rn(1.0f, dot);
 }
 
 // Count of entries of the sorted array a[0, n) whose key (flag masked) is < key.
@@ -360,12 +404,13 @@ __device__ void lean_rerank(const SearchParams& p, const LeanSmem& s, int lane, 
         if (a == 0 && valid) s.pool[v] = mkkey(r, id);
         __syncwarp();
     }
-    // rank by counting into the idle visited cache, then copy back
+    // rank by counting into the idle visited cache (equal keys by position,
+    // so every slot is written), then copy back
     uint64_t* tmp = reinterpret_cast<uint64_t*>(s.vis);
     for (int r = lane; r < R; r += 32) {
         const uint64_t kr = s.pool[r];
         int rank = 0;
-        for (int t = 0; t < R; t++) rank += s.pool[t] < kr;
+        for (int t = 0; t < R; t++) rank += s.pool[t] < kr || (s.pool[t] == kr && t < r);
         if (LCHK((size_t)(rank + 1) * 8 <= ((size_t)4 << p.log2_vis), 252, rank, R)) tmp[rank] = kr;
     }
     __syncwarp();
@@ -433,14 +478,12 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     const uint32_t nvis = 1u << p.log2_vis;
     for (uint32_t i = lane; i < nvis; i += 32) s.vis[i] = INVALID_ID;
     __syncwarp();
-    uint32_t bq[2 * NS];
-    if (!MULTI) load_bfrag<NS>(s, D, 0, lane, bq);
 
     // ---- upper-layer greedy descent (hnswalg.h:1274-1302) on the fp8 rows
     uint32_t cur = p.ep, unused;
     if (lane == 0) s.cid[0] = cur;
     __syncwarp();
-    float curd = __shfl_sync(FULL, lean_pass<SPACE, NS, MULTI>(p, s, lq, bq, 0, 1, lane, unused), 0);
+    float curd = __shfl_sync(FULL, lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, 1, lane, unused), 0);
     __syncwarp();
     ct.upper_dists += 1;
     const uint32_t up_stride = p.maxM + 1;
@@ -459,9 +502,9 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
                 if (lane + 32 < n) s.cid[lane + 32] = __ldg(row + 1 + c0 + lane + 32);
                 __syncwarp();
                 uint32_t i0, i1 = INVALID_ID;
-                float d0 = lean_pass<SPACE, NS, MULTI>(p, s, lq, bq, 0, n, lane, i0);
+                float d0 = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, n, lane, i0);
                 float d1 = __int_as_float(0x7f800000);
-                if (n > 32) d1 = lean_pass<SPACE, NS, MULTI>(p, s, lq, bq, 32, n, lane, i1);
+                if (n > 32) d1 = lean_pass<SPACE, NS, MULTI>(p, s, lq, 32, n, lane, i1);
                 if (lane >= n) d0 = __int_as_float(0x7f800000);
                 if (lane + 32 >= n) d1 = __int_as_float(0x7f800000);
                 float m = fminf(d0, d1);
@@ -582,9 +625,9 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
 
         // ---- distances (lane L: candidates L and L + 32)
         uint32_t cidA, cidB = INVALID_ID;
-        const float dA = lean_pass<SPACE, NS, MULTI>(p, s, lq, bq, 0, nnew, lane, cidA);
+        const float dA = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, nnew, lane, cidA);
         float dB = 0.f;
-        if (nnew > 32) dB = lean_pass<SPACE, NS, MULTI>(p, s, lq, bq, 32, nnew, lane, cidB);
+        if (nnew > 32) dB = lean_pass<SPACE, NS, MULTI>(p, s, lq, 32, nnew, lane, cidB);
 
         // ---- acceptance by the beam's bound
         const bool full = psize == ef;
@@ -668,6 +711,8 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
     s.lacc = reinterpret_cast<uint64_t*>(base + p.off_lacc);
     s.pool = reinterpret_cast<uint64_t*>(base + p.off_pool);
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
+    s.stage = base + p.off_stage;
+    s.tails = reinterpret_cast<float2*>(base + p.off_lacc + 64 * 8);
     if (!LCHK(p.off_vis + ((size_t)4 << p.log2_vis) <= p.warp_smem && p.off_pool + (size_t)8 * p.ef <= p.off_vis,
               280, p.off_vis, p.warp_smem))
         return;
@@ -765,7 +810,12 @@ size_t lean_smem_layout(SearchParams& p) {
     p.off_cid = (uint32_t)off;
     off += 64 * 4;
     p.off_lacc = (uint32_t)off;
-    off += 64 * 8;
+    off += 64 * 8 + 32 * 8;  // accepted keys, then the pass's 32 row tails
+    // stage slots: one 128-byte block (or the whole shorter row) plus 16 bytes
+    // of padding, so that the two quads of a quarter-warp read disjoint banks
+    p.lean_stage = std::min<uint32_t>(D, 128u) + 16u;
+    p.off_stage = (uint32_t)off;
+    off += (size_t)32 * p.lean_stage;
     p.off_pool = (uint32_t)off;
     off += (size_t)p.ef * 8;
     off = (off + 15) & ~(size_t)15;

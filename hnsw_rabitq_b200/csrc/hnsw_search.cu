@@ -495,7 +495,7 @@ __device__ __forceinline__ void batch_dist_lowp(const SearchParams& p, const War
         acc += __shfl_xor_sync(FULL, acc, 1);
         acc += __shfl_xor_sync(FULL, acc, 2);
         float r = acc;
-        if (SPACE != 0) r = 1.0f - (PREC == 2 ? sc * acc : acc);
+        if (SPACE != 0) r = __fsub_rn(1.0f, PREC == 2 ? __fmul_rn(sc, acc) : acc);
         const int t = lane - s0 - g;
         const float got = __shfl_sync(FULL, r, (t & 7) << 2);
         if (t >= 0 && t < 8 && t + g < n) dc = got;
@@ -582,7 +582,21 @@ __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem&
 struct TermState {
     uint32_t last_change = 0;  // expansion count when the top-k last changed
     uint32_t nckpt = 0;        // checkpoints taken
+    uint32_t next = 0;         // expansion count at which the next checkpoint falls due
 };
+
+// A checkpoint falls due every term_period expansions; it is taken (trace
+// mode records it, learned mode consults the network) at the first
+// expansion from then on where no unexpanded candidate is closer than the
+// current k-th result -- the only states in which stopping can keep the
+// top-k.  Advances the due count once taken.
+__device__ __forceinline__ bool term_due(const SearchParams& p, const WarpSmem& s, uint32_t e, int psize,
+                                         uint32_t next_dk, TermState& ts) {
+    if (ts.next == 0) ts.next = p.term_period;
+    if (e < ts.next || psize < (int)p.k || !(next_dk > khi(s.pool[p.k - 1]))) return false;
+    while (ts.next <= e) ts.next += p.term_period;
+    return true;
+}
 
 // Checkpoint after `e` level-0 expansions, with a next candidate of distance
 // key `next_dk` waiting: trace mode records the features and the top-k ids;
@@ -853,7 +867,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             }
             break;
         }
-        if (TERM && have_next && ct.l0_exp % p.term_period == 0 &&
+        if (TERM && have_next && term_due(p, s, ct.l0_exp, psize, next_dk, ts) &&
             term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d0, qn, ts)) {
             // confident that the top-k is final: drain the prefetched
             // expansion and stop
@@ -947,7 +961,7 @@ __device__ bool rerank_fp32(const SearchParams& p, WarpSmem& s, uint32_t& phase,
     for (int r = lane; r < R; r += 32) {
         const uint64_t kr = s.pool[r];
         int rank = 0;
-        for (int t = 0; t < R; t++) rank += s.pool[t] < kr;
+        for (int t = 0; t < R; t++) rank += s.pool[t] < kr || (s.pool[t] == kr && t < r);
         if (DBG_OK(rank < R && reinterpret_cast<unsigned char*>(tmp + rank + 1) <= reinterpret_cast<unsigned char*>(s.pool),
                    60, rank, R))
             tmp[rank] = kr;
@@ -1128,7 +1142,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         bool from_extra = kx < kp;
         if (from_extra && psize == (int)ef && khi(kx) > khi(s.pool[psize - 1])) break;
         uint64_t ck = from_extra ? kx : kp;
-        if (TERM && ct.l0_exp > 0 && ct.l0_exp % p.term_period == 0 &&
+        if (TERM && ct.l0_exp > 0 && term_due(p, s, ct.l0_exp, psize, khi(ck), ts) &&
             term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, khi(ck), curd, qn, ts))
             break;
         __syncwarp();

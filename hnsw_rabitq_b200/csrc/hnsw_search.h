@@ -134,7 +134,7 @@ struct SearchParams {
     // lean fp8 beam (hnsw_lean.cu): id tie order, no filter or deletions;
     // `lean_w` link rows expanded per iteration (64 link slots per pass)
     uint32_t lean, lean_w;
-    uint32_t off_q8, off_cid, off_lacc;
+    uint32_t off_q8, off_cid, off_lacc, lean_stage;
     // per-warp shared memory layout
     uint32_t stage_slots, stage_stride, extra_cap, log2_vis;
     uint32_t off_query, off_stage, off_pool, off_extra, off_vis, off_top, off_cand, off_acc, off_ev, warp_smem;

@@ -325,12 +325,12 @@ def test_filters_evaluated_per_call_and_registered():
     q = g["hnsw_l2_d16/queries"]
     idx = gpu_index(f"{GOLDEN}/hnsw_l2_d16.bin", "l2", 16)
     idx.set_ef(32)
-    state = {"mod": 2}
-    flt = lambda l: l % state["mod"] == 0
+    state = {"mod": 2, "rem": 0}
+    flt = lambda l: l % state["mod"] == state["rem"]
     l2, d2 = idx.knn_query(q, k=10, filter=flt)
-    state["mod"] = 3
+    state["mod"], state["rem"] = 4, 1
     l3, d3 = idx.knn_query(q, k=10, filter=flt)
-    assert np.all(l2 % 2 == 0) and np.all(l3 % 3 == 0)
+    assert np.all(l2 % 2 == 0) and np.all(l3 % 4 == 1)
     assert np.array_equal(l2, g["hnsw_l2_d16/ef32_k10_even/labels"])
     reg = idx.register_filter(lambda l: l % 2 == 0)
     lr, dr = idx.knn_query(q, k=10, filter=reg)

@@ -87,10 +87,10 @@ def test_checkpoint_trace_is_the_search(gmm_index):
     pl, pd, pc, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id")
     ck = g.search_checkpoints(q, k, ef=ef, period=period, max_ckpt=400)
     assert np.array_equal(ck["labels"], pl) and np.array_equal(ck["dists"].view(np.uint32), pd.view(np.uint32))
-    # a checkpoint after every `period`-th expansion that has a successor,
-    # then the final state
+    # checkpoints fall due every `period` expansions and are taken where no
+    # unexpanded candidate is closer than the k-th result, then the final state
     n = ck["nckpt"].astype(np.int64) - 1
-    assert np.all(n <= pt[:, 2] // period) and np.all(n >= (pt[:, 2] - 1) // period)
+    assert np.all(n <= pt[:, 2] // period) and np.all(n >= 1)
     lab_of = g.labels_by_internal_id()
     final = ck["ids"][np.arange(300), n]
     assert np.array_equal(lab_of[final], pl)
@@ -100,9 +100,13 @@ def test_checkpoint_trace_is_the_search(gmm_index):
     assert np.all(small["nckpt"] == np.minimum(ck["nckpt"], 3))
     assert np.array_equal(small["ids"][np.arange(300), small["nckpt"].astype(np.int64) - 1], final)
     for i in range(0, 300, 15):
+        e_prev = 0
         for r in range(int(n[i])):
             f = ck["feat"][i, r]
-            assert abs(f[0] - np.log2(1 + period * (r + 1))) < 1e-5
+            e = int(round(2.0 ** f[0] - 1))
+            assert e >= period * (r + 1) and e > e_prev and abs(f[0] - np.log2(1 + e)) < 1e-5
+            e_prev = e
+            assert f[2] > 0  # taken only when the next candidate is farther than the k-th result
             ids = ck["ids"][i, r]
             assert np.all(ids != 0xffffffff)
             d = O.distances("l2", q[i], x[lab_of[ids].astype(np.int64)])
@@ -123,10 +127,11 @@ def test_stop_rule_bounds(gmm_index):
         g.set_termination_model(learned.TerminationModel(p, period, never))
         ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
         assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
+    # -inf stops at the first checkpoint taken
     g.set_termination_model(learned.TerminationModel(p, period, -float("inf")))
     ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
-    assert np.all(lt[:, 2] <= period) and np.all(lc == k)
-    assert np.all(np.diff(ld, axis=1) >= 0)
+    assert np.all(lt[:, 2] <= pt[:, 2]) and np.all(lt[:, 2] >= period) and lt[:, 2].mean() < pt[:, 2].mean()
+    assert np.all(lc == k) and np.all(np.diff(ld, axis=1) >= 0)
     g.set_termination_model(None)
     with pytest.raises(RuntimeError, match="no termination model"):
         g.knn_query_traced(q, k, ef=ef, tie_order="id", learned=True)
@@ -176,11 +181,13 @@ def test_learned_beats_fixed_ef_at_equal_recall(hetero_index, precision):
 
 def test_fit_fp8_labels_use_the_beam_state(gmm_index):
     """A low-precision beam is labelled against its own final top-k (before
-    the re-rank): the positive share stays far from zero."""
+    the re-rank): the positive share stays far from zero (checkpoints are
+    taken only where no unexpanded candidate is closer than the k-th result,
+    so most of them are positive)."""
     g, x, q = gmm_index
     model, rep = learned.fit(g, q[:600], k=10, ef_cap=64, period=4, target_recall=0.9, precision="fp8",
                              epochs=5, seed=1, caps=[48, 64])
-    assert 0.2 < rep["positive"] < 0.95, rep["positive"]
+    assert 0.2 < rep["positive"] < 1.0, rep["positive"]
     assert model.precision == "fp8" and model.ef_cap in (48, 64)
 
 
@@ -222,7 +229,7 @@ def test_learned_stop_general_path(tmp_path, dim):
     assert all(flt(int(v)) and int(v) % 37 for row in ll for v in row)
     g.set_termination_model(learned.TerminationModel(p, period, -float("inf")))
     ll, ld, lc, lt = g.knn_query_traced(q, k, filter=flt, ef=ef, tie_order="id", learned=True)
-    assert np.all(lt[:, 2] <= period)
+    assert np.all(lt[:, 2] <= pt[:, 2]) and lt[:, 2].mean() < pt[:, 2].mean()
     assert all(flt(int(v)) and int(v) % 37 for i in range(300) for v in ll[i, :lc[i]])
 
 
