@@ -417,9 +417,8 @@ def run_ours(args, dist: Dist):
         from hnsw_rabitq_b200.datasets import gmm_1m_128_queries
         tq = gmm_1m_128_queries(args.train_queries, stream_seed=1000)
         tgt = idx.knn_query_exact(tq, 10)[0]
-        ck = idx.search_checkpoints(tq, 10, ef=args.term_cap, period=args.term_period,
-                                    max_ckpt=max(16, 8 * args.term_cap // args.term_period), precision="fp8",
-                                    rerank=args.rerank)
+        ck = learned.traces(idx, tq, 10, args.term_cap, args.term_period,
+                            max(16, 8 * args.term_cap // args.term_period), "fp8", args.rerank)
         params, _ = learned.train(*learned.checkpoint_dataset(idx, ck, tgt), epochs=20, seed=0)
         idx.set_termination_model(learned.TerminationModel(params, args.term_period, args.profile_learned,
                                                            args.term_cap, "fp8", args.rerank))

@@ -22,9 +22,9 @@ EXACT_TIES = 0x4
 LEARNED_STOP = 0x8
 EXACT_SCAN = 0x10
 REPLAY_ALL = 0x20
-TERM_FEATURES = 6
+TERM_FEATURES = 16
 TERM_HIDDEN = 64
-TERM_PARAMS = 4685
+TERM_PARAMS = 5345
 PREC_FP32, PREC_BF16, PREC_FP8 = 0, 1, 2
 STATUS_TIMEOUT = 0x1
 STATUS_OVERFLOW = 0x2
@@ -87,7 +87,8 @@ SIGNATURES = {
     "hnswgpu_selftest_wait_timeout": (C.c_int, [C.c_int, C.POINTER(U32)]),
     "hnswgpu_search_epsilon": (C.c_int, [P, P, U64, C.c_float, U64, U64, C.POINTER(SearchOpts), P, P, P]),
     "hnswgpu_set_termination_model": (C.c_int, [P, P, U32, C.c_float]),
-    "hnswgpu_search_checkpoints": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), U32, U32, P, P, P, P, P, P]),
+    "hnswgpu_search_checkpoints": (C.c_int, [P, P, U64, U64, C.POINTER(SearchOpts), U32, U32, U32, P, P, P, P, P, P,
+                                             P]),
     "hnswgpu_term_train": (C.c_int, [C.c_int, P, P, U64, C.POINTER(TermTrainOpts), P, P]),
     "hnswgpu_term_loss_grad": (C.c_int, [C.c_int, P, P, P, U64, C.c_float, P, P]),
     "hnswgpu_term_logits": (C.c_int, [C.c_int, P, P, U64, P]),

@@ -319,29 +319,83 @@ __device__ __forceinline__ int lean_merge(uint64_t* pool, int& size, int cap, un
     return mpos;
 }
 
+// Link slots of an iteration: slot j = lane (id0) and lane + 32 (id1) is
+// entry j % maxM0 of the level-0 row of candidate j / maxM0 (c0, c1), for
+// the sel candidates taken; INVALID_ID elsewhere.
+__device__ __forceinline__ void lean_links(const SearchParams& p, int maxM0, int sel, uint32_t c0, uint32_t c1,
+                                           int lane, uint32_t& id0, uint32_t& id1) {
+    id0 = INVALID_ID;
+    id1 = INVALID_ID;
+    const int j0 = lane, ci0 = j0 >= maxM0 ? 1 : 0;
+    if (ci0 < sel && LCHK((ci0 ? c1 : c0) < p.count, 210, ci0 ? c1 : c0, sel) &&
+        LCHK(j0 - ci0 * maxM0 < maxM0, 211, j0, ci0))
+        id0 = __ldg(p.links0 + (size_t)(ci0 ? c1 : c0) * maxM0 + (j0 - ci0 * maxM0));
+    const int j1 = lane + 32, ci1 = j1 >= maxM0 ? (j1 >= 2 * maxM0 ? 2 : 1) : 0;
+    if (ci1 < sel && LCHK((ci1 ? c1 : c0) < p.count, 212, ci1 ? c1 : c0, sel) &&
+        LCHK(j1 - ci1 * maxM0 < maxM0 && j1 - ci1 * maxM0 >= 0, 213, j1, ci1))
+        id1 = __ldg(p.links0 + (size_t)(ci1 ? c1 : c0) * maxM0 + (j1 - ci1 * maxM0));
+}
+
 struct LeanTerm {
     uint32_t last_change = 0;  // expansions when the top-k last changed
+    uint32_t nchange = 0;      // expansions (iterations) that changed the top-k
     uint32_t nckpt = 0;        // checkpoints taken
     uint32_t next = 0;         // expansion count of the next checkpoint
+    uint32_t prev_e = 0, prev_d = 0;  // expansions and distance evaluations at the previous checkpoint
 };
 
+__device__ __forceinline__ TermInputs lean_term_inputs(const SearchParams& p, float e, float d1, float dk, float dn,
+                                                       float d_entry, float qn, uint32_t dists, const LeanTerm& ts) {
+    TermInputs in;
+    in.e = e;
+    in.d1 = d1;
+    in.dk = dk;
+    in.dn = dn;
+    in.d_entry = d_entry;
+    in.qn = qn;
+    in.since_change = e - (float)ts.last_change;
+    in.inv_period = 1.0f / (float)p.term_period;
+    in.nchange = (float)ts.nchange;
+    in.eval_rate = (float)(dists - ts.prev_d) / fmaxf(e - (float)ts.prev_e, 1.0f);
+    return in;
+}
+
+// Trace mode: the ids of the first ckpt_width beam entries of a checkpoint
+// row, and (when asked for) their float32 distances.
+template <int SPACE>
+__device__ __forceinline__ void lean_record_ids(const SearchParams& p, const LeanSmem& s, int lane, size_t row,
+                                                int psize) {
+    const int w = (int)p.ckpt_width;
+    for (int i = lane; i < w; i += 32) p.ckpt_ids[row * w + i] = i < psize ? kid(s.pool[i]) : INVALID_ID;
+    if (p.ckpt_dists) {
+        float* out = p.ckpt_dists + row * w;
+        for (int i = psize + lane; i < w; i += 32) out[i] = __int_as_float(0x7f800000);
+        trace_dists<SPACE>(p, s.q, s.pool, min(w, psize), lane, out);
+    }
+}
+
 // Checkpoint of the learned termination (trace mode 1 records it, mode 2
-// asks the network whether to stop), with the general beam's features.
-template <int TERM>
-__device__ __forceinline__ bool lean_checkpoint(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
-                                                uint32_t e, int psize, uint32_t next_dk, float d_entry, float qn,
-                                                LeanTerm& ts) {
+// asks the network whether to stop), with the general beam's features.  Not
+// inlined: it runs every few expansions, and the features and the network
+// would otherwise raise the register need of the whole beam loop.
+template <int SPACE, int TERM>
+__device__ __noinline__ bool lean_checkpoint(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
+                                                uint32_t e, uint32_t dists, int psize, uint32_t next_dk,
+                                                float d_entry, float qn, LeanTerm& ts) {
     if (psize == 0) return false;
     const int kq = (int)p.k;
     const int kk = min(kq, psize);
     float fe[kTermFeatures];
-    term_features((float)e, funkey(khi(s.pool[0])), funkey(khi(s.pool[kk - 1])), funkey(next_dk), d_entry, qn,
-                  (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    const TermInputs in = lean_term_inputs(p, (float)e, funkey(khi(s.pool[0])), funkey(khi(s.pool[kk - 1])),
+                                           funkey(next_dk), d_entry, qn, dists, ts);
+    term_features(in, s.pool, psize, (int)p.ef, lane, fe);
+    ts.prev_e = e;
+    ts.prev_d = dists;
     if (TERM == 1) {
         if (ts.nckpt + 1 < p.term_max_ckpt) {
             const size_t row = (size_t)qi * p.term_max_ckpt + ts.nckpt;
             if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-            for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+            lean_record_ids<SPACE>(p, s, lane, row, psize);
         }
         ts.nckpt++;
         return false;
@@ -349,8 +403,10 @@ __device__ __forceinline__ bool lean_checkpoint(const SearchParams& p, const Lea
     return term_logit(p.term_model, fe, lane) > p.term_logit;
 }
 
+template <int SPACE>
 __device__ __forceinline__ void lean_final_row(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
-                                               uint32_t e, int psize, float d_entry, float qn, const LeanTerm& ts) {
+                                               uint32_t e, uint32_t dists, int psize, float d_entry, float qn,
+                                               const LeanTerm& ts) {
     if (p.term_max_ckpt == 0) {
         if (lane == 0) p.ckpt_count[qi] = 0;
         return;
@@ -362,9 +418,14 @@ __device__ __forceinline__ void lean_final_row(const SearchParams& p, const Lean
     const float d1 = kk > 0 ? funkey(khi(s.pool[0])) : 0.f;
     const float dk = kk > 0 ? funkey(khi(s.pool[kk - 1])) : 0.f;
     float fe[kTermFeatures];
-    term_features((float)e, d1, dk, dk, d_entry, qn, (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    if (psize > 0) {
+        term_features(lean_term_inputs(p, (float)e, d1, dk, dk, d_entry, qn, dists, ts), s.pool, psize, (int)p.ef,
+                      lane, fe);
+    } else {
+        for (int i = 0; i < kTermFeatures; i++) fe[i] = 0.f;
+    }
     if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-    for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+    lean_record_ids<SPACE>(p, s, lane, row, psize);
     if (lane == 0) p.ckpt_count[qi] = r + 1;
 }
 
@@ -570,17 +631,17 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             if (u && __popc(m & lanemask_lt()) < take && LCHK(i < ef && psize <= ef, 230, i, psize))
                 s.pool[i] = e | EXP_BIT;
             const int src0 = __ffs(m) - 1;
-            const uint32_t id0 = __shfl_sync(FULL, kid(e), src0);
+            const uint32_t id0s = __shfl_sync(FULL, kid(e), src0);
             const uint32_t dk0 = __shfl_sync(FULL, khi(e), src0);
             const int src1 = take > 1 ? __ffs(m & (m - 1)) - 1 : src0;
-            const uint32_t id1 = __shfl_sync(FULL, kid(e), src1);
+            const uint32_t id1s = __shfl_sync(FULL, kid(e), src1);
             if (sel == 0) {
-                cand0 = id0;
+                cand0 = id0s;
                 next_dk = dk0;
                 hint = b + src0;
-                if (take > 1) cand1 = id1;
+                if (take > 1) cand1 = id1s;
             } else {
-                cand1 = id0;
+                cand1 = id0s;
             }
             sel += take;
         }
@@ -593,7 +654,8 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         // closer than the current k-th result, the only states in which
         // stopping can keep the top-k
         if (TERM && ct.l0_exp >= ts.next && psize >= kq && next_dk > khi(s.pool[kq - 1])) {
-            const bool stop = lean_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d_entry, lq.qn, ts);
+            const bool stop =
+                lean_checkpoint<SPACE, TERM>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, next_dk, d_entry, lq.qn, ts);
             while (ts.next <= ct.l0_exp) ts.next += p.term_period;
             if (stop) break;
         }
@@ -602,17 +664,8 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         ct.l0_exp += (uint32_t)sel;
 
         // ---- link slots j = lane and lane + 32 (row j / maxM0, entry j % maxM0)
-        uint32_t id0 = INVALID_ID, id1 = INVALID_ID;
-        {
-            const int j0 = lane, ci0 = j0 >= maxM0 ? 1 : 0;
-            if (ci0 < sel && LCHK((ci0 ? cand1 : cand0) < p.count, 210, ci0 ? cand1 : cand0, sel) &&
-                LCHK(j0 - ci0 * maxM0 < maxM0, 211, j0, ci0))
-                id0 = __ldg(p.links0 + (size_t)(ci0 ? cand1 : cand0) * maxM0 + (j0 - ci0 * maxM0));
-            const int j1 = lane + 32, ci1 = j1 >= maxM0 ? (j1 >= 2 * maxM0 ? 2 : 1) : 0;
-            if (ci1 < sel && LCHK((ci1 ? cand1 : cand0) < p.count, 212, ci1 ? cand1 : cand0, sel) &&
-                LCHK(j1 - ci1 * maxM0 < maxM0 && j1 - ci1 * maxM0 >= 0, 213, j1, ci1))
-                id1 = __ldg(p.links0 + (size_t)(ci1 ? cand1 : cand0) * maxM0 + (j1 - ci1 * maxM0));
-        }
+        uint32_t id0, id1;
+        lean_links(p, maxM0, sel, cand0, cand1, lane, id0, id1);
         bool f0 = id0 != INVALID_ID, f1 = id1 != INVALID_ID;
         if (!p.links_unique) {
             const unsigned p0 = __match_any_sync(FULL, id0), p1 = __match_any_sync(FULL, id1);
@@ -638,31 +691,34 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         if (f1 && LCHK(id1 < p.count, 215, id1, lane)) s.cid[n0 + __popc(m1 & lanemask_lt())] = id1;
         __syncwarp();
         LPT(3);
-        if (nnew == 0) continue;
-        ct.l0_dists += (uint32_t)nnew;
 
-        // ---- distances (lane L: candidates L and L + 32)
-        uint32_t cidA, cidB = INVALID_ID;
-        const float dA = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, nnew, lane, cidA);
-        float dB = 0.f;
-        if (nnew > 32) dB = lean_pass<SPACE, NS, MULTI>(p, s, lq, 32, nnew, lane, cidB);
-        LPT(4);
-
-        // ---- acceptance by the beam's bound
-        const bool full = psize == ef;
-        const uint32_t lbk = full ? khi(s.pool[psize - 1]) : 0xffffffffu;
-        const uint32_t dkA = fkey(dA), dkB = fkey(dB);
-        const bool accA = lane < nnew && (!full || dkA < lbk);
-        const bool accB = lane + 32 < nnew && (!full || dkB < lbk);
+        bool accA = false, accB = false;
+        uint64_t kA = ~0ull, kB = ~0ull;
+        if (nnew > 0) {
+            ct.l0_dists += (uint32_t)nnew;
+            // ---- distances (lane L: candidates L and L + 32)
+            uint32_t cidA, cidB = INVALID_ID;
+            const float dA = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, nnew, lane, cidA);
+            float dB = 0.f;
+            if (nnew > 32) dB = lean_pass<SPACE, NS, MULTI>(p, s, lq, 32, nnew, lane, cidB);
+            LPT(4);
+            // ---- acceptance by the beam's bound
+            const bool full = psize == ef;
+            const uint32_t lbk = full ? khi(s.pool[psize - 1]) : 0xffffffffu;
+            const uint32_t dkA = fkey(dA), dkB = fkey(dB);
+            accA = lane < nnew && (!full || dkA < lbk);
+            accB = lane + 32 < nnew && (!full || dkB < lbk);
+            if (accA) kA = ((uint64_t)dkA << 32) | cidA;
+            if (accB) kB = ((uint64_t)dkB << 32) | cidB;
+        }
         const unsigned am0 = __ballot_sync(FULL, accA), am1 = __ballot_sync(FULL, accB);
         const int na0 = __popc(am0);
         const int na = na0 + __popc(am1);
-        if (na == 0) continue;
-        __syncwarp();
-        if (accA) s.lacc[__popc(am0 & lanemask_lt())] = ((uint64_t)dkA << 32) | cidA;
-        if (accB) s.lacc[na0 + __popc(am1 & lanemask_lt())] = ((uint64_t)dkB << 32) | cidB;
-        __syncwarp();
         LPT(5);
+        if (na == 0) continue;
+        if (accA) s.lacc[__popc(am0 & lanemask_lt())] = kA;
+        if (accB) s.lacc[na0 + __popc(am1 & lanemask_lt())] = kB;
+        __syncwarp();
         // ---- merge into the pool (at most 32 keys per round)
         bool top = false;
         for (int b0 = 0; b0 < na; b0 += 32) {
@@ -686,10 +742,13 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             hint = min(hint, lean_merge(s.pool, psize, ef, amask, key, pos, lane, kq, t2));
             top |= t2;
         }
-        if (TERM && top) ts.last_change = ct.l0_exp;
+        if (TERM && top) {
+            ts.last_change = ct.l0_exp;
+            ts.nchange++;
+        }
         LPT(6);
     }
-    if (TERM == 1) lean_final_row(p, s, lane, qi, ct.l0_exp, psize, d_entry, lq.qn, ts);
+    if (TERM == 1) lean_final_row<SPACE>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, d_entry, lq.qn, ts);
 
     // ---- exact re-rank, then the k best ordered by (distance, label)
     lean_rerank<SPACE>(p, s, lane, psize);

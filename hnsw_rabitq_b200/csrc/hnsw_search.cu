@@ -581,8 +581,10 @@ __device__ __forceinline__ bool fetch_distances(const SearchParams& p, WarpSmem&
 // ---- learned early termination (see term_mlp.cuh)
 struct TermState {
     uint32_t last_change = 0;  // expansion count when the top-k last changed
+    uint32_t nchange = 0;      // expansions that changed the top-k
     uint32_t nckpt = 0;        // checkpoints taken
     uint32_t next = 0;         // expansion count at which the next checkpoint falls due
+    uint32_t prev_e = 0, prev_d = 0;  // expansions and distance evaluations at the previous checkpoint
 };
 
 // A checkpoint falls due every term_period expansions; it is taken (trace
@@ -598,24 +600,58 @@ __device__ __forceinline__ bool term_due(const SearchParams& p, const WarpSmem& 
     return true;
 }
 
-// Checkpoint after `e` level-0 expansions, with a next candidate of distance
-// key `next_dk` waiting: trace mode records the features and the top-k ids;
-// learned mode returns true when the network says stop.
-template <int TERM>
+__device__ __forceinline__ TermInputs term_inputs(const SearchParams& p, float e, float d1, float dk, float dn,
+                                                  float d_entry, float qn, uint32_t dists, const TermState& ts) {
+    TermInputs in;
+    in.e = e;
+    in.d1 = d1;
+    in.dk = dk;
+    in.dn = dn;
+    in.d_entry = d_entry;
+    in.qn = qn;
+    in.since_change = e - (float)ts.last_change;
+    in.inv_period = 1.0f / (float)p.term_period;
+    in.nchange = (float)ts.nchange;
+    in.eval_rate = (float)(dists - ts.prev_d) / fmaxf(e - (float)ts.prev_e, 1.0f);
+    return in;
+}
+
+// Trace mode: the ids of the first ckpt_width beam entries of a checkpoint
+// row, and (when asked for) their float32 distances.
+template <int SPACE>
+__device__ __forceinline__ void term_record_ids(const SearchParams& p, const WarpSmem& s, int lane, size_t row,
+                                                int psize) {
+    const int w = (int)p.ckpt_width;
+    for (int i = lane; i < w; i += 32) p.ckpt_ids[row * w + i] = i < psize ? kid(s.pool[i]) : INVALID_ID;
+    if (p.ckpt_dists) {
+        float* out = p.ckpt_dists + row * w;
+        for (int i = psize + lane; i < w; i += 32) out[i] = __int_as_float(0x7f800000);
+        trace_dists<SPACE>(p, s.q, s.pool, min(w, psize), lane, out);
+    }
+}
+
+// Checkpoint after `e` level-0 expansions (`dists` distance evaluations),
+// with a next candidate of distance key `next_dk` waiting: trace mode records
+// the features and the first beam ids; learned mode returns true when the
+// network says stop.
+template <int SPACE, int TERM>
 __device__ __forceinline__ bool term_checkpoint(const SearchParams& p, const WarpSmem& s, int lane, uint32_t qi,
-                                                uint32_t e, int psize, uint32_t next_dk, float d_entry, float qn,
-                                                TermState& ts) {
+                                                uint32_t e, uint32_t dists, int psize, uint32_t next_dk,
+                                                float d_entry, float qn, TermState& ts) {
     if (psize == 0) return false;  // nothing admissible found yet
     const int kq = (int)p.k;
     const int kk = min(kq, psize);
     float fe[kTermFeatures];
-    term_features((float)e, funkey(khi(s.pool[0])), funkey(khi(s.pool[kk - 1])), funkey(next_dk), d_entry, qn,
-                  (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    term_features(term_inputs(p, (float)e, funkey(khi(s.pool[0])), funkey(khi(s.pool[kk - 1])), funkey(next_dk),
+                              d_entry, qn, dists, ts),
+                  s.pool, psize, (int)p.ef, lane, fe);
+    ts.prev_e = e;
+    ts.prev_d = dists;
     if (TERM == 1) {
         if (ts.nckpt + 1 < p.term_max_ckpt) {  // the last row is kept for the final state
             const size_t row = (size_t)qi * p.term_max_ckpt + ts.nckpt;
             if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-            for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+            term_record_ids<SPACE>(p, s, lane, row, psize);
         }
         ts.nckpt++;
         return false;
@@ -623,10 +659,13 @@ __device__ __forceinline__ bool term_checkpoint(const SearchParams& p, const War
     return term_logit(p.term_model, fe, lane) > p.term_logit;
 }
 
-// Trace mode, end of the beam: the final row holds its top-k (before any
-// re-rank) and the features of that state; labels of earlier rows refer to it.
+// Trace mode, end of the beam: the final row holds its first beam ids
+// (before any re-rank) and the features of that state; labels of earlier
+// rows refer to it.
+template <int SPACE>
 __device__ __forceinline__ void term_final_row(const SearchParams& p, const WarpSmem& s, int lane, uint32_t qi,
-                                               uint32_t e, int psize, float d_entry, float qn, const TermState& ts) {
+                                               uint32_t e, uint32_t dists, int psize, float d_entry, float qn,
+                                               const TermState& ts) {
     if (p.term_max_ckpt == 0) {
         if (lane == 0) p.ckpt_count[qi] = 0;
         return;
@@ -638,9 +677,14 @@ __device__ __forceinline__ void term_final_row(const SearchParams& p, const Warp
     const float d1 = kk > 0 ? funkey(khi(s.pool[0])) : 0.f;
     const float dk = kk > 0 ? funkey(khi(s.pool[kk - 1])) : 0.f;
     float fe[kTermFeatures];
-    term_features((float)e, d1, dk, dk, d_entry, qn, (float)(e - ts.last_change), 1.0f / (float)p.term_period, fe);
+    if (psize > 0) {
+        term_features(term_inputs(p, (float)e, d1, dk, dk, d_entry, qn, dists, ts), s.pool, psize, (int)p.ef, lane,
+                      fe);
+    } else {
+        for (int i = 0; i < kTermFeatures; i++) fe[i] = 0.f;
+    }
     if (lane < kTermFeatures) p.ckpt_feat[row * kTermFeatures + lane] = fe[lane];
-    for (int i = lane; i < kq; i += 32) p.ckpt_ids[row * kq + i] = i < kk ? kid(s.pool[i]) : INVALID_ID;
+    term_record_ids<SPACE>(p, s, lane, row, psize);
     if (lane == 0) p.ckpt_count[qi] = r + 1;
 }
 
@@ -714,7 +758,10 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         const bool accept = live && cntP + cntN < ef;
         const unsigned pmask = __ballot_sync(FULL, accept && allowed);
         const unsigned xmask = FILTER ? __ballot_sync(FULL, accept && !allowed) : 0u;
-        if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < kq)) ts.last_change = ct.l0_exp;
+        if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < kq)) {
+            ts.last_change = ct.l0_exp;
+            ts.nchange++;
+        }
         PT_MARK(6);
         // ---- the next candidate
         // smallest accepted key: the smallest distance key, then the smallest
@@ -868,7 +915,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
             break;
         }
         if (TERM && have_next && term_due(p, s, ct.l0_exp, psize, next_dk, ts) &&
-            term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, next_dk, d0, qn, ts)) {
+            term_checkpoint<SPACE, TERM>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, next_dk, d0, qn, ts)) {
             // confident that the top-k is final: drain the prefetched
             // expansion and stop
             if (fn.n0 > 0) {
@@ -919,7 +966,7 @@ __device__ bool base_pipelined(const SearchParams& p, WarpSmem& s, uint32_t& pha
         ct.l0_exp += 1;
         PT_MARK(2);
     }
-    if (TERM == 1) term_final_row(p, s, lane, qi, ct.l0_exp, psize, d0, qn, ts);
+    if (TERM == 1) term_final_row<SPACE>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, d0, qn, ts);
     return true;
 }
 
@@ -1143,7 +1190,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         if (from_extra && psize == (int)ef && khi(kx) > khi(s.pool[psize - 1])) break;
         uint64_t ck = from_extra ? kx : kp;
         if (TERM && ct.l0_exp > 0 && term_due(p, s, ct.l0_exp, psize, khi(ck), ts) &&
-            term_checkpoint<TERM>(p, s, lane, qi, ct.l0_exp, psize, khi(ck), curd, qn, ts))
+            term_checkpoint<SPACE, TERM>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, khi(ck), curd, qn, ts))
             break;
         __syncwarp();
         if (lane == 0) {
@@ -1219,7 +1266,10 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
             }
             bool accept = live && (uint32_t)(cntP + cntN) < ef;
             unsigned pmask = __ballot_sync(FULL, accept && allowed);
-            if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < (int)p.k)) ts.last_change = ct.l0_exp;
+            if (TERM && __any_sync(FULL, accept && allowed && cntP + cntN < (int)p.k)) {
+                ts.last_change = ct.l0_exp;
+                ts.nchange++;
+            }
             unsigned xmask = bare ? 0u : __ballot_sync(FULL, accept && !allowed);
             PT_MARK(6);
             int nev = 0;
@@ -1275,7 +1325,7 @@ __device__ bool search_one(const SearchParams& p, WarpSmem& s, uint32_t& phase, 
         }
     }
     PT_MARK(2);
-    if (TERM == 1) term_final_row(p, s, lane, qi, ct.l0_exp, psize, curd, qn, ts);
+    if (TERM == 1) term_final_row<SPACE>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, curd, qn, ts);
     }  // general loop
 
     const uint32_t k = p.k;

@@ -22,11 +22,11 @@ namespace hnswgpu {
 #endif
 constexpr int kWarpsPerBlock = HNSWGPU_WPB;  // independent query warps per CTA
 // Early-termination network: kTermFeatures -> kTermHidden -> kTermHidden -> 1.
-constexpr int kTermFeatures = 6;
+constexpr int kTermFeatures = 16;
 constexpr int kTermHidden = 64;
 // Packed float32 parameters, in this order:
-//   mu[6], inv_sigma[6] (feature standardisation),
-//   W1[64][6], b1[64], W2[64][64], b2[64], w3[64], b3[1].
+//   mu[16], inv_sigma[16] (feature standardisation),
+//   W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3[1].
 constexpr int kTermOffMu = 0;
 constexpr int kTermOffInvSigma = kTermOffMu + kTermFeatures;
 constexpr int kTermOffW1 = kTermOffInvSigma + kTermFeatures;
@@ -41,15 +41,17 @@ constexpr int kTermParams = kTermOffB3 + 1;
 // fragments each lane reads.  With g = lane / 4 and t = lane % 4, tile v of a
 // layer covers units 8v .. 8v + 7 and lane (g, t) accumulates units 8v + 2t
 // and 8v + 2t + 1 of every tile.  In order:
-//   float mu[6], inv_sigma[6], b3, pad[3]                      (16 floats)
+//   float mu[16], inv_sigma[16], b3, pad[3]                    (kTermPackedHead floats)
 //   float2 b1f[4][8], b2f[4][8]: (b[8v + 2t], b[8v + 2t + 1]) at [t][v]
 //   half2 w3f[4][8]:             (w3[8v + 2t], w3[8v + 2t + 1]) at [t][v]
-//   half2 W1f[32][8]:            (W1[8v + g][2t], W1[8v + g][2t + 1]) at
-//                                [lane][v] (features 6, 7 are zero)
+//   half2 W1f[32][8][2]:         (W1[8v + g][2t + 8h], W1[8v + g][2t + 8h + 1])
+//                                at [lane][v][h]
 //   half2 W2f[32][4][8][2]:      (W2[8v + g][16s + 2t + 8h],
 //                                 W2[8v + g][16s + 2t + 8h + 1]) at [lane][s][v][h]
-constexpr int kTermPackedFloats = 16 + 2 * 4 * 8 * 2;
-constexpr int kTermPackedHalf2 = 4 * 8 + 32 * 8 + 32 * 4 * 8 * 2;
+static_assert(kTermFeatures == 16, "layer 1 is one m16n8k16 k-step: 16 features");
+constexpr int kTermPackedHead = 2 * kTermFeatures + 4;
+constexpr int kTermPackedFloats = kTermPackedHead + 2 * 4 * 8 * 2;
+constexpr int kTermPackedHalf2 = 4 * 8 + 32 * 8 * 2 + 32 * 4 * 8 * 2;
 constexpr size_t kTermPackedBytes = (size_t)kTermPackedFloats * 4 + (size_t)kTermPackedHalf2 * 4;
 // Convert the float32 parameter vector (kTermParams) into the inference form.
 void pack_term_model(const float* params, unsigned char* out);
@@ -119,7 +121,9 @@ struct SearchParams {
     uint32_t term_period;        // expansions between checkpoints (T)
     uint32_t term_max_ckpt;      // checkpoint rows per query (trace mode)
     float* ckpt_feat;            // trace: nq x max_ckpt x kTermFeatures
-    uint32_t* ckpt_ids;          // trace: nq x max_ckpt x k internal ids of the current top-k
+    uint32_t* ckpt_ids;          // trace: nq x max_ckpt x ckpt_width ids of the first beam entries
+    float* ckpt_dists;           // trace (optional): their float32 distances, recomputed from the rows
+    uint32_t ckpt_width;
     uint32_t* ckpt_count;        // trace: checkpoints written per query
     const float* term_model;     // learned: packed network (see term_model_layout)
     float term_logit;            // learned: stop when the network's logit exceeds this

@@ -494,6 +494,8 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
         p.term_max_ckpt = t->max_ckpt;
         p.ckpt_feat = t->feat;
         p.ckpt_ids = t->ids;
+        p.ckpt_dists = t->dists;
+        p.ckpt_width = t->width ? t->width : p.k;
         p.ckpt_count = t->count;
     } else {
         if (!h->term_model.p) throw ApiError(HNSWGPU_ERR_STATE, "no termination model set");
@@ -1445,9 +1447,9 @@ int hnswgpu_set_termination_model(hnswgpu_index* h, const float* params, uint32_
 }
 
 int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t nq, uint64_t k,
-                               const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt, float* out_feat,
-                               uint32_t* out_ids, uint32_t* out_nckpt, uint64_t* out_labels, float* out_dists,
-                               int32_t* out_counts) {
+                               const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt,
+                               uint32_t ids_width, float* out_feat, uint32_t* out_ids, float* out_ckpt_dists,
+                               uint32_t* out_nckpt, uint64_t* out_labels, float* out_dists, int32_t* out_counts) {
     return guarded([&] {
         if (!h || h->is_bf || k == 0 || period == 0)
             return fail(HNSWGPU_ERR_ARG, "invalid argument");
@@ -1455,6 +1457,8 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
                    (max_ckpt && (!out_feat || !out_ids))))
             return fail(HNSWGPU_ERR_ARG, "invalid argument");
         if (nq > 0xffffffffull || k > 0xffffffffull) return fail(HNSWGPU_ERR_ARG, "batch too large");
+        const uint64_t w = ids_width ? ids_width : k;
+        if (w < k || w > 4096) return fail(HNSWGPU_ERR_ARG, "ids_width must be 0 or in [k, 4096]");
         hnswgpu_search_opts o{};
         if (opts) o = *opts;
         if (o.flags & ~(uint32_t)HNSWGPU_TRACE)
@@ -1465,7 +1469,7 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
         const uint64_t ef = o.ef ? o.ef : h->ef;
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : h->stream;
         const size_t rows = (size_t)nq * max_ckpt;
-        DevBuf<float> dq, dd, df;
+        DevBuf<float> dq, dd, df, dx;
         DevBuf<uint64_t> dl;
         DevBuf<int32_t> dc;
         DevBuf<uint32_t> di, dn;
@@ -1475,7 +1479,8 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
         dc.alloc(nq);
         dn.alloc(nq);
         df.alloc(rows * hnswgpu::kTermFeatures);
-        di.alloc(rows * k);
+        di.alloc(rows * w);
+        if (out_ckpt_dists) dx.alloc(rows * w);
         cuda_check(cudaMemcpyAsync(dq.p, queries, nq * h->dim * 4, cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
         TermCfg term;
         term.mode = 1;
@@ -1483,6 +1488,8 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
         term.max_ckpt = max_ckpt;
         term.feat = df.p;
         term.ids = di.p;
+        term.width = (uint32_t)w;
+        term.dists = out_ckpt_dists ? dx.p : nullptr;
         term.count = dn.p;
         run_hnsw(h, dq.p, nq, k, ef, nullptr, dl.p, dd.p, dc.p, nullptr, st, false, o.precision, o.rerank, &term,
                  false);
@@ -1493,7 +1500,10 @@ int hnswgpu_search_checkpoints(hnswgpu_index* h, const float* queries, uint64_t 
         if (rows) {
             cuda_check(cudaMemcpyAsync(out_feat, df.p, rows * hnswgpu::kTermFeatures * 4, cudaMemcpyDeviceToHost, st),
                        "cudaMemcpyAsync");
-            cuda_check(cudaMemcpyAsync(out_ids, di.p, rows * k * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+            cuda_check(cudaMemcpyAsync(out_ids, di.p, rows * w * 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+            if (out_ckpt_dists)
+                cuda_check(cudaMemcpyAsync(out_ckpt_dists, dx.p, rows * w * 4, cudaMemcpyDeviceToHost, st),
+                           "cudaMemcpyAsync");
         }
         uint32_t status = 0;
         cuda_check(cudaMemcpyAsync(&status, h->status.p, 4, cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");

@@ -138,9 +138,10 @@ inline int kspace(const hnswgpu_index* h) {
 // Learned-termination settings of one launch (mode 1: record checkpoints,
 // 2: stop early with the index's network).
 struct TermCfg {
-    uint32_t mode = 0, period = 0, max_ckpt = 0;
+    uint32_t mode = 0, period = 0, max_ckpt = 0, width = 0;
     float* feat = nullptr;
     uint32_t* ids = nullptr;
+    float* dists = nullptr;
     uint32_t* count = nullptr;
 };
 

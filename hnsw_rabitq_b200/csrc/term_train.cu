@@ -40,7 +40,7 @@ void pack_term_model(const float* params, unsigned char* out) {
         f[kTermFeatures + i] = params[kTermOffInvSigma + i];
     }
     f[2 * kTermFeatures] = params[kTermOffB3];
-    float* b1f = f + 16;
+    float* b1f = f + kTermPackedHead;
     float* b2f = b1f + 4 * 8 * 2;
     for (int t = 0; t < 4; t++)
         for (int v = 0; v < 8; v++)
@@ -54,17 +54,18 @@ void pack_term_model(const float* params, unsigned char* out) {
         for (int v = 0; v < 8; v++)
             for (int e = 0; e < 2; e++) h[(t * 8 + v) * 2 + e] = __float2half_rn(params[kTermOffW3 + 8 * v + 2 * t + e]);
     h += 4 * 8 * 2;
-    // W1f[lane][v]
+    // W1f[lane][v][hh]
     for (int lane = 0; lane < 32; lane++) {
         const int g = lane >> 2, t = lane & 3;
         for (int v = 0; v < 8; v++)
-            for (int e = 0; e < 2; e++) {
-                const int feat = 2 * t + e;
-                h[(lane * 8 + v) * 2 + e] =
-                    __float2half_rn(feat < kTermFeatures ? params[kTermOffW1 + (8 * v + g) * kTermFeatures + feat] : 0.f);
-            }
+            for (int hh = 0; hh < 2; hh++)
+                for (int e = 0; e < 2; e++) {
+                    const int feat = 2 * t + 8 * hh + e;
+                    h[((lane * 8 + v) * 2 + hh) * 2 + e] =
+                        __float2half_rn(params[kTermOffW1 + (8 * v + g) * kTermFeatures + feat]);
+                }
     }
-    h += 32 * 8 * 2;
+    h += 32 * 8 * 2 * 2;
     // W2f[lane][s][v][hh]
     for (int lane = 0; lane < 32; lane++) {
         const int g = lane >> 2, t = lane & 3;

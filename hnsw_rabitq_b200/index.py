@@ -432,25 +432,33 @@ class Index(_GpuIndex):
         return _capi.LEARNED_STOP if use else 0
 
     def search_checkpoints(self, data, k: int, ef: int = 0, period: int = 4, max_ckpt: int = 128,
-                           precision: Optional[str] = None, rerank: Optional[int] = None):
-        """The id-tie-order search, recording every `period` level-0
-        expansions the termination features and the internal ids of the
-        current top-k.  Returns a dict with feat [nq, max_ckpt, 6], ids
-        [nq, max_ckpt, k] (uint32, 0xffffffff = none), nckpt [nq], labels,
-        dists, counts."""
+                           precision: Optional[str] = None, rerank: Optional[int] = None,
+                           ids_width: int = 0, dists: bool = False):
+        """The id-tie-order search, recording at every checkpoint (every
+        `period` level-0 expansions, at the first state where no waiting
+        candidate is closer than the k-th result) the termination features
+        and the internal ids of the first `ids_width` (default k) beam
+        entries.  Returns a dict with feat [nq, max_ckpt, TERM_FEATURES], ids
+        [nq, max_ckpt, W] (uint32, 0xffffffff = none), nckpt [nq], labels,
+        dists, counts; with dists=True also ckpt_dists [nq, max_ckpt, W],
+        the float32 distances of those entries (+inf = none)."""
         q, k = self._queries(data, k)
         nq = q.shape[0]
+        w = int(ids_width) or k
         out = dict(feat=np.zeros((nq, max_ckpt, _capi.TERM_FEATURES), np.float32),
-                   ids=np.full((nq, max_ckpt, k), 0xffffffff, np.uint32), nckpt=np.zeros(nq, np.uint32),
+                   ids=np.full((nq, max_ckpt, w), 0xffffffff, np.uint32), nckpt=np.zeros(nq, np.uint32),
                    labels=np.empty((nq, k), np.uint64), dists=np.empty((nq, k), np.float32),
                    counts=np.empty(nq, np.int32))
+        if dists:
+            out["ckpt_dists"] = np.full((nq, max_ckpt, w), np.inf, np.float32)
         opts = _capi.SearchOpts()
         opts.ef = int(ef)
         opts.precision = _PRECISIONS[precision or self.precision]
         opts.rerank = int(self.rerank if rerank is None else rerank)
         _capi.check(_capi.lib().hnswgpu_search_checkpoints(
-            self._h, _ptr(q), nq, k, C.byref(opts), int(period), int(max_ckpt), _ptr(out["feat"]),
-            _ptr(out["ids"]), _ptr(out["nckpt"]), _ptr(out["labels"]), _ptr(out["dists"]), _ptr(out["counts"])))
+            self._h, _ptr(q), nq, k, C.byref(opts), int(period), int(max_ckpt), int(ids_width), _ptr(out["feat"]),
+            _ptr(out["ids"]), _ptr(out["ckpt_dists"]) if dists else None, _ptr(out["nckpt"]), _ptr(out["labels"]),
+            _ptr(out["dists"]), _ptr(out["counts"])))
         return out
 
     def search_epsilon(self, data, epsilon: float, min_candidates: int, max_candidates: int,

@@ -5,12 +5,13 @@ queue is exhausted, so every query pays for the hardest query's ef.  Here a
 small network decides per query when the top-k has stopped changing:
 
 1. ``Index.search_checkpoints`` runs the search (ef = the cap) and records,
-   every `period` level-0 expansions, a 6-feature description of the beam and
-   the current top-k (GPU kernel, the same feature code the search uses);
-2. each checkpoint is labelled 1 when stopping there loses nothing: its top-k
-   already holds as many true neighbours (exact GPU scan) as the beam's final
-   answer;
-3. the 6 -> 64 -> 64 -> 1 network is trained on the GPU (forward / backward /
+   every `period` level-0 expansions, a 16-feature description of the beam
+   and its first entries (GPU kernel, the same feature code the search uses);
+2. each checkpoint is labelled 1 when stopping there loses nothing: the
+   answer it would return (its top-k; for a low-precision beam, the top-k of
+   the float32 re-rank of its first `rerank` entries) already holds as many
+   true neighbours (exact GPU scan) as the beam's final answer;
+3. the 16 -> 64 -> 64 -> 1 network is trained on the GPU (forward / backward /
    Adam kernels of libhnswgpu, float32 master weights);
 4. the stop threshold on the logit is calibrated on held-out queries by
    running the learned search itself (fp16 weights, in-warp inference) and
@@ -91,20 +92,46 @@ def recall(labels: np.ndarray, gt: np.ndarray) -> float:
     return float(_hits(labels[:, :k].astype(np.uint64), gt.astype(np.uint64)).mean() / k)
 
 
+def traces(index, queries: np.ndarray, k: int, ef_cap: int, period: int, max_ckpt: int, precision: str,
+           rerank: int = 0) -> dict:
+    """Checkpoint traces of the search at ef = ef_cap.  A low-precision beam
+    records its first R entries (R = the re-rank count the search uses: the
+    whole beam when rerank is 0) with their float32 distances, so that
+    checkpoint_answers sees what its re-rank would return."""
+    if precision == "fp32":
+        return index.search_checkpoints(queries, k, ef=ef_cap, period=period, max_ckpt=max_ckpt,
+                                        precision=precision, rerank=rerank)
+    width = max(k, min(int(rerank), ef_cap) if rerank else ef_cap)
+    return index.search_checkpoints(queries, k, ef=ef_cap, period=period, max_ckpt=max_ckpt, precision=precision,
+                                    rerank=rerank, ids_width=width, dists=True)
+
+
+def checkpoint_answers(ck: dict, k: int) -> np.ndarray:
+    """Internal ids [nq, R, k] each checkpoint row would return: the first k
+    beam entries, or with recorded float32 distances (a low-precision beam)
+    the k closest of the recorded entries (equal distances by beam position,
+    as the re-rank orders them)."""
+    ids = ck["ids"]
+    if "ckpt_dists" not in ck or ids.shape[2] == k:
+        return ids[:, :, :k]
+    order = np.argsort(ck["ckpt_dists"], axis=2, kind="stable")[:, :, :k]
+    return np.take_along_axis(ids, order, axis=2)
+
+
 def checkpoint_dataset(index, ck: dict, gt: np.ndarray):
-    """(features [n, 6], labels [n]) of every recorded checkpoint: label 1 when
-    the checkpoint's top-k holds at least as many true neighbours as the
-    beam's final top-k (the last row of each query, itself not a sample).
-    Both are taken before any re-rank, so low-precision searches compare
-    like with like."""
-    nq, R, k = ck["ids"].shape
+    """(features [n, TERM_FEATURES], labels [n]) of every recorded
+    checkpoint: label 1 when the answer the checkpoint would return
+    (checkpoint_answers) holds at least as many true neighbours as the beam's
+    final answer (the last row of each query, itself not a sample)."""
+    nq, R, _ = ck["ids"].shape
+    k = gt.shape[1]
     lab_of = index.labels_by_internal_id()
     gt = gt.astype(np.uint64)
     n = ck["nckpt"].astype(np.int64)
     X, Y = [], []
     for a in range(0, nq, 512):
         b = min(nq, a + 512)
-        ids = ck["ids"][a:b]
+        ids = checkpoint_answers({key: v[a:b] for key, v in ck.items() if key in ("ids", "ckpt_dists")}, k)
         lab = np.where(ids == _NONE, np.uint64(2**64 - 1), lab_of[np.minimum(ids, len(lab_of) - 1)])
         hits = _hits(lab, gt[a:b, None, :])                         # [q, R]
         last = np.maximum(n[a:b] - 1, 0)
@@ -228,8 +255,7 @@ def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int =
     hold, tr = perm[:nh], perm[nh:]
     if max_ckpt is None:
         max_ckpt = max(16, (8 * ef_cap) // period)
-    ck = index.search_checkpoints(queries[tr], k, ef=ef_cap, period=period, max_ckpt=max_ckpt, precision=precision,
-                                  rerank=rerank)
+    ck = traces(index, queries[tr], k, ef_cap, period, max_ckpt, precision, rerank)
     X, y = checkpoint_dataset(index, ck, gt[tr])
     params, losses = train(X, y, epochs=epochs, seed=seed, device=device)
     model = TerminationModel(params, period, float("inf"), ef_cap, precision, int(rerank))

@@ -335,18 +335,30 @@ HNSWGPU_API int hnswgpu_fp64_distances(hnswgpu_index* index, const float* querie
  * No counterpart in the reference, whose beam always runs until its
  * candidate queue is exhausted (hnswlib/hnswalg.h:368-376).
  *
- * Every `period` level-0 expansions the beam forms a feature vector of its
- * state (log2(1 + expansions); d_1 / |d_k|; (d_next - d_k) / |d_k|;
- * log2(1 + d_entry / |d_k|); log2(1 + |q|^2); expansions since the top-k
- * last changed / period; d_1, d_k = best and k-th distances in the beam,
- * d_next = the candidate expanded next, d_entry = the level-0 entry point).
- * A 6 -> 64 -> 64 -> 1 ReLU network maps it to the logit of "the top-k is
+ * Every `period` level-0 expansions (at the first state from then on where
+ * no waiting candidate is closer than the k-th result) the beam forms a
+ * feature vector of its state, with a = |d_k|:
+ *   f0 log2(1 + expansions)            f8..f10 log2(1 + n(x)), x = 0.1, 0.25, 0.5
+ *   f1 d_1 / a                         f11 waiting candidates / ef
+ *   f2 (d_next - d_k) / a              f12 beam size / ef
+ *   f3 log2(1 + d_entry / a)           f13 log2(1 + expansions that changed the top-k)
+ *   f4 log2(1 + |q|^2)                 f14 distance evaluations per expansion
+ *   f5 expansions since the top-k          since the previous checkpoint
+ *      last changed / period           f15 (d_median - d_k) / a
+ *   f6 (d_wait - d_k) / a
+ *   f7 (d_worst - d_k) / a
+ * d_1, d_k = best and k-th distances in the beam, d_next = the candidate
+ * expanded next, d_entry = the level-0 entry point, waiting candidates =
+ * beam entries not expanded yet (d_wait the closest of them after those
+ * taken for expansion; n(x) how many are closer than d_k + x a), d_worst /
+ * d_median = the beam's last and middle entries; ratios clamped to [-4, 4].
+ * A 16 -> 64 -> 64 -> 1 ReLU network maps it to the logit of "the top-k is
  * final".  Parameters: HNSWGPU_TERM_PARAMS float32 in the order
- * mu[6], inv_sigma[6] (x = (f - mu) * inv_sigma), W1[64][6], b1[64],
+ * mu[16], inv_sigma[16] (x = (f - mu) * inv_sigma), W1[64][16], b1[64],
  * W2[64][64], b2[64], w3[64], b3. */
-#define HNSWGPU_TERM_FEATURES 6
+#define HNSWGPU_TERM_FEATURES 16
 #define HNSWGPU_TERM_HIDDEN 64
-#define HNSWGPU_TERM_PARAMS 4685
+#define HNSWGPU_TERM_PARAMS 5345
 
 /* Install (params != NULL) or remove (NULL) the index's termination network;
  * HNSWGPU_LEARNED_STOP searches evaluate it every `period` expansions and
@@ -357,18 +369,23 @@ HNSWGPU_API int hnswgpu_set_termination_model(hnswgpu_index* index, const float*
                                               float logit_threshold);
 
 /* Training data: the same search as hnswgpu_search (host pointers, id tie
- * order, opts->precision / rerank / ef honoured) that also records, every
- * `period` expansions, the feature vector (out_feat: nq x max_ckpt x 6) and
- * the internal ids of the current top-k (out_ids: nq x max_ckpt x k,
- * 0xffffffff where the beam holds fewer); out_nckpt[i] = rows written for
+ * order, opts->precision / rerank / ef honoured) that also records, at every
+ * checkpoint, the feature vector (out_feat: nq x max_ckpt x
+ * HNSWGPU_TERM_FEATURES) and the internal ids of the first W beam entries
+ * (out_ids: nq x max_ckpt x W, W = ids_width, or k when 0; 0xffffffff
+ * where the beam holds fewer); out_ckpt_dists (optional, same shape): their
+ * float32 distances recomputed from the float32 rows (+inf for missing
+ * entries), so that a low-precision beam can be labelled by what its
+ * re-rank of those W entries would return.  out_nckpt[i] = rows written for
  * query i (1..max_ckpt when max_ckpt > 0).  The last row of each query
- * (out_nckpt[i] - 1) holds the state at the end of the beam: its top-k
- * before any re-rank, the reference for labelling the earlier rows;
+ * (out_nckpt[i] - 1) holds the state at the end of the beam (its first W
+ * entries before any re-rank), the reference for labelling the earlier rows;
  * checkpoints beyond max_ckpt - 1 are dropped. */
 HNSWGPU_API int hnswgpu_search_checkpoints(hnswgpu_index* index, const float* queries, uint64_t nq, uint64_t k,
                                            const hnswgpu_search_opts* opts, uint32_t period, uint32_t max_ckpt,
-                                           float* out_feat, uint32_t* out_ids, uint32_t* out_nckpt,
-                                           uint64_t* out_labels, float* out_dists, int32_t* out_counts);
+                                           uint32_t ids_width, float* out_feat, uint32_t* out_ids,
+                                           float* out_ckpt_dists, uint32_t* out_nckpt, uint64_t* out_labels,
+                                           float* out_dists, int32_t* out_counts);
 
 typedef struct hnswgpu_term_train_opts {
     uint32_t epochs;

@@ -8,14 +8,14 @@ tests import this module, to check the GPU's gradients and logits.  The
 reference (hnswlib) has no such network, so there is nothing in it to pin
 against; the gradient itself is pinned by a finite-difference test.
 
-Parameter vector (float32 on the GPU, HNSWGPU_TERM_PARAMS = 4685 entries):
-mu[6], inv_sigma[6], W1[64][6], b1[64], W2[64][64], b2[64], w3[64], b3.
+Parameter vector (float32 on the GPU, HNSWGPU_TERM_PARAMS = 5345 entries):
+mu[16], inv_sigma[16], W1[64][16], b1[64], W2[64][64], b2[64], w3[64], b3.
 """
 from __future__ import annotations
 
 import numpy as np
 
-F, H = 6, 64
+F, H = 16, 64
 OFF_MU = 0
 OFF_INV_SIGMA = OFF_MU + F
 OFF_W1 = OFF_INV_SIGMA + F
@@ -44,7 +44,7 @@ def _f16(a):
 
 
 def forward(params, feats, fp16_weights: bool = False, fp16_activations: bool = False):
-    """Logits (float64) of feature rows [n, 6].  fp16_weights: round W1, W2,
+    """Logits (float64) of feature rows [n, 16].  fp16_weights: round W1, W2,
     w3 to fp16 first; fp16_activations: also round the standardised features
     (in float32 arithmetic) and the first hidden layer to fp16 -- the
     operands of the search's tensor-core inference form."""

@@ -137,8 +137,8 @@ def test_newer_entry_points_reject_bad_arguments():
     # learned termination
     assert lib.hnswgpu_set_termination_model(None, None, 4, C.c_float(0.0)) == _capi.ERR_ARG
     opts = _capi.SearchOpts()
-    assert lib.hnswgpu_search_checkpoints(None, None, 1, 10, C.byref(opts), 4, 8, None, None, None, None, None,
-                                          None) == _capi.ERR_ARG
+    assert lib.hnswgpu_search_checkpoints(None, None, 1, 10, C.byref(opts), 4, 8, 0, None, None, None, None, None,
+                                          None, None) == _capi.ERR_ARG
     to = _capi.TermTrainOpts(epochs=1, batch=16, lr=1e-3, pos_weight=1.0, weight_decay=0.0, reserved=0, seed=0)
     assert lib.hnswgpu_term_train(0, None, None, 0, C.byref(to), None, None) == _capi.ERR_ARG
     assert lib.hnswgpu_term_loss_grad(0, None, None, None, 0, C.c_float(1.0), None, None) == _capi.ERR_ARG
@@ -165,7 +165,7 @@ def test_newer_entry_points_reject_bad_arguments():
 def test_termination_model_file_round_trip(tmp_path):
     from hnsw_rabitq_b200 import learned
     rng = np.random.default_rng(0)
-    m = learned.TerminationModel(learned.init_params(rng.normal(size=(50, 6)), 1), 8, 1.25, 96, "fp8", 40,
+    m = learned.TerminationModel(learned.init_params(rng.normal(size=(50, _capi.TERM_FEATURES)), 1), 8, 1.25, 96, "fp8", 40,
                                  {"note": "x"})
     m.save(str(tmp_path / "t.npz"))
     r = learned.TerminationModel.load(str(tmp_path / "t.npz"))

@@ -93,7 +93,7 @@ def test_lean_learned_stop_bounds(tmp_path):
     g.load_index(str(path))
     k, ef, period = 10, 64, 4
     pl, pd, _, pt = g.knn_query_traced(q, k, ef=ef, tie_order="id", precision="fp8")
-    f = rng.normal(size=(64, 6)).astype(np.float32)
+    f = rng.normal(size=(64, learned.F)).astype(np.float32)
     p = learned.init_params(f, 0)
     for never in (float("inf"), 1e30):
         g.set_termination_model(learned.TerminationModel(p, period, never, ef, "fp8"))

@@ -26,7 +26,7 @@ def served(tmp_path_factory):
         g.mark_deleted(lab)
     # a termination network (random weights, finite threshold): what matters
     # here is that the learned stop is deterministic per query
-    f = rng.normal(size=(100, 6)).astype(np.float32)
+    f = rng.normal(size=(100, learned.F)).astype(np.float32)
     g.set_termination_model(learned.TerminationModel(learned.init_params(f, 1), 4, 0.5))
     return g, x, q
 

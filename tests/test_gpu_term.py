@@ -15,7 +15,9 @@ pytestmark = pytest.mark.gpu
 
 def _random_problem(n, seed=0):
     rng = np.random.default_rng(seed)
-    f = (rng.normal(size=(n, 6)) * [1, 0.5, 0.3, 2, 1, 3] + [3, 0.5, 0.1, 1, 10, 2]).astype(np.float32)
+    scale = np.resize([1, 0.5, 0.3, 2, 1, 3], learned.F)
+    shift = np.resize([3, 0.5, 0.1, 1, 10, 2], learned.F)
+    f = (rng.normal(size=(n, learned.F)) * scale + shift).astype(np.float32)
     y = (rng.random(n) < 0.35).astype(np.float32)
     p = learned.init_params(f, seed)
     p[T.OFF_B1:T.OFF_W2] = rng.normal(0, 0.1, T.H)
@@ -56,7 +58,7 @@ def test_inference_matches_oracle_with_fp16_weights():
 
 def test_training_learns_a_separable_rule():
     rng = np.random.default_rng(3)
-    f = rng.normal(size=(20000, 6)).astype(np.float32)
+    f = rng.normal(size=(20000, learned.F)).astype(np.float32)
     y = ((f[:, 0] + 0.5 * f[:, 3] > 0.2) & (f[:, 5] > -1)).astype(np.float32)
     p, losses = learned.train(f, y, epochs=15, batch=512, lr=3e-3, seed=1)
     assert losses[-1] < 0.5 * losses[0]

@@ -65,12 +65,12 @@ def test_checkpoint_labels():
         ids=np.array([[[0, 1, N], [0, 1, 2], [0, 1, 3], [9, 9, 9]],
                       [[5, 6, 7], [5, 6, 8], [0, 0, 0], [0, 0, 0]]], np.uint32),
         nckpt=np.array([3, 2], np.uint32),
-        feat=np.arange(2 * 4 * 6, dtype=np.float32).reshape(2, 4, 6))
+        feat=np.arange(2 * 4 * learned.F, dtype=np.float32).reshape(2, 4, learned.F))
     gt = np.array([[100, 101, 102], [105, 106, 107]], np.uint64)
     X, y = learned.checkpoint_dataset(idx, ck, gt)
     # query 0: final row [0,1,3] hits 2; rows hit 2, 3 -> 1, 1
     # query 1: final row [5,6,8] hits 2; row 0 hits 3 -> 1
-    assert X.shape == (3, 6) and np.array_equal(y, [1, 1, 1])
+    assert X.shape == (3, learned.F) and np.array_equal(y, [1, 1, 1])
     assert np.array_equal(X[2], ck["feat"][1, 0])
     ck["ids"][0, 2] = [0, 1, 2]  # final hits 3: only row 1 reaches it
     X, y = learned.checkpoint_dataset(idx, ck, gt)
