@@ -90,8 +90,8 @@ def parse():
     ap.add_argument("--tie-order", default="reference", choices=["reference", "id"],
                     help="tie order of --profile-steps: reference (heap replay, results identical to hnswlib) "
                          "or id (ties by internal id)")
-    ap.add_argument("--train-queries", type=int, default=20_000, help="learned termination: training queries")
-    ap.add_argument("--term-cap", type=int, default=64, help="learned termination: ef of the training traces")
+    ap.add_argument("--train-queries", type=int, default=12_000, help="learned termination: training queries")
+    ap.add_argument("--term-cap", type=int, default=96, help="learned termination: ef of the training traces")
     ap.add_argument("--term-period", type=int, default=4, help="learned termination: expansions per checkpoint")
     ap.add_argument("--rerank", type=int, default=0, help="FP8 beam: candidates re-ranked in FP32 (0: the pool)")
     ap.add_argument("--workload", default="gmm1m128", choices=["gmm1m128", "bf768", "serve768", "learned96"],
@@ -418,7 +418,7 @@ def run_ours(args, dist: Dist):
         tq = gmm_1m_128_queries(args.train_queries, stream_seed=1000)
         tgt = idx.knn_query_exact(tq, 10)[0]
         ck = learned.traces(idx, tq, 10, args.term_cap, args.term_period,
-                            max(16, 8 * args.term_cap // args.term_period), "fp8", args.rerank)
+                            max(16, 2 * args.term_cap // args.term_period + 8), "fp8", args.rerank)
         params, _ = learned.train(*learned.checkpoint_dataset(idx, ck, tgt), epochs=20, seed=0)
         idx.set_termination_model(learned.TerminationModel(params, args.term_period, args.profile_learned,
                                                            args.term_cap, "fp8", args.rerank))

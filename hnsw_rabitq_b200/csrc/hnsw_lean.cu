@@ -244,19 +244,39 @@ __device__ __forceinline__ float lean_pass(const SearchParams& p, const LeanSmem
         if (blk == 0 && mine)
             cp_async8(smem_u32(s.tails + lane), p.tvecs + (size_t)my_id * p.trow_bytes + D);
         cp_async_wait_all();
-        uint32_t b[2 * NS];
-        load_bfrag<NS>(s, D, blk, lane, b);
         __syncwarp();  // mma.sync needs the whole warp converged
-        // tile 0: rows (g, g + 8) = candidates 4g, 4g + 2; tile 1: 4g + 1, 4g + 3
+        // tile 0: rows (g, g + 8) = candidates 4g, 4g + 2; tile 1: 4g + 1, 4g + 3.
+        // One load unit at a time (both tiles), so that few fragments are live.
+        const unsigned char* qsrc = s.q8 + (g & 1) * D + blk * 128;
+        const unsigned char* r0 = s.stage + (4 * g) * SS;
+        if (NS % 2 == 0) {
 #pragma unroll
-        for (int tile = 0; tile < 2; tile++) {
-            uint32_t a0[2 * NS], a1[2 * NS];
-            read_quarter<NS>(s.stage + (4 * g + tile) * SS, t, valid[tile], a0);
-            read_quarter<NS>(s.stage + (4 * g + tile + 2) * SS, t, valid[tile + 2], a1);
+            for (int u = 0; u < NS / 2; u++) {
+                const int off = (u * 4 + t) * 16;
+                const uint4 bq = *reinterpret_cast<const uint4*>(qsrc + off);
+#pragma unroll
+                for (int tile = 0; tile < 2; tile++) {
+                    const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+                    const uint4 x0 = valid[tile] ? *reinterpret_cast<const uint4*>(r0 + tile * SS + off) : z;
+                    const uint4 x1 = valid[tile + 2] ? *reinterpret_cast<const uint4*>(r0 + (tile + 2) * SS + off) : z;
+                    float (&c)[4] = tile == 0 ? c0 : c1;
+                    mma_e4m3(c, x0.x, x1.x, x0.y, x1.y, bq.x, bq.y);  // step 2u
+                    mma_e4m3(c, x0.z, x1.z, x0.w, x1.w, bq.z, bq.w);  // step 2u + 1
+                }
+            }
+        } else {
 #pragma unroll
             for (int st = 0; st < NS; st++) {
-                if (tile == 0) mma_e4m3(c0, a0[2 * st], a1[2 * st], a0[2 * st + 1], a1[2 * st + 1], b[2 * st], b[2 * st + 1]);
-                else mma_e4m3(c1, a0[2 * st], a1[2 * st], a0[2 * st + 1], a1[2 * st + 1], b[2 * st], b[2 * st + 1]);
+                const int off = (st * 4 + t) * 8;
+                const uint2 bq = *reinterpret_cast<const uint2*>(qsrc + off);
+#pragma unroll
+                for (int tile = 0; tile < 2; tile++) {
+                    const uint2 z = make_uint2(0u, 0u);
+                    const uint2 x0 = valid[tile] ? *reinterpret_cast<const uint2*>(r0 + tile * SS + off) : z;
+                    const uint2 x1 = valid[tile + 2] ? *reinterpret_cast<const uint2*>(r0 + (tile + 2) * SS + off) : z;
+                    float (&c)[4] = tile == 0 ? c0 : c1;
+                    mma_e4m3(c, x0.x, x1.x, x0.y, x1.y, bq.x, bq.y);
+                }
             }
         }
         if (blk == 0 && mine) tail = s.tails[lane];

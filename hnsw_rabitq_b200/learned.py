@@ -254,7 +254,9 @@ def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int =
     nh = max(1, int(round(n * holdout)))
     hold, tr = perm[:nh], perm[nh:]
     if max_ckpt is None:
-        max_ckpt = max(16, (8 * ef_cap) // period)
+        # checkpoints fall at most once per period; a beam of ef_cap rarely
+        # exceeds twice ef_cap expansions
+        max_ckpt = max(16, (2 * ef_cap) // period + 8)
     ck = traces(index, queries[tr], k, ef_cap, period, max_ckpt, precision, rerank)
     X, y = checkpoint_dataset(index, ck, gt[tr])
     params, losses = train(X, y, epochs=epochs, seed=seed, device=device)
