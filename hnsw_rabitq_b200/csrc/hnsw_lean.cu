@@ -84,6 +84,7 @@ struct LeanSmem {
     uint32_t* vis;       // direct-mapped visited cache; re-rank scratch after the beam
     unsigned char* stage;  // 32 row slots (lean_stage bytes apart): one distance pass's gathered rows
     float2* tails;       // 32 (scale, squared norm) of the pass's candidates
+    const float* model;  // learned stop: the CTA's copy of the packed network
 };
 
 struct LeanQuery {
@@ -395,11 +396,9 @@ __device__ __forceinline__ void lean_record_ids(const SearchParams& p, const Lea
 }
 
 // Checkpoint of the learned termination (trace mode 1 records it, mode 2
-// asks the network whether to stop), with the general beam's features.  Not
-// inlined: it runs every few expansions, and the features and the network
-// would otherwise raise the register need of the whole beam loop.
+// asks the network whether to stop), with the general beam's features.
 template <int SPACE, int TERM>
-__device__ __noinline__ bool lean_checkpoint(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
+__device__ __forceinline__ bool lean_checkpoint(const SearchParams& p, const LeanSmem& s, int lane, uint32_t qi,
                                                 uint32_t e, uint32_t dists, int psize, uint32_t next_dk,
                                                 float d_entry, float qn, LeanTerm& ts) {
     if (psize == 0) return false;
@@ -420,7 +419,7 @@ __device__ __noinline__ bool lean_checkpoint(const SearchParams& p, const LeanSm
         ts.nckpt++;
         return false;
     }
-    return term_logit(p.term_model, fe, lane) > p.term_logit;
+    return term_logit<true>(s.model, fe, lane) > p.term_logit;
 }
 
 template <int SPACE>
@@ -670,10 +669,11 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         if (sel == 0) break;
         // a checkpoint falls due every term_period expansions; it is taken
         // (trace mode records it, learned mode consults the network) at the
-        // first iteration from then on where no unexpanded candidate is
-        // closer than the current k-th result, the only states in which
-        // stopping can keep the top-k
-        if (TERM && ct.l0_exp >= ts.next && psize >= kq && next_dk > khi(s.pool[kq - 1])) {
+        // first iteration from then on where the top-k has not changed for a
+        // period and no unexpanded candidate is closer than the current k-th
+        // result, the only states in which stopping can keep the top-k
+        if (TERM && ct.l0_exp >= ts.next && ct.l0_exp - ts.last_change >= p.term_period && psize >= kq &&
+            next_dk > khi(s.pool[kq - 1])) {
             const bool stop =
                 lean_checkpoint<SPACE, TERM>(p, s, lane, qi, ct.l0_exp, ct.l0_dists, psize, next_dk, d_entry, lq.qn, ts);
             while (ts.next <= ct.l0_exp) ts.next += p.term_period;
@@ -800,11 +800,26 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     LPT(8);
 }
 
+// Query warps per CTA: the learned-stop kernels keep one copy of the packed
+// network in shared memory for four warps.
+template <int TERM>
+struct LeanCta {
+    static constexpr int kWarps = TERM == 2 ? kLeanWarpsPerBlockLearned : kLeanWarpsPerBlock;
+    static constexpr size_t kModel = TERM == 2 ? kLeanModelSmem : 0;
+};
+
 template <int SPACE, int TERM, int NS, bool MULTI>
-__global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hnsw_lean_kernel(SearchParams p) {
+__global__ void __launch_bounds__(LeanCta<TERM>::kWarps * 32, HNSWGPU_MINB_LEAN * 2 / LeanCta<TERM>::kWarps)
+    hnsw_lean_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* base = smem + (size_t)warp * p.warp_smem;
+    if (TERM == 2) {
+        const uint4* src = reinterpret_cast<const uint4*>(p.term_model);
+        uint4* dst = reinterpret_cast<uint4*>(smem);
+        for (uint32_t i = threadIdx.x; i < (uint32_t)(kTermPackedBytes / 16); i += blockDim.x) dst[i] = __ldg(src + i);
+        __syncthreads();
+    }
+    unsigned char* base = smem + LeanCta<TERM>::kModel + (size_t)warp * p.warp_smem;
     LeanSmem s;
     s.q = reinterpret_cast<float*>(base + p.off_query);
     s.q8 = base + p.off_q8;
@@ -814,6 +829,7 @@ __global__ void __launch_bounds__(kLeanWarpsPerBlock * 32, HNSWGPU_MINB_LEAN) hn
     s.vis = reinterpret_cast<uint32_t*>(base + p.off_vis);
     s.stage = base + p.off_stage;
     s.tails = reinterpret_cast<float2*>(base + p.off_lacc + 64 * 8);
+    s.model = reinterpret_cast<const float*>(smem);
     LeanClock lc;
     if (!LCHK(p.off_vis + ((size_t)4 << p.log2_vis) <= p.warp_smem && p.off_pool + (size_t)8 * p.ef <= p.off_vis,
               280, p.off_vis, p.warp_smem))
@@ -858,24 +874,25 @@ cudaError_t launch_lean_t(const SearchParams& p, int num_sms, cudaStream_t strea
     static size_t occ_smem = 0;
     static int occ_per_sm = 0;
     const void* fn = (const void*)hnsw_lean_kernel<SPACE, TERM, NS, MULTI>;
-    const size_t smem = (size_t)p.warp_smem * kLeanWarpsPerBlock;
+    constexpr int wpb = LeanCta<TERM>::kWarps;
+    const size_t smem = LeanCta<TERM>::kModel + (size_t)p.warp_smem * wpb;
     if ((int)smem > attr_smem) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         attr_smem = (int)smem;
     }
     if (smem != occ_smem) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, fn, kLeanWarpsPerBlock * 32, smem);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, fn, wpb * 32, smem);
         if (e != cudaSuccess) return e;
         occ_smem = smem;
     }
     if (occ_per_sm < 1) return cudaErrorInvalidConfiguration;
-    const uint64_t need = (p.nq + kLeanWarpsPerBlock - 1) / kLeanWarpsPerBlock;
+    const uint64_t need = (p.nq + wpb - 1) / wpb;
     uint64_t blocks = (uint64_t)occ_per_sm * (uint64_t)num_sms;
     if (blocks > need) blocks = need;
     if (blocks < 1) blocks = 1;
     if (blocks_out) *blocks_out = (int)blocks;
-    hnsw_lean_kernel<SPACE, TERM, NS, MULTI><<<(unsigned)blocks, kLeanWarpsPerBlock * 32, smem, stream>>>(p);
+    hnsw_lean_kernel<SPACE, TERM, NS, MULTI><<<(unsigned)blocks, wpb * 32, smem, stream>>>(p);
     return cudaGetLastError();
 }
 

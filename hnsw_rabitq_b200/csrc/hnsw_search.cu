@@ -589,13 +589,15 @@ struct TermState {
 
 // A checkpoint falls due every term_period expansions; it is taken (trace
 // mode records it, learned mode consults the network) at the first
-// expansion from then on where no unexpanded candidate is closer than the
-// current k-th result -- the only states in which stopping can keep the
-// top-k.  Advances the due count once taken.
+// expansion from then on where the top-k has not changed for a period and no
+// unexpanded candidate is closer than the current k-th result -- the only
+// states in which stopping can keep the top-k.  Advances the due count once
+// taken.
 __device__ __forceinline__ bool term_due(const SearchParams& p, const WarpSmem& s, uint32_t e, int psize,
                                          uint32_t next_dk, TermState& ts) {
     if (ts.next == 0) ts.next = p.term_period;
-    if (e < ts.next || psize < (int)p.k || !(next_dk > khi(s.pool[p.k - 1]))) return false;
+    if (e < ts.next || e - ts.last_change < p.term_period || psize < (int)p.k || !(next_dk > khi(s.pool[p.k - 1])))
+        return false;
     while (ts.next <= e) ts.next += p.term_period;
     return true;
 }

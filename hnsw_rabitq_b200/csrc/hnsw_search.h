@@ -166,6 +166,10 @@ size_t lean_smem_layout(SearchParams& p);
 bool lean_eligible(const SearchParams& p);
 cudaError_t launch_hnsw_lean(const SearchParams& p, int space, int num_sms, cudaStream_t stream, int* blocks_out);
 constexpr int kLeanWarpsPerBlock = 2;
+// learned-stop lean kernels: four query warps share one copy of the packed
+// network in shared memory
+constexpr int kLeanWarpsPerBlockLearned = 4;
+constexpr size_t kLeanModelSmem = (kTermPackedBytes + 127) & ~(size_t)127;
 
 // Low-precision traversal copies (quantize.cu).  Row layouts:
 //   bf16: dim x bf16, zero padded to a 16-byte multiple;

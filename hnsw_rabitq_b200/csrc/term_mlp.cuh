@@ -42,15 +42,16 @@ struct TermInputs {
     float eval_rate;  // distance evaluations per expansion since the previous checkpoint
 };
 
-__device__ __forceinline__ float term_ratio(float d, float dk, float a) {
-    return fminf(fmaxf((d - dk) / a, -4.f), 4.f);
+// (d - d_k) / |d_k| clamped to [-4, 4]; inv_a = 1 / |d_k|
+__device__ __forceinline__ float term_ratio(float d, float dk, float inv_a) {
+    return fminf(fmaxf((d - dk) * inv_a, -4.f), 4.f);
 }
 
 // f6 .. f12 and f15 from the sorted beam (distance key << 32 | id, EXP_BIT on
 // expanded entries), psize >= 1 entries; whole warp, identical in every lane.
 __device__ __forceinline__ void term_pool_features(const uint64_t* pool, int psize, int ef, float dk, int lane,
                                                    float f[kTermFeatures]) {
-    const float a = fabsf(dk) + 1e-30f;
+    const float a = fabsf(dk) + 1e-30f, inv_a = 1.0f / a;
     const uint32_t t1 = fkey(dk + 0.1f * a), t2 = fkey(dk + 0.25f * a), t3 = fkey(dk + 0.5f * a);
     int n1 = 0, n2 = 0, n3 = 0, nw = 0;
     uint32_t first_wait = 0xffffffffu;
@@ -67,24 +68,24 @@ __device__ __forceinline__ void term_pool_features(const uint64_t* pool, int psi
         n3 += __popc(__ballot_sync(0xffffffffu, w && h < t3));
     }
     const float inv_ef = 1.0f / (float)ef;
-    f[6] = first_wait == 0xffffffffu ? 4.f : term_ratio(funkey(first_wait), dk, a);
-    f[7] = term_ratio(funkey(khi(pool[psize - 1])), dk, a);
+    f[6] = first_wait == 0xffffffffu ? 4.f : term_ratio(funkey(first_wait), dk, inv_a);
+    f[7] = term_ratio(funkey(khi(pool[psize - 1])), dk, inv_a);
     f[8] = __log2f(1.0f + (float)n1);
     f[9] = __log2f(1.0f + (float)n2);
     f[10] = __log2f(1.0f + (float)n3);
     f[11] = (float)nw * inv_ef;
     f[12] = (float)psize * inv_ef;
-    f[15] = term_ratio(funkey(khi(pool[psize >> 1])), dk, a);
+    f[15] = term_ratio(funkey(khi(pool[psize >> 1])), dk, inv_a);
 }
 
 // All features: the scalar ones here, the beam's from term_pool_features.
 __device__ __forceinline__ void term_features(const TermInputs& in, const uint64_t* pool, int psize, int ef,
                                               int lane, float f[kTermFeatures]) {
-    const float a = fabsf(in.dk) + 1e-30f;
+    const float inv_a = 1.0f / (fabsf(in.dk) + 1e-30f);
     f[0] = __log2f(1.0f + in.e);
-    f[1] = fminf(fmaxf(in.d1 / a, -4.f), 4.f);
-    f[2] = term_ratio(in.dn, in.dk, a);
-    f[3] = __log2f(1.0f + fminf(fmaxf(in.d_entry / a, 0.f), 1e6f));
+    f[1] = fminf(fmaxf(in.d1 * inv_a, -4.f), 4.f);
+    f[2] = term_ratio(in.dn, in.dk, inv_a);
+    f[3] = __log2f(1.0f + fminf(fmaxf(in.d_entry * inv_a, 0.f), 1e6f));
     f[4] = __log2f(1.0f + in.qn);
     f[5] = fminf(in.since_change * in.inv_period, 16.f);
     f[13] = __log2f(1.0f + in.nchange);
@@ -144,13 +145,22 @@ __device__ __forceinline__ uint32_t pack_half2(float lo, float hi) {
 // units 8v + 2t and 8v + 2t + 1 of tile v; the layer-1 accumulators, after
 // bias and ReLU, are exactly the A fragments of layer 2.  Operands are fp16
 // (standardised features, hidden activations, weights), accumulation fp32.
-// `m` is the packed inference form (pack_term_model).
+// `m` is the packed inference form (pack_term_model), in global memory or,
+// with SMEM, in shared memory.
+// Loads of the packed network: read-only cache, or shared memory (SMEM).
+template <bool SMEM, class T>
+__device__ __forceinline__ T term_ld(const T* p) {
+    if (SMEM) return *p;
+    return __ldg(p);
+}
+
+template <bool SMEM = false>
 __device__ __forceinline__ float term_logit(const float* __restrict__ m, const float f[kTermFeatures], int lane) {
     constexpr unsigned kFull = 0xffffffffu;
     const int t = lane & 3;
     const float* mu = m;
     const float* inv_sigma = m + kTermFeatures;
-    const float b3 = __ldg(m + 2 * kTermFeatures);
+    const float b3 = term_ld<SMEM>(m + 2 * kTermFeatures);
     const float4* b1f = reinterpret_cast<const float4*>(m + kTermPackedHead) + t * 4;  // [t][8] float2
     const float4* b2f = reinterpret_cast<const float4*>(m + kTermPackedHead + 64) + t * 4;
     const uint4* w3f = reinterpret_cast<const uint4*>(m + kTermPackedFloats) + t * 2;  // [t][8] half2
@@ -162,10 +172,10 @@ __device__ __forceinline__ float term_logit(const float* __restrict__ m, const f
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
         if (2 * t == i) {
-            x0 = (f[i] - __ldg(mu + i)) * __ldg(inv_sigma + i);
-            x1 = (f[i + 1] - __ldg(mu + i + 1)) * __ldg(inv_sigma + i + 1);
-            x2 = (f[i + 8] - __ldg(mu + i + 8)) * __ldg(inv_sigma + i + 8);
-            x3 = (f[i + 9] - __ldg(mu + i + 9)) * __ldg(inv_sigma + i + 9);
+            x0 = (f[i] - term_ld<SMEM>(mu + i)) * term_ld<SMEM>(inv_sigma + i);
+            x1 = (f[i + 1] - term_ld<SMEM>(mu + i + 1)) * term_ld<SMEM>(inv_sigma + i + 1);
+            x2 = (f[i + 8] - term_ld<SMEM>(mu + i + 8)) * term_ld<SMEM>(inv_sigma + i + 8);
+            x3 = (f[i + 9] - term_ld<SMEM>(mu + i + 9)) * term_ld<SMEM>(inv_sigma + i + 9);
         }
     }
     const uint32_t ax = pack_half2(x0, x1), ay = pack_half2(x2, x3);
@@ -174,40 +184,29 @@ __device__ __forceinline__ float term_logit(const float* __restrict__ m, const f
 #pragma unroll
     for (int v = 0; v < 8; v++) {
         float c[4] = {0.f, 0.f, 0.f, 0.f};
-        const uint2 w = __ldg(reinterpret_cast<const uint2*>(W1f) + v);
+        const uint2 w = term_ld<SMEM>(reinterpret_cast<const uint2*>(W1f) + v);
         mma_f16(c, ax, ax, ay, ay, w.x, w.y);
-        const float4 bb = __ldg(b1f + (v >> 1));
+        const float4 bb = term_ld<SMEM>(b1f + (v >> 1));
         const float bx = (v & 1) ? bb.z : bb.x, by = (v & 1) ? bb.w : bb.y;
         a2[v] = pack_half2(fmaxf(c[0] + bx, 0.f), fmaxf(c[1] + by, 0.f));
     }
-    // layer 2: k-step s uses units 16s + 2t (+1) (tile 2s) and 16s + 2t + 8 (+9) (tile 2s + 1)
-    float acc[8][4];
-#pragma unroll
-    for (int v = 0; v < 8; v++) acc[v][0] = acc[v][1] = acc[v][2] = acc[v][3] = 0.f;
-#pragma unroll
-    for (int st = 0; st < 4; st++) {
-        uint32_t wb[16];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const uint4 u = __ldg(W2f + st * 4 + i);
-            wb[4 * i] = u.x; wb[4 * i + 1] = u.y; wb[4 * i + 2] = u.z; wb[4 * i + 3] = u.w;
-        }
-#pragma unroll
-        for (int v = 0; v < 8; v++)
-            mma_f16(acc[v], a2[2 * st], a2[2 * st], a2[2 * st + 1], a2[2 * st + 1], wb[2 * v], wb[2 * v + 1]);
-    }
+    // layer 2, one output tile at a time (few live accumulators): k-step s
+    // uses units 16s + 2t (+1) (tile 2s) and 16s + 2t + 8 (+9) (tile 2s + 1);
+    // then bias, ReLU and the output weights of the tile's units 8v + 2t, + 1
     float sum = 0.f;
+#pragma unroll 2
+    for (int v = 0; v < 8; v++) {
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-    for (int v = 0; v < 8; v += 2) {
-        const float4 bb = __ldg(b2f + (v >> 1));
-        const uint4 wq = __ldg(w3f + (v >> 2));
-        const uint32_t wa = (v & 2) ? wq.z : wq.x, wc = (v & 2) ? wq.w : wq.y;
-        const float2 o0 = __half22float2(*reinterpret_cast<const __half2*>(&wa));
-        const float2 o1 = __half22float2(*reinterpret_cast<const __half2*>(&wc));
-        sum = fmaf(o0.x, fmaxf(acc[v][0] + bb.x, 0.f), sum);
-        sum = fmaf(o0.y, fmaxf(acc[v][1] + bb.y, 0.f), sum);
-        sum = fmaf(o1.x, fmaxf(acc[v + 1][0] + bb.z, 0.f), sum);
-        sum = fmaf(o1.y, fmaxf(acc[v + 1][1] + bb.w, 0.f), sum);
+        for (int st = 0; st < 4; st++) {
+            const uint2 w = term_ld<SMEM>(reinterpret_cast<const uint2*>(W2f) + st * 8 + v);
+            mma_f16(acc, a2[2 * st], a2[2 * st], a2[2 * st + 1], a2[2 * st + 1], w.x, w.y);
+        }
+        const float2 bb = term_ld<SMEM>(reinterpret_cast<const float2*>(b2f) + v);
+        const uint32_t wv = term_ld<SMEM>(reinterpret_cast<const uint32_t*>(w3f) + v);
+        const float2 o = __half22float2(*reinterpret_cast<const __half2*>(&wv));
+        sum = fmaf(o.x, fmaxf(acc[0] + bb.x, 0.f), sum);
+        sum = fmaf(o.y, fmaxf(acc[1] + bb.y, 0.f), sum);
     }
     sum += __shfl_xor_sync(kFull, sum, 1);
     sum += __shfl_xor_sync(kFull, sum, 2);

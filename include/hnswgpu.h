@@ -336,8 +336,9 @@ HNSWGPU_API int hnswgpu_fp64_distances(hnswgpu_index* index, const float* querie
  * candidate queue is exhausted (hnswlib/hnswalg.h:368-376).
  *
  * Every `period` level-0 expansions (at the first state from then on where
- * no waiting candidate is closer than the k-th result) the beam forms a
- * feature vector of its state, with a = |d_k|:
+ * the top-k has not changed for `period` expansions and no waiting
+ * candidate is closer than the k-th result) the beam forms a feature vector
+ * of its state, with a = |d_k|:
  *   f0 log2(1 + expansions)            f8..f10 log2(1 + n(x)), x = 0.1, 0.25, 0.5
  *   f1 d_1 / a                         f11 waiting candidates / ef
  *   f2 (d_next - d_k) / a              f12 beam size / ef

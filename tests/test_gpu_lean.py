@@ -100,8 +100,8 @@ def test_lean_learned_stop_bounds(tmp_path):
         ll, ld, _, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", precision="fp8", learned=True)
         assert np.array_equal(ll, pl) and np.array_equal(lt[:, 2], pt[:, 2])
     # -inf stops at the first checkpoint taken: the first one due (every
-    # `period` expansions) at which no unexpanded candidate is closer than
-    # the current k-th result
+    # `period` expansions) at which the top-k has been stable for a period
+    # and no unexpanded candidate is closer than the current k-th result
     g.set_termination_model(learned.TerminationModel(p, period, -float("inf"), ef, "fp8"))
     ll, ld, lc, lt = g.knn_query_traced(q, k, ef=ef, tie_order="id", precision="fp8", learned=True)
     assert np.all(lt[:, 2] <= pt[:, 2]) and lt[:, 2].mean() < 0.8 * pt[:, 2].mean() and np.all(lc == k)
