@@ -50,9 +50,20 @@ constexpr int kKBytes = 128;                   // bytes of K per stage (one swiz
 constexpr int kABytes = kTileM * kKBytes;      // 16 KB
 constexpr int kBBytes = kTileN * kKBytes;      // 32 KB
 constexpr int kStageBytes = kABytes + kBBytes;
-constexpr int kThreads = 192;
+// warp 0: TMA producer; warp 1: MMA issuer; warps 2-9: epilogue, two warps
+// per TMEM lane quarter (each reads half of a tile's columns), so that every
+// scheduler has two epilogue warps to interleave
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr int kTopT = 16;                      // sample rank of the threshold
-constexpr int kStageC = 8;                     // candidates staged per thread and tile
+constexpr int kStageC = 4;                     // candidates staged per epilogue thread and tile
+// Resident query tile (fp8, K <= 768 bytes): the work item's A tiles stay in
+// shared memory for all its row tiles (one L2 read instead of one per row
+// tile) and only the B tiles stream, through a 3-stage ring; the two layouts
+// take the same bytes (6 x 16 KB + 3 x 32 KB = 4 x 48 KB).
+constexpr int kResAKb = 6;
+constexpr int kStagesB = 3;
+static_assert(kResAKb * kABytes + kStagesB * kBBytes == kStages * kStageBytes, "resident layout");
 
 #ifdef HNSWGPU_TC_TIMING
 // Opt-in role timing of the scores pass (not in the shipped library): per
@@ -66,8 +77,9 @@ __device__ unsigned long long g_tc_timing[256][10];
 
 struct TcSmem {
     float2 hinfo[2][kTileN];  // per-row helpers of the tiles in the two accumulators
-    uint64_t cst[128][2][kStageC];  // candidates of the current / previous tile per epilogue thread
+    uint64_t cst[2][128][2][kStageC];  // candidates of the current / previous tile per epilogue thread
     uint64_t full[kStages], empty[kStages], tfull[2], tempty[2], done;
+    uint64_t afull, aempty;  // resident query tile loaded / no longer read by the MMAs
     uint32_t tmem, error;
 };
 constexpr size_t kSmemBytes = 1024 + (size_t)kStages * kStageBytes + sizeof(TcSmem);
@@ -171,7 +183,7 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 
 // MODE 0: filter-append pass over all rows; MODE 1: threshold pass over the
 // sample (one work item per query tile, top-16 kept in registers).
-template <int PREC, int SPACE, int MODE>
+template <int PREC, int SPACE, int MODE, bool RESA>
 __global__ void __launch_bounds__(kThreads, 1)
     bf_tc_kernel(const __grid_constant__ CUtensorMap qmap, const __grid_constant__ CUtensorMap xmap, TcArgs a) {
     extern __shared__ __align__(1024) unsigned char raw[];
@@ -195,9 +207,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(&s.tfull[i], 1);
-            mbar_init(&s.tempty[i], 128);
+            mbar_init(&s.tempty[i], kEpiWarps * 32);
         }
         mbar_init(&s.done, 1);
+        mbar_init(&s.afull, 1);
+        mbar_init(&s.aempty, 1);
         s.error = 0;
         fence_mbar_init();
     }
@@ -215,11 +229,22 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---- TMA producer
         if (lane == 0) {
             int stage = 0, hacc = 0;
-            uint32_t phase = 0, haphase = 0;
+            uint32_t phase = 0, haphase = 0, nitem = 0;
             const long long p0 = clock64();
-            for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x) {
+            constexpr int nst = RESA ? kStagesB : kStages;
+            for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x, nitem++) {
                 const uint32_t qt = it % q_tiles, ck = it / q_tiles;
                 const uint32_t t_end = min(n_tiles, (ck + 1) * chunk);
+                if (RESA) {
+                    // the previous item's MMAs have finished with the resident tile
+                    if (nitem > 0 && !tc_wait(&s.aempty, (nitem - 1) & 1u)) {
+                        *err = 1;
+                        break;
+                    }
+                    mbar_arrive_expect_tx(&s.afull, (uint32_t)(kb_count * kABytes));
+                    for (int kb = 0; kb < kb_count; kb++)
+                        tma_load_2d(base + (size_t)kb * kABytes, &qmap, kb * kKBytes, (int)(qt * kTileM), &s.afull);
+                }
                 for (uint32_t t = ck * chunk; t < t_end && !*err; t++) {
                     // the helper slot of this tile is the one of its accumulator:
                     // free once the epilogue released that accumulator
@@ -234,14 +259,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                             break;
                         }
                         TCT_ADD(0, clock64() - w0);
-                        unsigned char* sa = base + (size_t)stage * kStageBytes;
                         const bool with_h = NEEDH && kb == 0;
-                        mbar_arrive_expect_tx(&s.full[stage], kStageBytes + (with_h ? kTileN * 8 : 0));
                         const int x = kb * (PREC == 1 ? kKBytes / 2 : kKBytes);
-                        tma_load_2d(sa, &qmap, x, (int)(qt * kTileM), &s.full[stage]);
-                        tma_load_2d(sa + kABytes, &xmap, x, (int)(t * kTileN), &s.full[stage]);
+                        if (RESA) {
+                            unsigned char* sb = base + (size_t)kResAKb * kABytes + (size_t)stage * kBBytes;
+                            mbar_arrive_expect_tx(&s.full[stage], kBBytes + (with_h ? kTileN * 8 : 0));
+                            tma_load_2d(sb, &xmap, x, (int)(t * kTileN), &s.full[stage]);
+                        } else {
+                            unsigned char* sa = base + (size_t)stage * kStageBytes;
+                            mbar_arrive_expect_tx(&s.full[stage], kStageBytes + (with_h ? kTileN * 8 : 0));
+                            tma_load_2d(sa, &qmap, x, (int)(qt * kTileM), &s.full[stage]);
+                            tma_load_2d(sa + kABytes, &xmap, x, (int)(t * kTileN), &s.full[stage]);
+                        }
                         if (with_h) bulk_g2s(&s.hinfo[hacc][0], a.rowinfo + (size_t)t * kTileN, kTileN * 8, &s.full[stage]);
-                        if (++stage == kStages) {
+                        if (++stage == nst) {
                             stage = 0;
                             phase ^= 1u;
                         }
@@ -262,11 +293,16 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t idesc = (1u << 4) | (PREC == 1 ? (1u << 7) | (1u << 10) : 0u) |
                                    ((uint32_t)(kTileN >> 3) << 17) | ((uint32_t)(kTileM >> 4) << 24);
             int stage = 0, acc = 0;
-            uint32_t phase = 0, aphase = 0;
+            uint32_t phase = 0, aphase = 0, nitem = 0;
+            constexpr int nst = RESA ? kStagesB : kStages;
             const long long m0 = clock64();
-            for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x) {
+            for (uint32_t it = blockIdx.x; it < items && !*err; it += gridDim.x, nitem++) {
                 const uint32_t ck = it / q_tiles;
                 const uint32_t t_end = min(n_tiles, (ck + 1) * chunk);
+                if (RESA && !tc_wait(&s.afull, nitem & 1u)) {
+                    *err = 1;
+                    break;
+                }
                 for (uint32_t t = ck * chunk; t < t_end && !*err; t++) {
                     const long long w1 = clock64();
                     if (!tc_wait(&s.tempty[acc], aphase ^ 1u)) {
@@ -284,13 +320,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                         }
                         TCT_ADD(2, clock64() - w2);
                         tc_fence_after();
-                        const uint32_t sa = smem_u32(base + (size_t)stage * kStageBytes);
-                        const uint64_t da = umma_desc(sa), db = umma_desc(sa + kABytes);
+                        uint64_t da, db;
+                        if (RESA) {
+                            da = umma_desc(smem_u32(base + (size_t)kb * kABytes));
+                            db = umma_desc(smem_u32(base + (size_t)kResAKb * kABytes + (size_t)stage * kBBytes));
+                        } else {
+                            const uint32_t sa = smem_u32(base + (size_t)stage * kStageBytes);
+                            da = umma_desc(sa);
+                            db = umma_desc(sa + kABytes);
+                        }
 #pragma unroll
                         for (int ks = 0; ks < 4; ks++)  // 32 bytes of K per MMA
                             umma<PREC>(d, da + 2 * ks, db + 2 * ks, idesc, (kb | ks) != 0);
                         umma_commit(&s.empty[stage]);
-                        if (++stage == kStages) {
+                        if (++stage == nst) {
                             stage = 0;
                             phase ^= 1u;
                         }
@@ -301,6 +344,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                         aphase ^= 1u;
                     }
                 }
+                // the resident query tile is free once this item's MMAs complete
+                if (RESA) umma_commit(&s.aempty);
             }
             TCT_ADD(4, clock64() - m0);
             // every MMA issued has completed before TMEM is released
@@ -309,9 +354,14 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         __syncwarp();
     } else {
-        // ---- epilogue: warps 2-5, TMEM lane quarter = warp % 4
+        // ---- epilogue: warps 2-9, TMEM lane quarter = warp % 4; half h of
+        // them reads the tile's columns [128 h, 128 h + 128) (the threshold
+        // pass: half 0 reads all 256, half 1 only releases the accumulator)
         const int quarter = warp & 3;
+        const int half = (warp - 2) >> 2;
         const int r = quarter * 32 + lane;  // query row within the tile
+        const int cb_begin = MODE == 1 ? 0 : 2 * half;
+        const int cb_end = MODE == 1 ? (half == 0 ? 4 : 0) : 2 * half + 2;
         int acc = 0;
         uint32_t aphase = 0;
         const long long e0 = clock64();
@@ -327,7 +377,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const float coef = (SPACE == 0 ? -2.0f : -1.0f) * sq;
             // candidates of a tile are staged, then claimed with one atomic
             // whose result is used a tile later (its latency hidden)
-            uint64_t* cst = &s.cst[r][0][0];
+            uint64_t* cst = &s.cst[half][r][0][0];
             int cb_cur = 0, n_cur = 0, n_prev = 0;
             uint32_t prev_slot = 0;
             float top[kTopT];
@@ -346,7 +396,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)acc * kTileN;
                 const float2* hinfo = s.hinfo[acc];
 #pragma unroll 1
-                for (int cb = 0; cb < 4; cb++) {
+                for (int cb = cb_begin; cb < cb_end; cb++) {
                     float v[64];
 #ifdef HNSWGPU_TC_TIMING
                     const long long l0 = clock64();
@@ -439,7 +489,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     aphase ^= 1u;
                 }
             }
-            if (MODE == 1 && qok) a.tau[q] = top[kTopT - 1];
+            if (MODE == 1 && qok && half == 0) a.tau[q] = top[kTopT - 1];
             if (MODE == 0)  // the item's last claimed batch
                 for (int i = 0; i < n_prev; i++)
                     if (prev_slot + i < a.cap)
@@ -709,7 +759,8 @@ __global__ void fp64_distance_kernel(const float* __restrict__ q, uint64_t npair
 
 template <int PREC, int SPACE, int MODE>
 cudaError_t launch_tc(const CUtensorMap& qm, const CUtensorMap& xm, const TcArgs& a, int grid, cudaStream_t st) {
-    auto fn = bf_tc_kernel<PREC, SPACE, MODE>;
+    const bool resa = PREC == 2 && a.k_blocks <= (uint32_t)kResAKb;
+    auto fn = resa ? bf_tc_kernel<PREC, SPACE, MODE, PREC == 2> : bf_tc_kernel<PREC, SPACE, MODE, false>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmemBytes);
     if (e != cudaSuccess) return e;
     fn<<<grid, kThreads, kSmemBytes, st>>>(qm, xm, a);

@@ -38,6 +38,12 @@
 #include "hnsw_search.h"
 #include "hnsw_multivec.h"
 
+// smallest visited cache of a beam, log2 entries (the cache grows with ef
+// up to 2^12 entries)
+#ifndef HNSWGPU_VIS_LOG2_MIN
+#define HNSWGPU_VIS_LOG2_MIN 10
+#endif
+
 static_assert(HNSWGPU_TERM_PARAMS == hnswgpu::kTermParams, "termination parameter count");
 static_assert(HNSWGPU_TERM_FEATURES == hnswgpu::kTermFeatures, "termination feature count");
 
@@ -435,7 +441,7 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     } else {
         p.cand_cap = exact ? std::max<uint32_t>(512u, 12u * p.ef) : 0u;
     }
-    p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(10, next_pow2_log2(16ull * p.ef)));
+    p.log2_vis = std::min<uint32_t>(12, std::max<uint32_t>(HNSWGPU_VIS_LOG2_MIN, next_pow2_log2(16ull * p.ef)));
     if (prec) {
         const char* need =
             "low-precision traversal needs dim % 16 == 0, maxM0 <= 32 (fp8 without deletions or a filter: "
