@@ -728,8 +728,8 @@ def run_bf768(args, dist: Dist):
         stream.synchronize()
         return ev0.elapsed_time(ev1) / steps, dl.cpu().numpy().view(np.uint64), dd.cpu().numpy()
 
-    if args.profile_steps:  # only the bf16 tensor-core search (for ncu)
-        timed(_capi.PREC_BF16, args.steps, args.warmup)
+    if args.profile_steps:  # one tensor-core form (for ncu): fp8 with --profile-precision fp8, else bf16
+        timed(_capi.PREC_FP8 if args.profile_precision == "fp8" else _capi.PREC_BF16, args.steps, args.warmup)
         return None
     peak, kind = measured_tflops()
     arms = {}

@@ -668,6 +668,10 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         __syncwarp();
         LPT(2);
         if (sel == 0) break;
+        // ---- link slots j = lane and lane + 32 (row j / maxM0, entry j % maxM0),
+        // loaded before a checkpoint so that the network runs in their shadow
+        uint32_t id0, id1;
+        lean_links(p, maxM0, sel, cand0, cand1, lane, id0, id1);
         // a checkpoint falls due every term_period expansions; it is taken
         // (trace mode records it, learned mode consults the network) at the
         // first iteration from then on where the top-k has not changed for a
@@ -684,9 +688,6 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
         if (ct.l0_exp >= p.max_expansions) break;
         ct.l0_exp += (uint32_t)sel;
 
-        // ---- link slots j = lane and lane + 32 (row j / maxM0, entry j % maxM0)
-        uint32_t id0, id1;
-        lean_links(p, maxM0, sel, cand0, cand1, lane, id0, id1);
         bool f0 = id0 != INVALID_ID, f1 = id1 != INVALID_ID;
         if (!p.links_unique) {
             const unsigned p0 = __match_any_sync(FULL, id0), p1 = __match_any_sync(FULL, id1);
