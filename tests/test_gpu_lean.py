@@ -111,3 +111,45 @@ def test_lean_learned_stop_bounds(tmp_path):
     assert np.array_equal(ck["labels"], pl)
     n = ck["nckpt"].astype(np.int64)
     assert np.all(n >= 1) and np.all(n - 1 <= pt[:, 2] // period)
+
+
+@pytest.mark.parametrize("space", ["l2", "ip"])
+def test_lean_traces_record_rerank_inputs(tmp_path, space):
+    """Trace mode of the fp8 beam records the first R beam entries with their
+    float32 distances (R = the re-rank count, the whole pool by default): the
+    distances are the float32 distances of those ids (within summation-order
+    rounding), and the final row's answer -- the k closest of its recorded
+    entries -- is what the search itself returns after its re-rank."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((8000, 64)).astype(np.float32)
+    q = rng.standard_normal((200, 64)).astype(np.float32)
+    if space == "ip":
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+        q /= np.linalg.norm(q, axis=1, keepdims=True)
+    path = tmp_path / "g.bin"
+    build_hnsw(path, x, space, M=16, efc=100, num_threads=8)
+    g = H.Index(space, 64)
+    g.load_index(str(path))
+    k, ef, period = 10, 48, 4
+    ck = learned.traces(g, q, k, ef, period, 64, "fp8", 0)
+    assert ck["ids"].shape[2] == ef and ck["ckpt_dists"].shape == ck["ids"].shape
+    lab_of = g.labels_by_internal_id()
+    n = ck["nckpt"].astype(np.int64)
+    rows = np.arange(len(q))
+    # recorded distances against numpy float32 (the stored rows are the inputs)
+    for i in range(0, len(q), 7):
+        for r in range(n[i]):
+            ids = ck["ids"][i, r]
+            ok = ids != 0xffffffff
+            d = ck["ckpt_dists"][i, r]
+            assert np.all(np.isinf(d[~ok]))
+            xi = x[lab_of[ids[ok]].astype(np.int64)]
+            ref = ((xi - q[i]) ** 2).sum(1) if space == "l2" else 1.0 - xi @ q[i]
+            assert np.allclose(d[ok], ref, rtol=1e-4, atol=1e-4), (i, r)
+    # the final row's re-rank answer is the search's own result
+    final = learned.checkpoint_answers({"ids": ck["ids"][rows, n - 1][:, None, :],
+                                        "ckpt_dists": ck["ckpt_dists"][rows, n - 1][:, None, :]}, k)[:, 0, :]
+    assert np.all(final != 0xffffffff)  # full pools: 8,000 rows, ef 48
+    got = lab_of[final.astype(np.int64)]
+    same = np.mean([set(got[i]) == set(ck["labels"][i]) for i in rows])
+    assert same >= 0.99, same

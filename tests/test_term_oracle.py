@@ -75,3 +75,20 @@ def test_checkpoint_labels():
     ck["ids"][0, 2] = [0, 1, 2]  # final hits 3: only row 1 reaches it
     X, y = learned.checkpoint_dataset(idx, ck, gt)
     assert np.array_equal(y, [0, 1, 1])
+
+
+def test_checkpoint_answers_rerank_order():
+    """With recorded float32 distances a row's answer is its k closest
+    recorded entries (equal distances by beam position), as a re-rank
+    returns them; without, the first k entries."""
+    N = 0xffffffff
+    ids = np.array([[[7, 3, 5, 9, N]]], np.uint32)
+    d = np.array([[[0.5, 0.1, 0.3, 0.1, np.inf]]], np.float32)
+    assert np.array_equal(learned.checkpoint_answers({"ids": ids}, 2), [[[7, 3]]])
+    assert np.array_equal(learned.checkpoint_answers({"ids": ids, "ckpt_dists": d}, 3), [[[3, 9, 5]]])
+    # labels then follow the re-ranked answer
+    idx = _FakeIndex(100 + np.arange(10))
+    ck = dict(ids=np.concatenate([ids, ids], axis=1), ckpt_dists=np.concatenate([d, d], axis=1),
+              nckpt=np.array([2], np.uint32), feat=np.zeros((1, 2, learned.F), np.float32))
+    X, y = learned.checkpoint_dataset(idx, ck, np.array([[103, 109]], np.uint64))
+    assert X.shape == (1, learned.F) and np.array_equal(y, [1])
