@@ -582,19 +582,26 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     __syncwarp();
     ct.upper_dists += 1;
     const uint32_t up_stride = p.maxM + 1;
+    // the upper-layer offset of the current node; each pass loads its
+    // candidates' offsets beside their rows, so the next hop's is known
+    uint32_t cur_off = LCHK(cur < p.count, 272, cur, 0) ? __ldg(p.upper_off + cur) : 0xffffffffu;
     for (int level = p.maxlevel; level > 0; level--) {
         while (true) {
-            if (!LCHK(cur < p.count && p.upper_off[cur] != 0xffffffffu, 270, cur, level)) break;
-            const uint32_t* row = p.upper_links + (size_t)(p.upper_off[cur] + (uint32_t)(level - 1)) * up_stride;
+            if (!LCHK(cur < p.count && cur_off != 0xffffffffu, 270, cur, level)) break;
+            const uint32_t* row = p.upper_links + (size_t)(cur_off + (uint32_t)(level - 1)) * up_stride;
             const int cnt = LCHK((__ldg(row) & 0xffffu) <= p.maxM, 271, __ldg(row), cur) ? (int)(__ldg(row) & 0xffffu) : 0;
             ct.upper_hops += 1;
             ct.upper_dists += cnt;
             float best = curd;
-            uint32_t best_id = INVALID_ID;
+            uint32_t best_id = INVALID_ID, best_off = 0xffffffffu;
             for (int c0 = 0; c0 < cnt; c0 += 64) {
                 const int n = min(64, cnt - c0);
-                if (lane < n) s.cid[lane] = __ldg(row + 1 + c0 + lane);
-                if (lane + 32 < n) s.cid[lane + 32] = __ldg(row + 1 + c0 + lane + 32);
+                const uint32_t ida = lane < n ? __ldg(row + 1 + c0 + lane) : INVALID_ID;
+                const uint32_t idb = lane + 32 < n ? __ldg(row + 1 + c0 + lane + 32) : INVALID_ID;
+                if (lane < n) s.cid[lane] = ida;
+                if (lane + 32 < n) s.cid[lane + 32] = idb;
+                const uint32_t offa = ida < p.count ? __ldg(p.upper_off + ida) : 0xffffffffu;
+                const uint32_t offb = idb < p.count ? __ldg(p.upper_off + idb) : 0xffffffffu;
                 __syncwarp();
                 uint32_t i0, i1 = INVALID_ID;
                 float d0 = lean_pass<SPACE, NS, MULTI>(p, s, lq, 0, n, lane, i0);
@@ -608,14 +615,17 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
                 if (m < best) {
                     // the first neighbour in list order with that distance
                     const unsigned h0 = __ballot_sync(FULL, d0 == m), h1 = __ballot_sync(FULL, d1 == m);
+                    const int src = h0 ? __ffs(h0) - 1 : __ffs(h1) - 1;
                     best = m;
-                    best_id = h0 ? __shfl_sync(FULL, i0, __ffs(h0) - 1) : __shfl_sync(FULL, i1, __ffs(h1) - 1);
+                    best_id = __shfl_sync(FULL, h0 ? i0 : i1, src);
+                    best_off = __shfl_sync(FULL, h0 ? offa : offb, src);
                 }
                 __syncwarp();
             }
             if (best_id == INVALID_ID) break;
             cur = best_id;
             curd = best;
+            cur_off = best_off;
         }
     }
 
