@@ -856,8 +856,9 @@ def run_learned96(args, dist: Dist):
     reference-built HNSW M=32, ef_construction=400, k=10, ef cap 512.  QPS at
     recall@10 >= target of the plain fixed-ef beam (smallest ef of the sweep)
     and of the learned stop (cap and threshold calibrated on held-out
-    training queries).  The low-precision beam needs maxM0 <= 32, so both
-    arms traverse float32 rows here."""
+    training queries), over float32 rows and over the fp8 copy (the lean
+    beam, one 64-slot link row per iteration for M = 32) with a float32
+    re-rank."""
     import torch
 
     from hnsw_rabitq_b200 import Index, _capi, learned
@@ -918,6 +919,38 @@ def run_learned96(args, dist: Dist):
     ms_l, clk = loop.time(o, args.steps, args.warmup, dist, clocks=True)
     _, _, _, tr_l = idx.knn_query_traced(q, 10, ef=model.ef_cap, tie_order="id", learned=True)
     qps_l, qps_p = nq / (ms_l / 1e3), nq / (ms_p / 1e3)
+
+    # ---- FP8 traversal + float32 re-rank: fixed ef, then the learned stop
+    # (traces at ef 128, labelled by what the re-rank returns; calibrated on
+    # measured time, so it falls back to fixed ef when the network does not pay)
+    _capi.check(_capi.lib().hnswgpu_build_traversal_copy(idx._h, _capi.PREC_FP8))
+    sweep8, ef_8 = [], None
+    for ef in [16, 24, 32, 40, 48, 56, 64, 80, 96, 128, 160, 192, 256, 320, 384, 448, 512]:
+        loop.step(loop.opts(ef, 0, _capi.PREC_FP8))
+        r = recall(loop.labels(), gt)
+        sweep8.append({"ef": ef, "recall": round(r, 5)})
+        if r >= target:
+            ef_8 = ef
+            break
+    ef_8 = ef_8 or 512
+    ms_8, _ = loop.time(loop.opts(ef_8, 0, _capi.PREC_FP8), args.steps, args.warmup, dist)
+    _, _, _, tr_8 = idx.knn_query_traced(q, 10, ef=ef_8, tie_order="id", precision="fp8")
+    t0 = time.perf_counter()
+    model8, rep8 = learned.fit(idx, tq[: min(len(tq), 6000)], k=10, ef_cap=128, period=4, target_recall=target,
+                               precision="fp8", epochs=20, seed=0)
+    fit8_s = time.perf_counter() - t0
+    o8 = loop.opts(model8.ef_cap, _capi.LEARNED_STOP, _capi.PREC_FP8)
+    loop.step(o8)
+    rec8 = recall(loop.labels(), gt)
+    ms_l8, _ = loop.time(o8, args.steps, args.warmup, dist)
+    _, _, _, tr_l8 = idx.knn_query_traced(q, 10, ef=model8.ef_cap, tie_order="id", precision="fp8", learned=True)
+    fp8 = {"fixed": {"ef": ef_8, "qps": round(nq / (ms_8 / 1e3), 1), "recall@10": sweep8[-1]["recall"],
+                     "mean_l0_expansions": round(float(tr_8[:, 2].mean()), 1), "sweep": sweep8},
+           "learned": {"ef_cap": model8.ef_cap, "threshold": model8.threshold, "recall@10": round(rec8, 5),
+                       "qps": round(nq / (ms_l8 / 1e3), 1),
+                       "mean_l0_expansions": round(float(tr_l8[:, 2].mean()), 1), "samples": rep8["samples"],
+                       "fit_seconds": round(fit8_s, 1)},
+           "speedup_fp8_learned_vs_fp32_plain": round(ms_p / ms_l8, 3)}
     return {"metric": "QPS at recall@10>=0.95, learned termination vs fixed ef, heterogeneous 96-d mixture",
             "value": round(qps_l, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_l, 4), "higher_is_better": True, "scaling": "weak",
@@ -932,7 +965,7 @@ def run_learned96(args, dist: Dist):
                        "plain": {"ef": ef_p, "qps": round(qps_p, 1), "recall@10": sweep[-1]["recall"],
                                  "mean_l0_expansions": round(float(tr_p[:, 2].mean()), 1),
                                  "p99_l0_expansions": float(np.percentile(tr_p[:, 2], 99)), "sweep": sweep}},
-            "speedup_vs_plain": round(qps_l / qps_p, 3), "clocks": clk, "gpu_launches": args.steps}
+            "speedup_vs_plain": round(qps_l / qps_p, 3), "fp8": fp8, "clocks": clk, "gpu_launches": args.steps}
 
 
 def committed_traffic(tie_order, ef):
