@@ -46,6 +46,13 @@
 #define HNSWGPU_MINB_LEAN 10
 #endif
 
+// Where the learned-stop kernels read the packed network: 1 = one copy in
+// shared memory per 4-warp CTA (residency 16 warps per SM), 0 = through the
+// read-only cache from 2-warp CTAs (the fixed-ef residency).
+#ifndef HNSWGPU_LEAN_MODEL_SMEM
+#define HNSWGPU_LEAN_MODEL_SMEM 1
+#endif
+
 namespace hnswgpu {
 
 // Optional self-checks (compile with -DHNSWGPU_BOUNDS_CHECK; the shipped
@@ -420,7 +427,8 @@ __device__ __forceinline__ bool lean_checkpoint(const SearchParams& p, const Lea
         ts.nckpt++;
         return false;
     }
-    return term_logit<true>(s.model, fe, lane) > p.term_logit;
+    if (HNSWGPU_LEAN_MODEL_SMEM) return term_logit<true>(s.model, fe, lane) > p.term_logit;
+    return term_logit<false>(p.term_model, fe, lane) > p.term_logit;
 }
 
 template <int SPACE>
@@ -812,14 +820,14 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
     LPT(8);
 }
 
-// Query warps per CTA: the learned-stop kernels keep one copy of the packed
-// network in shared memory for four warps.
+// Query warps per CTA of each kernel form.
 template <int TERM>
 struct LeanCta {
-    static constexpr int kWarps = TERM == 2 ? kLeanWarpsPerBlockLearned : kLeanWarpsPerBlock;
-    static constexpr size_t kModel = TERM == 2 ? kLeanModelSmem : 0;
-    // learned stop: the network copy limits residency to four CTAs (16 warps)
-    static constexpr int kMinBlocks = TERM == 2 ? 4 : HNSWGPU_MINB_LEAN;
+    static constexpr bool kSmemModel = TERM == 2 && HNSWGPU_LEAN_MODEL_SMEM;
+    static constexpr int kWarps = kSmemModel ? kLeanWarpsPerBlockLearned : kLeanWarpsPerBlock;
+    static constexpr size_t kModel = kSmemModel ? kLeanModelSmem : 0;
+    // learned stop in shared memory: the network copy limits residency to four CTAs (16 warps)
+    static constexpr int kMinBlocks = kSmemModel ? 4 : HNSWGPU_MINB_LEAN;
 };
 
 template <int SPACE, int TERM, int NS, bool MULTI>
@@ -827,7 +835,7 @@ __global__ void __launch_bounds__(LeanCta<TERM>::kWarps * 32, LeanCta<TERM>::kMi
     hnsw_lean_kernel(SearchParams p) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (TERM == 2) {
+    if (LeanCta<TERM>::kSmemModel) {
         const uint4* src = reinterpret_cast<const uint4*>(p.term_model);
         uint4* dst = reinterpret_cast<uint4*>(smem);
         for (uint32_t i = threadIdx.x; i < (uint32_t)(kTermPackedBytes / 16); i += blockDim.x) dst[i] = __ldg(src + i);
