@@ -38,6 +38,7 @@
 
 #include "device_common.cuh"
 #include "hnsw_search.h"
+#include "launch_cache.h"
 #include "term_mlp.cuh"
 
 // resident 2-warp CTAs per SM: 10 (20 query warps, 96 registers) was 9 %
@@ -892,22 +893,13 @@ __global__ void __launch_bounds__(LeanCta<TERM>::kWarps * 32, LeanCta<TERM>::kMi
 
 template <int SPACE, int TERM, int NS, bool MULTI>
 cudaError_t launch_lean_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
-    static int attr_smem = -1;
-    static size_t occ_smem = 0;
-    static int occ_per_sm = 0;
+    static LaunchCache cache;  // per device: opt-in shared memory and occupancy
     const void* fn = (const void*)hnsw_lean_kernel<SPACE, TERM, NS, MULTI>;
     constexpr int wpb = LeanCta<TERM>::kWarps;
     const size_t smem = LeanCta<TERM>::kModel + (size_t)p.warp_smem * wpb;
-    if ((int)smem > attr_smem) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_smem = (int)smem;
-    }
-    if (smem != occ_smem) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, fn, wpb * 32, smem);
-        if (e != cudaSuccess) return e;
-        occ_smem = smem;
-    }
+    int occ_per_sm = 0;
+    cudaError_t e = cache.blocks_per_sm(fn, wpb * 32, smem, &occ_per_sm);
+    if (e != cudaSuccess) return e;
     if (occ_per_sm < 1) return cudaErrorInvalidConfiguration;
     const uint64_t need = (p.nq + wpb - 1) / wpb;
     uint64_t blocks = (uint64_t)occ_per_sm * (uint64_t)num_sms;

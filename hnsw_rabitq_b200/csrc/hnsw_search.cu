@@ -42,6 +42,7 @@
 
 #include "device_common.cuh"
 #include "hnsw_search.h"
+#include "launch_cache.h"
 #include "ref_heap.h"
 #include "term_mlp.cuh"
 
@@ -1532,22 +1533,13 @@ size_t warp_smem_layout(SearchParams& p) {
 namespace {
 template <int SPACE, bool FAST16, bool EXACT, int PREC, int TERM = 0, bool TIES = false, bool FILTER = false>
 cudaError_t launch_t(const SearchParams& p, int num_sms, cudaStream_t stream, int* blocks_out) {
-    // per-instantiation cache of the opt-in shared-memory size and occupancy
-    static int attr_smem = -1;
-    static size_t occ_smem = 0;
-    static int occ_per_sm = 0;
+    // per-instantiation, per-device cache of the opt-in shared-memory size and occupancy
+    static LaunchCache cache;
     const void* fn = (const void*)hnsw_search_kernel<SPACE, FAST16, EXACT, PREC, TERM, TIES, FILTER>;
     const size_t smem = (size_t)p.warp_smem * kWarpsPerBlock;
-    if ((int)smem > attr_smem) {
-        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_smem = (int)smem;
-    }
-    if (smem != occ_smem) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_per_sm, fn, kWarpsPerBlock * 32, smem);
-        if (e != cudaSuccess) return e;
-        occ_smem = smem;
-    }
+    int occ_per_sm = 0;
+    cudaError_t e = cache.blocks_per_sm(fn, kWarpsPerBlock * 32, smem, &occ_per_sm);
+    if (e != cudaSuccess) return e;
     if (occ_per_sm < 1) return cudaErrorInvalidConfiguration;
     uint64_t need = (p.nq + kWarpsPerBlock - 1) / kWarpsPerBlock;
     uint64_t blocks = (uint64_t)occ_per_sm * (uint64_t)num_sms;
