@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "bf_tc.h"
@@ -792,7 +793,9 @@ cudaError_t launch_fp64_distances(const float* q, uint64_t nq, uint32_t m, uint3
 
 cudaError_t tc_encode_map(void* base, uint32_t prec, uint64_t rows, uint32_t dim, uint64_t row_pitch_bytes,
                           uint32_t box_rows, CUtensorMap* out) {
-    static PFN_cuTensorMapEncodeTiled encode = nullptr;
+    // the driver entry point, looked up once (host threads may race here)
+    static std::atomic<PFN_cuTensorMapEncodeTiled> encode_fn{nullptr};
+    PFN_cuTensorMapEncodeTiled encode = encode_fn.load(std::memory_order_acquire);
     if (!encode) {
         cudaDriverEntryPointQueryResult q;
         void* fp = nullptr;
@@ -800,6 +803,7 @@ cudaError_t tc_encode_map(void* base, uint32_t prec, uint64_t rows, uint32_t dim
         if (e != cudaSuccess) return e;
         if (q != cudaDriverEntryPointSuccess || !fp) return cudaErrorNotSupported;
         encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(fp);
+        encode_fn.store(encode, std::memory_order_release);
     }
     const cuuint64_t gdim[2] = {dim, rows};
     const cuuint64_t gstride[1] = {row_pitch_bytes};
