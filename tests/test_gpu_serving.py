@@ -7,6 +7,7 @@ import pytest
 
 import hnsw_rabitq_b200 as H
 from hnsw_rabitq_b200 import learned
+from oracle import oracle as O
 from hnsw_rabitq_b200.serving import Server, poisson_arrivals
 from tests.helpers import build_hnsw
 
@@ -28,7 +29,7 @@ def served(tmp_path_factory):
     # here is that the learned stop is deterministic per query
     f = rng.normal(size=(100, learned.F)).astype(np.float32)
     g.set_termination_model(learned.TerminationModel(learned.init_params(f, 1), 4, 0.5))
-    return g, x, q
+    return g, x, q, path
 
 
 def _mix(n, rng, parity_id):
@@ -50,7 +51,7 @@ def _mix(n, rng, parity_id):
 
 
 def test_same_alone_and_in_mix(served):
-    g, x, q = served
+    g, x, q, _ = served
     rng = np.random.default_rng(9)
     with Server(g, max_inflight=6, max_batch=256) as srv:
         parity = srv.add_filter(lambda l: l % 2 == 0)
@@ -76,7 +77,7 @@ def test_same_alone_and_in_mix(served):
 @pytest.mark.parametrize("precision", ["fp32", "fp8"])
 def test_matches_batch_search(served, precision):
     """A served request equals the batched C-ABI search with the same settings."""
-    g, x, q = served
+    g, x, q, _ = served
     with Server(g) as srv:
         parity = srv.add_filter(lambda l: l % 2 == 0)
         n = 300
@@ -92,7 +93,7 @@ def test_matches_batch_search(served, precision):
 
 def test_admission_budget_serialises(served):
     """A budget of one query's footprint forces batches of one."""
-    g, x, q = served
+    g, x, q, _ = served
     with Server(g, smem_budget=1) as srv:
         with pytest.raises(RuntimeError, match="exceeds the admission budget"):
             srv.replay(q[:3], [Server.request(k=10, ef=64)] * 3, np.zeros(3))
@@ -105,7 +106,7 @@ def test_admission_budget_serialises(served):
 
 
 def test_rejects_bad_requests(served):
-    g, x, q = served
+    g, x, q, _ = served
     with Server(g) as srv:
         with pytest.raises(RuntimeError, match="unknown filter"):
             srv.submit(q[0], k=10, filter=3)
@@ -113,3 +114,36 @@ def test_rejects_bad_requests(served):
             srv.submit(q[0], k=10, tie_order="reference", learned=True)
         with pytest.raises(RuntimeError, match="k must be positive"):
             srv.submit(q[0], k=0)
+
+
+def test_mix_matches_the_reference(served):
+    """Float32 requests served inside the mix (5 % deleted, label-parity
+    filter on 30 %, mixed k and ef, fp8 / learned-stop / tie-exact neighbours
+    in flight) return the reference's own results: tie-exact requests
+    hnswlib's searchKnn (the oracle's reference mode), plain id-order ones
+    the oracle's canonical mode, labels and distance bits."""
+    g, x, q, path = served
+    o = O.Hnsw(str(path), "l2", 64)
+    for lab in range(0, 20000, 20):
+        assert o.set_deleted(lab, True) == 0
+    allow = np.array([1 if int(l) % 2 == 0 else 0 for l in o.labels()], np.uint8)
+    rng = np.random.default_rng(21)
+    with Server(g, max_inflight=6, max_batch=256) as srv:
+        parity = srv.add_filter(lambda l: l % 2 == 0)
+        reqs = _mix(len(q), rng, parity)
+        ml, md, mc, _ = srv.replay(q, reqs, poisson_arrivals(len(q), 100_000, seed=4))
+    groups = {}
+    for i, r in enumerate(reqs):
+        if r.precision != H._capi.PREC_FP32 or r.flags & H._capi.LEARNED_STOP:
+            continue
+        mode = O.REFERENCE if r.flags & H._capi.EXACT_TIES else O.CANONICAL
+        groups.setdefault((r.k, r.ef, r.filter >= 0, mode), []).append(i)
+    checked = 0
+    for (k, ef, filtered, mode), idx in groups.items():
+        rl, rd, rc = o.search(q[idx], k, ef, mode=mode, allow=allow if filtered else None)
+        for j, i in enumerate(idx):
+            assert mc[i] == rc[j], (i, k, ef, filtered, mode)
+            assert np.array_equal(ml[i, :mc[i]], rl[j, :rc[j]]), (i, k, ef, filtered, mode)
+            assert np.array_equal(md[i, :mc[i]].view(np.uint32), rd[j, :rc[j]].view(np.uint32)), i
+        checked += len(idx)
+    assert checked > 300
