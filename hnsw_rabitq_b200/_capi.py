@@ -66,6 +66,7 @@ SIGNATURES = {
     "hnswgpu_last_error": (C.c_char_p, []),
     "hnswgpu_version": (C.c_char_p, []),
     "hnswgpu_load_hnsw": (C.c_int, [C.c_char_p, C.c_int, U64, U64, C.c_int, C.POINTER(P)]),
+    "hnswgpu_load_hnsw_buffer": (C.c_int, [P, U64, C.c_int, U64, U64, C.c_int, C.POINTER(P)]),
     "hnswgpu_load_bf": (C.c_int, [C.c_char_p, C.c_int, U64, C.c_int, C.POINTER(P)]),
     "hnswgpu_create_bf": (C.c_int, [C.c_int, U64, P, P, U64, U64, C.c_int, C.POINTER(P)]),
     "hnswgpu_free": (C.c_int, [P]),

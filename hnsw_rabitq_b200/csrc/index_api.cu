@@ -69,9 +69,31 @@ using namespace hnswgpu_host;
 
 namespace {
 template <class T>
-void rd(std::ifstream& in, T& v) {
+void rd(std::istream& in, T& v) {
     in.read((char*)&v, sizeof(T));
 }
+
+// Read-only, seekable stream buffer over a caller's memory (an index image,
+// e.g. the bytes of a pickled state): the file loader reads it in place.
+class MemBuf : public std::streambuf {
+public:
+    MemBuf(const char* p, size_t n) {
+        char* b = const_cast<char*>(p);
+        setg(b, b, b + n);
+    }
+
+protected:
+    pos_type seekoff(off_type off, std::ios_base::seekdir dir, std::ios_base::openmode) override {
+        const std::ptrdiff_t size = egptr() - eback();
+        const std::ptrdiff_t base = dir == std::ios_base::beg ? 0 : dir == std::ios_base::cur ? gptr() - eback() : size;
+        if (off < -base || off > size - base) return pos_type(off_type(-1));
+        setg(eback(), eback() + base + off, egptr());
+        return pos_type(base + off);
+    }
+    pos_type seekpos(pos_type pos, std::ios_base::openmode m) override {
+        return seekoff(off_type(pos), std::ios_base::beg, m);
+    }
+};
 }  // namespace
 
 namespace hnswgpu_host {
@@ -92,10 +114,8 @@ void init_common(hnswgpu_index* h, int device) {
 // HierarchicalNSW::loadIndex (hnswlib/hnswalg.h:715-821) plus the structural
 // checks a GPU kernel needs before it may follow the links (ids in range,
 // upper-level lists present where the descent reads them).
-void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim, uint64_t max_elements_i,
-                    bool multivector) {
-    std::ifstream in(path, std::ios::binary);
-    if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+void load_hnsw_stream(hnswgpu_index* h, std::istream& in, int space, uint64_t dim, uint64_t max_elements_i,
+                      bool multivector) {
     in.seekg(0, in.end);
     const std::streamoff total = in.tellg();
     in.seekg(0, in.beg);
@@ -279,6 +299,13 @@ void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim,
         h->docs.alloc(std::max<size_t>(cur, 1));
         up(h->docs.p, hdocs.data(), cur * 4);
     }
+}
+
+void load_hnsw_file(hnswgpu_index* h, const char* path, int space, uint64_t dim, uint64_t max_elements_i,
+                    bool multivector) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in.is_open()) throw ApiError(HNSWGPU_ERR_IO, "Cannot open file");
+    load_hnsw_stream(h, in, space, dim, max_elements_i, multivector);
 }
 
 // BruteforceSearch::loadIndex (hnswlib/bruteforce.h:142-161).
@@ -895,6 +922,22 @@ int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_el
         init_common(h.get(), device);
         load_hnsw_file(h.get(), path, space, dim, max_elements, false);
         h->source_path = path;
+        *out = h.release();
+        return HNSWGPU_OK;
+    });
+}
+
+int hnswgpu_load_hnsw_buffer(const void* data, uint64_t size, int space, uint64_t dim, uint64_t max_elements,
+                             int device, hnswgpu_index** out) {
+    return guarded([&] {
+        if (!data || !out || dim == 0) return fail(HNSWGPU_ERR_ARG, "invalid argument");
+        if (space < 0 || space > 3) return fail(HNSWGPU_ERR_ARG, "Space name must be one of l2, ip, or cosine.");
+        *out = nullptr;
+        std::unique_ptr<hnswgpu_index> h(new hnswgpu_index());
+        init_common(h.get(), device);
+        MemBuf mb(static_cast<const char*>(data), (size_t)size);
+        std::istream in(&mb);
+        load_hnsw_stream(h.get(), in, space, dim, max_elements, false);
         *out = h.release();
         return HNSWGPU_OK;
     });

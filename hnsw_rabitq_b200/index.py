@@ -348,18 +348,20 @@ class Index(_GpuIndex):
         if not d.get("index_inited", False):
             self._default_ef = int(d.get("ef", 10))
             return
-        import tempfile
-        fd, tmp = tempfile.mkstemp(suffix=".bin")
-        try:
-            with os.fdopen(fd, "wb") as f:
-                f.write(pickling.state_to_file_bytes(d))
-            self.load_index(tmp)
-            # a later pickle or save_index rereads the source: keep it in memory
-            with open(tmp, "rb") as f:
-                self._state_bytes = f.read()
-        finally:
-            os.unlink(tmp)
+        # the state's index image goes to the GPU loader straight from memory;
+        # a later pickle or save_index rebuilds from the same bytes
+        buf = pickling.state_to_file_bytes(d)
+        self._free()
+        h = C.c_void_p()
+        space_id = _SPACES.get(self.space, self._extra_spaces.get(self.space))
+        cbuf = C.c_char_p(buf)
+        _capi.check(_capi.lib().hnswgpu_load_hnsw_buffer(C.cast(cbuf, C.c_void_p), len(buf), space_id, self.dim, 0,
+                                                         self.device, C.byref(h)))
+        self._h = h
+        self._state_bytes = buf
         self._source = None
+        self._marks = {}
+        self._max_elements = None
         self.set_ef(int(d["ef"]))
 
     @classmethod

@@ -165,6 +165,14 @@ HNSWGPU_API const char* hnswgpu_version(void);
 HNSWGPU_API int hnswgpu_load_hnsw(const char* path, int space, uint64_t dim, uint64_t max_elements, int device,
                       hnswgpu_index** out);
 
+/* The same from an index image in memory (`size` bytes laid out as the file):
+ * the Python binding's unpickling (createFromParams, bindings.cpp:485-519)
+ * goes through it without a file.  The buffer is read during the call only.
+ * hnswgpu_save_hnsw has no source to rewrite for such an index (the caller
+ * holds the image). */
+HNSWGPU_API int hnswgpu_load_hnsw_buffer(const void* data, uint64_t size, int space, uint64_t dim,
+                                         uint64_t max_elements, int device, hnswgpu_index** out);
+
 /* Load a BruteforceSearch index file.  Replaces
  * BruteforceSearch(SpaceInterface*, const std::string& location)
  * (hnswlib/bruteforce.h:35-43) and BruteforceSearch::loadIndex

@@ -143,6 +143,9 @@ def test_newer_entry_points_reject_bad_arguments():
     assert lib.hnswgpu_term_train(0, None, None, 0, C.byref(to), None, None) == _capi.ERR_ARG
     assert lib.hnswgpu_term_loss_grad(0, None, None, None, 0, C.c_float(1.0), None, None) == _capi.ERR_ARG
     assert lib.hnswgpu_term_logits(0, None, None, 3, None) == _capi.ERR_ARG
+    h = C.c_void_p()
+    assert lib.hnswgpu_load_hnsw_buffer(None, 16, 0, 16, 0, 0, C.byref(h)) == _capi.ERR_ARG
+    assert lib.hnswgpu_load_hnsw_buffer(C.c_char_p(b"x" * 16), 16, 7, 16, 0, 0, C.byref(h)) == _capi.ERR_ARG
     # float64 oracle, serving loop
     assert lib.hnswgpu_fp64_distances(None, None, 1, None, 1, None) == _capi.ERR_ARG
     srv = C.c_void_p()

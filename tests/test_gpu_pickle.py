@@ -57,3 +57,26 @@ def test_pickle_from_params_and_save_index(tmp_path):
     c.set_ef(32)
     _check(c, g, "ef32_k10_del")
     assert c.get_max_elements() == 5000
+
+
+def test_load_from_memory_image():
+    """hnswgpu_load_hnsw_buffer (the unpickling path) reads the file image in
+    place: the same results as the file, bit for bit; a truncated or
+    corrupted image is rejected with the loader's format error."""
+    import ctypes as C
+    from hnsw_rabitq_b200 import _capi
+    g = golden()
+    buf = open(f"{GOLDEN}/hnsw_l2_d16.bin", "rb").read()
+    a = H.Index("l2", 16)
+    a.load_index(f"{GOLDEN}/hnsw_l2_d16.bin")
+    a.set_ef(32)
+    b = H.Index.from_params(PK.file_bytes_to_state(buf, "l2", 16, ef=32))
+    la, da = a.knn_query(g["hnsw_l2_d16/queries"], k=10)
+    lb, db = b.knn_query(g["hnsw_l2_d16/queries"], k=10)
+    assert np.array_equal(la, lb) and np.array_equal(da.view(np.uint32), db.view(np.uint32))
+    lib = _capi.lib()
+    for bad in (buf[: len(buf) // 2], buf[:40], buf + b"\0" * 8):
+        h = C.c_void_p()
+        cb = C.c_char_p(bad)
+        rc = lib.hnswgpu_load_hnsw_buffer(C.cast(cb, C.c_void_p), len(bad), 0, 16, 0, 0, C.byref(h))
+        assert rc == _capi.ERR_FORMAT and not h.value, (len(bad), rc)
