@@ -495,9 +495,9 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
     // per iteration where maxM0 <= 32) serves unfiltered id-order fp8 searches
     p.lean = hnswgpu::lean_eligible(p) ? 1u : 0u;
     p.lean_w = p.maxM0 <= 32 ? 2u : 1u;
-    // the lean beam's learned-stop kernels run four warps per CTA beside one
-    // copy of the network: budget for that case
-    const size_t wpb = p.lean ? hnswgpu::kLeanWarpsPerBlockLearned : hnswgpu::kWarpsPerBlock;
+    // (the lean beam's learned-stop kernels, four warps per CTA beside one
+    // copy of the network, are budgeted in apply_term)
+    const size_t wpb = p.lean ? hnswgpu::kLeanWarpsPerBlock : hnswgpu::kWarpsPerBlock;
     size_t ws = hnswgpu::warp_smem_layout(p);
     int max_optin = 0;
     cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
@@ -509,7 +509,7 @@ hnswgpu::SearchParams hnsw_params(const hnswgpu_index* h, const float* dq, uint6
         p.cand_cap -= p.ef;
         ws = hnswgpu::warp_smem_layout(p);
     }
-    if ((p.lean ? hnswgpu::kLeanModelSmem : 0) + ws * wpb > (size_t)max_optin)
+    if (ws * wpb > (size_t)max_optin)
         throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the per-query shared-memory budget");
     return p;
 }
@@ -549,6 +549,12 @@ void apply_term(const hnswgpu_index* h, hnswgpu::SearchParams& p, const TermCfg*
     if (p.log2_vis > 11) {
         p.log2_vis = 11;
         hnswgpu::warp_smem_layout(p);
+    }
+    if (p.term_mode == 2 && p.lean) {
+        int max_optin = 0;
+        cuda_check(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device), "attr");
+        if (hnswgpu::kLeanModelSmem + (size_t)p.warp_smem * hnswgpu::kLeanWarpsPerBlockLearned > (size_t)max_optin)
+            throw ApiError(HNSWGPU_ERR_UNSUPPORTED, "ef too large for the learned stop's per-query shared-memory budget");
     }
 }
 

@@ -153,3 +153,23 @@ def test_lean_traces_record_rerank_inputs(tmp_path, space):
     got = lab_of[final.astype(np.int64)]
     same = np.mean([set(got[i]) == set(ck["labels"][i]) for i in rows])
     assert same >= 0.99, same
+
+
+def test_lean_large_ef_budget(tmp_path):
+    """The fixed-ef fp8 beam is budgeted at its own two warps per CTA: ef 3000
+    runs (and finds nearly all true neighbours); the learned-stop form, four
+    warps beside the network copy, reports that this ef does not fit."""
+    rng = np.random.default_rng(17)
+    x = rng.standard_normal((20000, 64)).astype(np.float32)
+    q = rng.standard_normal((64, 64)).astype(np.float32)
+    path = tmp_path / "g.bin"
+    build_hnsw(path, x, "l2", M=16, efc=100, num_threads=8)
+    g = H.Index("l2", 64)
+    g.load_index(str(path))
+    ll, ld, _, _ = g.knn_query_traced(q, 10, ef=3000, tie_order="id", precision="fp8")
+    gt = g.knn_query_exact(q, 10)[0]
+    assert learned.recall(ll, gt) >= 0.99
+    g.set_termination_model(learned.TerminationModel(learned.init_params(rng.normal(size=(64, learned.F)), 0), 4,
+                                                     0.5, 3000, "fp8"))
+    with pytest.raises(RuntimeError, match="too large"):
+        g.knn_query_traced(q, 10, ef=3000, tie_order="id", precision="fp8", learned=True)
