@@ -41,10 +41,11 @@
 #include "launch_cache.h"
 #include "term_mlp.cuh"
 
-// resident 2-warp CTAs per SM: 10 (20 query warps, 96 registers) was 9 %
-// faster than 8 (128 registers) and no slower than 12 on the 1M x 128 workload
+// resident 2-warp CTAs per SM: on the 1M x 128 workload 9 (18 query warps,
+// 112 registers) was 2 % faster than 10 (96 registers, more spills), which
+// was 9 % faster than 8 (128 registers); 11 and 12 were slower
 #ifndef HNSWGPU_MINB_LEAN
-#define HNSWGPU_MINB_LEAN 10
+#define HNSWGPU_MINB_LEAN 9
 #endif
 
 // Where the learned-stop kernels read the packed network: 1 = one copy in
@@ -314,15 +315,16 @@ __device__ __forceinline__ int lower_bound_masked(const uint64_t* a, int n, uint
 
 // Insert the distinct keys of the lanes in `amask` (not present in the pool;
 // `pos` = lower_bound_masked of the lane's key) into the sorted pool, keeping
-// at most cap entries.  Returns the smallest insertion index; `top` is set
+// at most cap entries.  `klist[i]` is lane i's key (in shared memory: one
+// broadcast load per key instead of two shuffles).  Returns the smallest insertion index; `top` is set
 // when a key lands within the first kq entries.
 __device__ __forceinline__ int lean_merge(uint64_t* pool, int& size, int cap, unsigned amask, uint64_t key, int pos,
-                                         int lane, int kq, bool& top) {
+                                         int lane, int kq, bool& top, const uint64_t* klist) {
     const int na = __popc(amask);
     const bool mine = (amask >> lane) & 1u;
     int rank = 0;
     for (unsigned m = amask; m; m &= m - 1) {
-        const uint64_t k2 = shfl64(key, __ffs(m) - 1);
+        const uint64_t k2 = klist[__ffs(m) - 1];
         rank += k2 < key;
     }
     const int mpos = (int)__reduce_min_sync(FULL, mine ? (unsigned)pos : 0x7fffffffu);
@@ -335,7 +337,7 @@ __device__ __forceinline__ int lean_merge(uint64_t* pool, int& size, int cap, un
             const uint64_t e = have ? pool[i] : 0ull;
             const uint64_t em = e & KEY_MASK;
             int sh = 0;
-            for (unsigned m = amask; m; m &= m - 1) sh += shfl64(key, __ffs(m) - 1) < em;
+            for (unsigned m = amask; m; m &= m - 1) sh += klist[__ffs(m) - 1] < em;
             __syncwarp();
             if (have && i + sh < cap && LCHK(i + sh >= 0, 231, i, sh)) pool[i + sh] = e;
             __syncwarp();
@@ -780,7 +782,7 @@ __device__ void lean_search(const SearchParams& p, const LeanSmem& s, uint32_t q
             const unsigned amask = __ballot_sync(FULL, keep);
             if (!amask) continue;
             bool t2 = false;
-            hint = min(hint, lean_merge(s.pool, psize, ef, amask, key, pos, lane, kq, t2));
+            hint = min(hint, lean_merge(s.pool, psize, ef, amask, key, pos, lane, kq, t2, s.lacc + b0));
             top |= t2;
         }
         if (TERM && top) {
