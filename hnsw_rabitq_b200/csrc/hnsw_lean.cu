@@ -41,9 +41,11 @@
 #include "launch_cache.h"
 #include "term_mlp.cuh"
 
-// resident 2-warp CTAs per SM: on the 1M x 128 workload 9 (18 query warps,
-// 112 registers) was 2 % faster than 10 (96 registers, more spills), which
-// was 9 % faster than 8 (128 registers); 11 and 12 were slower
+// launch bound, resident 2-warp CTAs per SM.  On the 1M x 128 workload a
+// bound of 10 (96 registers, 20 query warps) was 9 % faster than 8 (128
+// registers); 11 and 12 were slower.  With a bound of 9 the compiler still
+// allocates 96 registers (10 CTAs reside) but schedules the loop differently,
+// 2 % faster than the bound of 10 (same-box A/B)
 #ifndef HNSWGPU_MINB_LEAN
 #define HNSWGPU_MINB_LEAN 9
 #endif
