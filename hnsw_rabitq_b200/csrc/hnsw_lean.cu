@@ -9,9 +9,10 @@
 //
 // Compared with the general pipelined beam (hnsw_search.cu) it spends far
 // fewer instructions per expansion:
-//   * no shared-memory staging: each lane gathers its quarter of four
-//     candidate rows straight into registers (16-byte loads that do not
-//     allocate in L1);
+//   * per-lane gathers: each lane copies its quarter of four candidate rows
+//     into its own shared-memory stage slots with cp.async (no registers
+//     held while the copies fly, no warp-wide barrier: a lane reads back only
+//     what it copied), then reads them as mma fragments;
 //   * distances on the tensor cores: mma.sync m16n8k32 e4m3 x e4m3 -> f32.
 //     The query is split into two e4m3 vectors q ~ s_hi * hi + s_lo * lo
 //     (the second holds the rounding residual of the first), placed in the
@@ -23,7 +24,11 @@
 //     slots, two per lane.  maxM0 = 64 (M = 32 graphs) runs one row per
 //     iteration in the same code;
 //   * acceptance by the beam's bound (pool not full, or closer than its
-//     worst entry), then one sorted merge of the accepted keys.
+//     worst entry), then one sorted merge of the accepted keys;
+//   * optional learned stop: a checkpoint every term_period expansions (at
+//     states where the top-k has been stable for a period and no waiting
+//     candidate is closer than the k-th result) runs the termination network
+//     on the tensor cores from a per-CTA shared-memory copy.
 //
 // Exactness is not the goal of this beam (its distances are approximate and
 // several rows are expanded at once); the returned distances are exact
