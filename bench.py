@@ -30,7 +30,10 @@ same run.  Recall is measured against exact top-10 from the GPU brute force
   resident queries, timed with CUDA events on the launch stream.
 * ``e2e``    -- the learned + FP8 search through the C ABI (hnswgpu_search)
   with pinned host buffers: host->device copy of the queries, search,
-  device->host copy of the labels/distances/counts every step, wall clock.
+  device->host copy of the labels/distances/counts every step, wall clock;
+  the asynchronous form, steps double-buffered on three streams so that a
+  step's copies overlap its neighbours' searches.  ``e2e_sync``: the
+  synchronous host-pointer call (copy in, search, copy out, synchronise).
 * ``roofline`` -- HBM bound: algorithmic bytes per query of the headline
   kernel from its own work counters (link lists x their size, fp8 rows of
   136 B -- 128 e4m3 bytes, scale and squared norm -- for upper-layer and
