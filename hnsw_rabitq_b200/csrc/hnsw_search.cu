@@ -93,12 +93,16 @@ __device__ __forceinline__ void mbar_complete_tx(uint64_t* bar, uint32_t bytes) 
 // region [stage, pool), src inside [base, base + nrows * row_bytes).
 __device__ __forceinline__ void stage_copy(const SearchParams& p, const WarpSmem& s, void* dst, const void* base,
                                            uint64_t row, uint64_t nrows, uint32_t row_bytes, unsigned code) {
+#ifdef HNSWGPU_BOUNDS_CHECK
     const unsigned char* dp = static_cast<const unsigned char*>(dst);
     const unsigned char* lo = reinterpret_cast<const unsigned char*>(s.stage);
     const unsigned char* hi = reinterpret_cast<const unsigned char*>(s.pool);
     const bool ok = DBG_OK(dp >= lo && dp + row_bytes <= hi && ((uintptr_t)dp & 15) == 0 && (row_bytes & 15) == 0,
                            code, dp - lo, row_bytes) &&
                     DBG_OK(row < nrows, code + 1, row, nrows);
+#else
+    const bool ok = true;
+#endif
     if (ok) {
         bulk_g2s(dst, static_cast<const unsigned char*>(base) + row * row_bytes, row_bytes, s.bar);
     } else {
