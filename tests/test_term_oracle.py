@@ -92,3 +92,29 @@ def test_checkpoint_answers_rerank_order():
               nckpt=np.array([2], np.uint32), feat=np.zeros((1, 2, learned.F), np.float32))
     X, y = learned.checkpoint_dataset(idx, ck, np.array([[103, 109]], np.uint64))
     assert X.shape == (1, learned.F) and np.array_equal(y, [1])
+
+
+class _RecordingIndex:
+    def __init__(self):
+        self.calls = []
+
+    def search_checkpoints(self, queries, k, **kw):
+        self.calls.append(dict(k=k, **kw))
+        return {}
+
+
+def test_traces_record_what_the_rerank_sees():
+    """fp32 traces record the top k; a low-precision beam records its first R
+    entries (R = the re-rank count, the whole beam when 0, at most the cap)
+    with their float32 distances."""
+    q = np.zeros((2, 4), np.float32)
+    idx = _RecordingIndex()
+    learned.traces(idx, q, 10, 96, 4, 32, "fp32", 0)
+    learned.traces(idx, q, 10, 96, 4, 32, "fp8", 0)
+    learned.traces(idx, q, 10, 96, 4, 32, "fp8", 40)
+    learned.traces(idx, q, 10, 96, 4, 32, "bf16", 500)
+    learned.traces(idx, q, 10, 96, 4, 32, "fp8", 4)
+    c = idx.calls
+    assert "ids_width" not in c[0] and not c[0].get("dists", False)
+    assert [x["ids_width"] for x in c[1:]] == [96, 40, 96, 10]
+    assert all(x["dists"] for x in c[1:]) and all(x["ef"] == 96 and x["period"] == 4 for x in c)
