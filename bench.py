@@ -21,7 +21,7 @@ same run.  Recall is measured against exact top-10 from the GPU brute force
 * fp8 at fixed ef: the same sweep over the fp8 beam (the learned stop's
   fallback and cap).
 * learned + FP8 (``value``): the termination network is trained on the GPU
-  from checkpoint traces of 20,000 training queries (a query stream disjoint
+  from checkpoint traces of 12,000 training queries (a query stream disjoint
   from the 10,000 evaluation queries), its cap and logit threshold
   calibrated on a held-out third of them at the target recall; a second
   held-out stream of 5,000 queries checks the calibrated recall and, if it
@@ -67,7 +67,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 CACHE = os.path.join(ROOT, ".cache")
-EFS = [10, 16, 24, 32, 40, 44, 48, 52, 56, 64, 80, 96, 128, 192, 256, 320, 400]
+EFS = [10, 16, 24, 32, 40, 44, 48, 50, 52, 54, 56, 60, 64, 80, 96, 128, 192, 256, 320, 400]
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 

@@ -262,7 +262,7 @@ def fit(index, queries: np.ndarray, k: int = 10, ef_cap: int = 64, period: int =
     params, losses = train(X, y, epochs=epochs, seed=seed, device=device)
     model = TerminationModel(params, period, float("inf"), ef_cap, precision, int(rerank))
     if caps is None:
-        caps = [c for c in (k, 16, 24, 32, 40, 44, 48, 52, 56, 64, 80, 96, 128, 192, 256, 384, 512)
+        caps = [c for c in (k, 16, 24, 32, 40, 44, 48, 50, 52, 54, 56, 60, 64, 80, 96, 128, 192, 256, 384, 512)
                 if k <= c <= ef_cap]
     cap, thr, curve = calibrate(index, queries[hold], gt[hold], k, model, target_recall, caps=caps, cost=cost)
     model.ef_cap, model.threshold = cap, thr
