@@ -1,7 +1,7 @@
 // Per-device cache of a kernel's launch set-up: the opt-in dynamic shared
 // memory already granted (cudaFuncSetAttribute applies to the current
-// device's context) and the resident CTAs per SM for the last shared-memory
-// size asked.  One cache per kernel instantiation; safe to use from several
+// device's context) and the resident CTAs per SM for the last block size and
+// shared-memory size asked.  One cache per kernel instantiation; safe to use from several
 // host threads and with indexes on several devices in one process.
 #pragma once
 #include <cuda_runtime.h>
@@ -19,6 +19,7 @@ public:
         for (int d = 0; d < kMaxDevices; d++) {
             attr_[d] = -1;
             occ_smem_[d] = 0;
+            occ_threads_[d] = 0;
             occ_blocks_[d] = -1;
         }
     }
@@ -37,11 +38,12 @@ public:
             if (e != cudaSuccess) return e;
             attr_[dev] = (int)smem;
         }
-        if (occ_blocks_[dev] < 0 || occ_smem_[dev] != smem) {
+        if (occ_blocks_[dev] < 0 || occ_smem_[dev] != smem || occ_threads_[dev] != threads) {
             int b = 0;
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, threads, smem);
             if (e != cudaSuccess) return e;
             occ_smem_[dev] = smem;
+            occ_threads_[dev] = threads;
             occ_blocks_[dev] = b;
         }
         *out = occ_blocks_[dev];
@@ -58,6 +60,7 @@ private:
     std::mutex mu_;
     int attr_[kMaxDevices];
     size_t occ_smem_[kMaxDevices];
+    int occ_threads_[kMaxDevices];
     int occ_blocks_[kMaxDevices];
 };
 
