@@ -604,9 +604,8 @@ def run_ours(args, dist: Dist):
             "value": round(value, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp8 traversal, f32 accumulation and re-rank", "data": "synthetic",
-            "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
-                                   "HNSW M=16 efc=200, 10,000 queries, k=10",
-                       "method": ("learned early termination (6-64-64-1 fp16 MLP every "
+            "config": {"workload": gmm128_label(args),
+                       "method": (f"learned early termination ({learned.F}-64-64-1 fp16 MLP every "
                                   f"{model.period} expansions) over an fp8 e4m3 per-row-scaled beam, fp32 re-rank")
                        if np.isfinite(model.threshold) else
                        ("fixed ef: the calibrated logit threshold is +inf (the network never stops a query "
@@ -971,6 +970,12 @@ def run_learned96(args, dist: Dist):
             "speedup_vs_plain": round(qps_l / qps_p, 3), "fp8": fp8, "clocks": clk, "gpu_launches": args.steps}
 
 
+def gmm128_label(args):
+    """The headline workload's name in the bench line, with its sizes."""
+    return (f"gmm_1m_128: {args.n:,} x 128 L2 (1024-comp. GMM, integer-valued), reference-built HNSW M=16 "
+            f"efc=200, {args.nq:,} queries, k=10")
+
+
 def committed_traffic(tie_order, ef):
     """DRAM bytes per launch of hnsw_search_kernel from the committed ncu
     summary (profiles/), for the same tie order and ef, or None."""
@@ -1048,8 +1053,7 @@ def run_reference(args, dist: Dist):
             "value": round(qps, 1), "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt / args.steps * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "gmm_1m_128: 1,000,000 x 128 L2 (1024-comp. GMM, integer-valued), reference-built "
-                                   "HNSW M=16 efc=200, 10,000 queries, k=10",
+            "config": {"workload": gmm128_label(args),
                        "method": "hnswlib 0.9.0 knn_query (CPU, fixed ef: the reference has no learned or "
                                  "FP8 search)", "ef": ef_star,
                        "recall@10_sample500": round(recall(lab[:500], gt), 5)},
