@@ -691,7 +691,7 @@ def run_bf768(args, dist: Dist):
     from hnsw_rabitq_b200.groundtruth import fp64_distances, fp64_topk
     dev = dist.local
     torch.cuda.set_device(dev)
-    n = args.n if args.n != 1_000_000 else 1_000_000
+    n = args.n
     x, q = gmm_unit_ip(n=n, nq=args.nq, dim=768)
     g = BFIndex("ip", 768)
     g.device = dev
@@ -753,8 +753,8 @@ def run_bf768(args, dist: Dist):
             "value": best["qps"], "unit": "queries/s", "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": best["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16 / fp8 e4m3 tensor-core scores, f32 re-rank", "data": "synthetic",
-            "config": {"workload": "gmm_unit_ip: 1,000,000 x 768 unit vectors (256-component mixture, noise norm 0.3), "
-                                   "10,000 queries, inner product, k=100, over-fetch 400",
+            "config": {"workload": f"gmm_unit_ip: {n:,} x 768 unit vectors (256-component mixture, noise norm 0.3), "
+                                   f"{args.nq:,} queries, inner product, k=100, over-fetch 400",
                        "fp64_gt_seconds": round(gt_s, 1), "fp64_gt_certified": float(cert.mean())},
             "arms": arms,
             "exact_fp32": {"qps": round(nq / (ms32 / 1e3), 1), "ms_per_step": round(ms32, 2),
@@ -844,8 +844,8 @@ def run_serve768(args, dist: Dist):
             "value": top["p99_us"], "unit": "us", "n_gpus": dist.world, "steps": len(lines), "warmup": 1,
             "ms_per_step": None, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "gmm_unit_ip 1,000,000 x 768 inner product, reference-built HNSW M=16 efc=200; "
-                                   "5% of labels deleted; 10,000 requests: k in {1,10,100}, ef in {32..512}, "
+            "config": {"workload": f"gmm_unit_ip {n:,} x 768 inner product, reference-built HNSW M=16 efc=200; "
+                                   f"5% of labels deleted; {args.nq:,} requests: k in {{1,10,100}}, ef in {{32..512}}, "
                                    "30% label-parity filter, learned termination (trained cap 128)",
                        "termination": {"threshold": model.threshold, "samples": rep["samples"],
                                        "fit_seconds": round(fit_s, 1)}},
