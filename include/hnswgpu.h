@@ -126,7 +126,9 @@ typedef struct hnswgpu_search_opts {
                                   distances before returning k.  The HNSW
                                   form needs dim % 16 == 0, maxM0 <= 32 and
                                   the id tie order; deletes and `allow` are
-                                  honoured.                                    */
+                                  honoured.  FP8 with no deleted element and
+                                  no `allow` / filter runs the lean beam and
+                                  takes maxM0 <= 64.                           */
     uint64_t ef;               /* 0: use the index's ef_ (setEf)               */
     const uint8_t* allow;      /* optional per-internal-id byte mask: nonzero =
                                   the filter functor accepts that node's label.
